@@ -1,0 +1,262 @@
+/*
+ * gprx_cuda.h — C ABI of the B200 (sm_100a) backend for gprx's exact-GPR and
+ * VFE-SGPR objective-and-prediction path.
+ *
+ * The reference (gprx 0.2.0, a Rust crate) has no FFI layer: its seams are
+ * Rust traits.  Each entry point below names the reference function whose
+ * work it takes over; a Rust `cuda` backend calls it from that seam (the
+ * binding is shown in INTEGRATION.md).
+ *
+ * Conventions
+ *  - Every call returns a gprx_status.  No exception, abort or panic crosses
+ *    this boundary.  A failed call leaves the handle as it was before the call
+ *    unless the entry point says otherwise; gprx_last_error() gives details.
+ *  - Host buffers are owned by the caller and only read or written during the
+ *    call.  Points are column-major: x[i + f*n] is feature f of point i
+ *    (gprx `data::pack_points`, src/data.rs).
+ *  - Hyperparameters are in log space, kernel parameters first in depth-first
+ *    leaf order, then log σn² (src/gpr/exact_fit.rs:212-236; docs/design.md
+ *    §"parameter order").
+ *  - One handle owns one CUDA stream and its device state; a handle is not
+ *    re-entrant, distinct handles may be used from distinct threads.
+ */
+#ifndef GPRX_CUDA_H
+#define GPRX_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GPRX_CUDA_ABI_VERSION 1
+
+/* ---- status codes: each maps onto a gprx GprError variant (src/error.rs:308-500) ---- */
+typedef int32_t gprx_status;
+enum {
+  GPRX_OK = 0,
+  GPRX_CHOLESKY_FAILED = 1,        /* GprError::CholeskyFailed{jitter, matrix_size, stage} */
+  GPRX_NONFINITE_KERNEL = 2,       /* GprError::NonFiniteKernelValue */
+  GPRX_SHAPE_MISMATCH = 3,         /* ShapeMismatch / LengthMismatch / DimensionMismatch */
+  GPRX_INVALID_POINT_ID = 4,       /* IndexOutOfRange on an unknown PointId (src/points.rs:156) */
+  GPRX_INSUFFICIENT_DATA = 5,      /* InsufficientData{n, min: 2} (src/gpr/online.rs:565) */
+  GPRX_CUDA_ERROR = 6,             /* no gprx counterpart: a CUDA runtime error */
+  GPRX_TIMEOUT = 7,                /* no gprx counterpart: a bounded device wait ran out */
+  GPRX_INVALID_HYPERPARAMETER = 8, /* InvalidHyperparameter / IntervalError::OutOfRange */
+  GPRX_NONFINITE_INPUT = 9,        /* NonFiniteInput */
+  GPRX_EMPTY_INPUT = 10,           /* EmptyInput */
+  GPRX_OUT_OF_MEMORY = 11,         /* no gprx counterpart: device allocation or HBM budget */
+  GPRX_INVALID_CONFIG = 12,        /* InvalidConfig */
+  GPRX_NOT_CONVERGED = 13,         /* OptimizationNotConverged{iterations} */
+  GPRX_INVALID_ARGUMENT = 14,      /* null handle / null pointer / bad enum */
+  GPRX_STALE_FACTOR = 15,          /* internal: the factor was consumed by a gradient */
+  GPRX_CAPACITY = 16               /* a fixed-size buffer was too small for the request */
+};
+
+/* CholeskyStage (src/error.rs:31-39) */
+enum {
+  GPRX_STAGE_FIT = 0,
+  GPRX_STAGE_PREDICT = 1,
+  GPRX_STAGE_ONLINE_INSERT = 2,
+  GPRX_STAGE_ONLINE_DELETE = 3
+};
+
+typedef struct {
+  gprx_status status;
+  double jitter;          /* CHOLESKY_FAILED: the last offset j tried */
+  uint64_t matrix_size;   /* CHOLESKY_FAILED: order of the matrix */
+  int32_t stage;          /* CHOLESKY_FAILED: GPRX_STAGE_* */
+  int32_t cuda_error;     /* CUDA_ERROR: the cudaError_t value */
+  uint64_t iterations;    /* NOT_CONVERGED: iterations run */
+  char message[256];
+} gprx_error_info;
+
+/* ---- kernel description: a flattened KernelSpec tree (src/kernel/spec.rs:106) ----
+ * Nodes are listed in prefix order.  SUM and PRODUCT give their arity in
+ * `arg`; RBF_ARD gives its number of dimensions in `arg`.  θ for the leaves is
+ * passed separately, in the same (depth-first) order:
+ *   RBF        1 param  log ℓ               k = exp(-r²/(2ℓ²))        (src/kernel/rbf.rs:18)
+ *   RBF_ARD    d params log ℓ_1..log ℓ_d    k = exp(-½ Σ Δ_f²/ℓ_f²)   (src/kernel/rbf_ard.rs:16)
+ *   CONSTANT   1 param  log c               k = c                     (src/kernel/constant.rs:12)
+ *   PERIODIC   2 params log ℓ, log p        k = exp(-2 sin²(π r/p)/ℓ²) (src/kernel/periodic.rs:598) */
+enum {
+  GPRX_NODE_SUM = 1,
+  GPRX_NODE_PRODUCT = 2,
+  GPRX_LEAF_RBF = 10,
+  GPRX_LEAF_RBF_ARD = 11,
+  GPRX_LEAF_CONSTANT = 12,
+  GPRX_LEAF_PERIODIC = 13
+};
+
+typedef struct {
+  int32_t kind;
+  int32_t arg;
+} gprx_kernel_node;
+
+/* Upper limits of the device kernel evaluator. */
+#define GPRX_MAX_NODES 16
+#define GPRX_MAX_PARAMS 40
+#define GPRX_MAX_DIM 32
+
+enum { GPRX_PRECISION_FP64 = 0, GPRX_PRECISION_MIXED = 1 };
+enum { GPRX_VARIANCE_LATENT = 0, GPRX_VARIANCE_OBSERVATION = 1 }; /* src/prediction.rs */
+enum { GPRX_JITTER_FIXED = 0, GPRX_JITTER_ADAPTIVE = 1 };          /* src/policy.rs:245,266 */
+
+/* Model options.  gprx_options_default() fills the reference's defaults:
+ * FP64, JitterPolicy::fixed(0.0) for exact models (src/policy.rs:230) and
+ * JitterPolicy::adaptive(1e-8, 10, 5, 1e-3) for the Sgpr K_mm factor. */
+typedef struct {
+  int32_t precision;
+  int32_t jitter_kind;
+  double jitter_initial;
+  double jitter_multiplier;
+  int32_t jitter_max_retries;
+  double jitter_max;
+  int32_t device;
+  int32_t block_size;     /* 0 = autotuned panel width of the blocked factor */
+} gprx_options;
+
+/* L-BFGS settings (src/optimizer/lbfgs.rs:28-46): history 10, ≤100 iterations,
+ * gradient tolerance √ε, logit map onto (1e-5, 1e5) per parameter. */
+typedef struct {
+  uint64_t max_iterations;
+  double tolerance;
+  int32_t history_size;
+  int32_t restarts;       /* extra starts (0 = none) */
+  uint64_t seed;          /* seed of the extra starts */
+  double interval_lo;     /* open interval of every parameter, user units */
+  double interval_hi;
+} gprx_lbfgs_options;
+
+typedef struct {
+  double nlml;
+  uint64_t iterations;
+  uint64_t evaluations;
+  double grad_norm;
+  int32_t converged;
+} gprx_fit_report;
+
+/* ------------------------------------------------------------------ */
+/* common                                                               */
+/* ------------------------------------------------------------------ */
+int32_t gprx_abi_version(void);
+void gprx_options_default(gprx_options* opt);
+void gprx_options_default_sparse(gprx_options* opt);
+void gprx_lbfgs_options_default(gprx_lbfgs_options* opt);
+/* Details of the last failed call on this thread. */
+gprx_status gprx_last_error(gprx_error_info* out);
+/* Number of kernels this library launched since load (instrumentation). */
+uint64_t gprx_launch_count(void);
+
+/* ------------------------------------------------------------------ */
+/* exact GPR (src/gpr/)                                                 */
+/* ------------------------------------------------------------------ */
+typedef struct gprx_exact gprx_exact;
+
+/* Validates and uploads X (n×d, column-major) and y; sizes the n×n device
+ * buffers.  Replaces FittedGpr::prepare + FitBuffers::new
+ * (src/gpr/fitted.rs:210-290, src/workspace.rs:100-119).  No factor yet. */
+gprx_status gprx_exact_create(const double* x, uint64_t n, uint64_t d, const double* y,
+                              const gprx_kernel_node* nodes, int32_t n_nodes,
+                              const double* theta, int32_t n_theta,
+                              const gprx_options* options, gprx_exact** out);
+gprx_status gprx_exact_destroy(gprx_exact* h);
+/* Re-uploads X and y of the same shape (the handle keeps its buffers). */
+gprx_status gprx_exact_set_data(gprx_exact* h, const double* x, const double* y);
+uint64_t gprx_exact_num_params(const gprx_exact* h);
+/* log θ of the kernel then log σn² (Gpr::get_params). */
+gprx_status gprx_exact_get_params(gprx_exact* h, double* out, uint64_t p);
+/* Writes θ and factors A = K + σn² I (+ jitter retries) at it; on failure
+ * the previous θ and its factor are restored (src/gpr/exact_fit.rs:196-206). */
+gprx_status gprx_exact_set_params(gprx_exact* h, const double* params, uint64_t p);
+/* Factors at the stored θ (Gpr<Fixed>::factor → factor_written_k_with_policy,
+ * src/gpr/factor.rs:515-542). */
+gprx_status gprx_exact_factor(gprx_exact* h);
+/* One NLML + gradient evaluation at `params` (ExactFit::value_and_gradient_into_fit,
+ * src/gpr/exact_fit.rs:319-341).  `grad` may be NULL (value only). */
+gprx_status gprx_exact_eval(gprx_exact* h, const double* params, uint64_t p,
+                            double* nlml, double* grad);
+/* NLML of the current factor (GprCore::neg_log_marginal_likelihood, src/gpr/shared.rs:245-260). */
+gprx_status gprx_exact_nlml(gprx_exact* h, double* nlml);
+/* jitter j the current factor took (ExactFit factor_jitter). */
+gprx_status gprx_exact_factor_jitter(gprx_exact* h, double* jitter);
+/* Predictive mean and diagonal variance at q query points (column-major q×d)
+ * (GprCore::write_moments, src/gpr/shared.rs:754-820). */
+gprx_status gprx_exact_predict(gprx_exact* h, const double* xs, uint64_t q, int32_t variance_kind,
+                               double* mean, double* var);
+/* α = A⁻¹ y of the current factor (n values). */
+gprx_status gprx_exact_alpha(gprx_exact* h, double* out, uint64_t n);
+/* Gpr::fit with the default Lbfgs (src/gpr/trainer.rs:533-613, src/optimizer/lbfgs.rs:126-172):
+ * optimizes θ, then refactors at the best θ and publishes α for predict. */
+gprx_status gprx_exact_fit(gprx_exact* h, const gprx_lbfgs_options* opt, gprx_fit_report* report);
+/* Per-stage device time of the last eval in milliseconds:
+ * [fill, factor, inverse, gradient, total] (the reference's insert-stages idea). */
+gprx_status gprx_exact_stage_times(gprx_exact* h, double* out5);
+
+/* ---- online exact GPR (src/gpr/online.rs) ---- */
+/* FittedGpr::into_online: LLT → LDLT (src/gpr/fitted.rs:757-765,
+ * src/gpr/factor_store.rs:157-179); assigns PointIds 0..n-1. */
+gprx_status gprx_online_begin(gprx_exact* h);
+/* OnlineGpr::insert (src/gpr/online.rs:794-906): bordered LDLT append. */
+gprx_status gprx_online_insert(gprx_exact* h, const double* x_new, double y_new, uint64_t* id);
+/* OnlineGpr::delete (src/gpr/online.rs:564-611): LDLT row/column delete. */
+gprx_status gprx_online_delete(gprx_exact* h, uint64_t id);
+uint64_t gprx_online_n(const gprx_exact* h);
+/* PointIds in buffer order (src/points.rs:76). */
+gprx_status gprx_online_point_ids(gprx_exact* h, uint64_t* out, uint64_t n);
+
+/* ------------------------------------------------------------------ */
+/* VFE sparse GPR (src/sgpr/)                                           */
+/* ------------------------------------------------------------------ */
+typedef struct gprx_sgpr gprx_sgpr;
+
+/* Uploads X (n×d), y and the inducing points Z (m×d); SparseCore::prepare
+ * (src/sparse/core.rs:314).  No assembly yet. */
+gprx_status gprx_sgpr_create(const double* x, uint64_t n, uint64_t d, const double* y,
+                             const double* z, uint64_t m,
+                             const gprx_kernel_node* nodes, int32_t n_nodes,
+                             const double* theta, int32_t n_theta,
+                             const gprx_options* options, gprx_sgpr** out);
+gprx_status gprx_sgpr_destroy(gprx_sgpr* h);
+uint64_t gprx_sgpr_num_params(const gprx_sgpr* h);
+gprx_status gprx_sgpr_get_params(gprx_sgpr* h, double* out, uint64_t p);
+/* assemble_vfe at the stored θ (src/sgpr/factor/vfe.rs:191-277). */
+gprx_status gprx_sgpr_factor(gprx_sgpr* h);
+/* FittedSgpr::value_and_gradient_into (src/sgpr/fitted.rs:306-326):
+ * reassembly, vfe_neg_log_marginal_likelihood (vfe.rs:338-369) and
+ * analytic_gradient (derivatives.rs:283-366).  `grad` may be NULL. */
+gprx_status gprx_sgpr_eval(gprx_sgpr* h, const double* params, uint64_t p, double* nlml, double* grad);
+gprx_status gprx_sgpr_nlml(gprx_sgpr* h, double* nlml);
+/* vfe_predict_into / vfe_latent (src/sgpr/factor/predict.rs:102-262). */
+gprx_status gprx_sgpr_predict(gprx_sgpr* h, const double* xs, uint64_t q, int32_t variance_kind,
+                              double* mean, double* var);
+gprx_status gprx_sgpr_fit(gprx_sgpr* h, const gprx_lbfgs_options* opt, gprx_fit_report* report);
+/* OnlineSgpr::insert → append_point (src/sgpr/online/mod.rs:1695-1810). */
+gprx_status gprx_sgpr_insert(gprx_sgpr* h, const double* x_new, double y_new, uint64_t* id);
+/* OnlineSgpr::delete (src/sgpr/online/mod.rs:903-1000): rank-1 downdate of L_B,
+ * reassembly when the downdate fails or the pivot gate does not hold. */
+gprx_status gprx_sgpr_delete(gprx_sgpr* h, uint64_t id);
+uint64_t gprx_sgpr_n(const gprx_sgpr* h);
+/* 1 when the last insert/delete updated in place, 0 when it reassembled. */
+int32_t gprx_sgpr_last_step_in_place(const gprx_sgpr* h);
+
+/* ------------------------------------------------------------------ */
+/* seeded random numbers (src/rng.rs): Xoshiro256++ seeded by SplitMix64 */
+/* ------------------------------------------------------------------ */
+typedef struct { uint64_t s[4]; } gprx_rng;
+void gprx_rng_seed(gprx_rng* rng, uint64_t seed);
+uint64_t gprx_rng_next_u64(gprx_rng* rng);
+double gprx_rng_unit(gprx_rng* rng);
+uint64_t gprx_rng_up_to(gprx_rng* rng, uint64_t max);
+double gprx_rng_normal(gprx_rng* rng);
+void gprx_rng_fill_unit(gprx_rng* rng, double* out, uint64_t count);
+void gprx_rng_fill_normal(gprx_rng* rng, double* out, uint64_t count);
+/* `count` distinct indices of 0..n-1 by a partial Fisher–Yates shuffle
+ * driven by up_to (the seeded inducing subset). */
+gprx_status gprx_rng_subset(gprx_rng* rng, uint64_t n, uint64_t count, uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPRX_CUDA_H */
