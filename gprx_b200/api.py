@@ -1,0 +1,564 @@
+"""The gprx model API over the CUDA backend.
+
+Mirrors gprx 0.2.0's public surface for the exact / VFE path
+(src/lib.rs:33-55): `KernelSpec` trees built from `RbfKernel`,
+`RbfArdKernel`, `ConstantKernel`, `PeriodicKernel` with `+` and `*`;
+`GaussianLikelihood`; `Gpr` (trainer) → `FittedGpr` → `OnlineGpr`;
+`Lbfgs` / `Fixed` optimizers; `PredictOptions` / `VarianceKind` /
+`Prediction`; typed `GprError`s (src/error.rs).  Points are column-major
+(`x[i + f*n_rows]`), as in the reference.  Every computation runs in
+libgprx_cuda.so; this module only checks arguments and maps errors.
+"""
+
+import ctypes as C
+import enum
+import math
+
+import numpy as np
+
+from . import _lib as L
+
+
+# ---------------------------------------------------------------------------
+# errors (src/error.rs:308-500)
+# ---------------------------------------------------------------------------
+class GprError(Exception):
+    """Base of every error the backend reports."""
+
+    def __init__(self, message, status=None, info=None):
+        super().__init__(message)
+        self.status = status
+        self.info = info
+
+
+class CholeskyFailed(GprError):
+    """GprError::CholeskyFailed { jitter, matrix_size, stage }."""
+
+    @property
+    def jitter(self):
+        return self.info.jitter
+
+    @property
+    def matrix_size(self):
+        return self.info.matrix_size
+
+    @property
+    def stage(self):
+        return CholeskyStage(self.info.stage)
+
+
+class NonFiniteKernelValue(GprError):
+    pass
+
+
+class ShapeMismatch(GprError):
+    pass
+
+
+class IndexOutOfRange(GprError):
+    pass
+
+
+class InsufficientData(GprError):
+    pass
+
+
+class InvalidHyperparameter(GprError):
+    pass
+
+
+class NonFiniteInput(GprError):
+    pass
+
+
+class EmptyInput(GprError):
+    pass
+
+
+class InvalidConfig(GprError):
+    pass
+
+
+class OptimizationNotConverged(GprError):
+    pass
+
+
+class CudaError(GprError):
+    pass
+
+
+class DeviceTimeout(GprError):
+    pass
+
+
+class OutOfDeviceMemory(GprError):
+    pass
+
+
+_ERRORS = {
+    L.CHOLESKY_FAILED: CholeskyFailed,
+    L.NONFINITE_KERNEL: NonFiniteKernelValue,
+    L.SHAPE_MISMATCH: ShapeMismatch,
+    L.INVALID_POINT_ID: IndexOutOfRange,
+    L.INSUFFICIENT_DATA: InsufficientData,
+    L.CUDA_ERROR: CudaError,
+    L.TIMEOUT: DeviceTimeout,
+    L.INVALID_HYPERPARAMETER: InvalidHyperparameter,
+    L.NONFINITE_INPUT: NonFiniteInput,
+    L.EMPTY_INPUT: EmptyInput,
+    L.OUT_OF_MEMORY: OutOfDeviceMemory,
+    L.INVALID_CONFIG: InvalidConfig,
+    L.NOT_CONVERGED: OptimizationNotConverged,
+    L.INVALID_ARGUMENT: ShapeMismatch,
+    L.CAPACITY: InvalidConfig,
+}
+
+
+def check(status):
+    if status == L.OK:
+        return
+    info = L.last_error()
+    cls = _ERRORS.get(status, GprError)
+    raise cls(info.message.decode(errors="replace") or "status %d" % status, status, info)
+
+
+class CholeskyStage(enum.IntEnum):
+    Fit = 0
+    Predict = 1
+    OnlineInsert = 2
+    OnlineDelete = 3
+
+
+# ---------------------------------------------------------------------------
+# kernels (src/kernel/)
+# ---------------------------------------------------------------------------
+DEFAULT_LO, DEFAULT_HI = 1e-5, 1e5  # Interval::DEFAULT_POSITIVE (src/param.rs:91)
+
+
+def _positive(v, what):
+    v = float(v)
+    if not (math.isfinite(v) and DEFAULT_LO < v < DEFAULT_HI):
+        raise InvalidHyperparameter("%s must be in (1e-5, 1e5), got %r" % (what, v))
+    return v
+
+
+class KernelSpec:
+    """A kernel tree: a leaf, or a Sum / Product of trees (flattened)."""
+
+    def __init__(self, kind, children=(), params=(), dims=0):
+        self.kind = kind
+        self.children = list(children)
+        self._params = list(params)  # log θ of a leaf
+        self.dims = dims
+
+    # tree building -------------------------------------------------------
+    def _flat(self, op):
+        return self.children if self.kind == op else [self]
+
+    def __add__(self, other):
+        return KernelSpec(L.NODE_SUM, self._flat(L.NODE_SUM) + other._flat(L.NODE_SUM))
+
+    def __mul__(self, other):
+        return KernelSpec(L.NODE_PRODUCT, self._flat(L.NODE_PRODUCT) + other._flat(L.NODE_PRODUCT))
+
+    # parameters (log space, depth-first) ------------------------------------
+    def num_params(self):
+        if self.kind in (L.NODE_SUM, L.NODE_PRODUCT):
+            return sum(c.num_params() for c in self.children)
+        return len(self._params)
+
+    def get_params(self):
+        if self.kind in (L.NODE_SUM, L.NODE_PRODUCT):
+            out = []
+            for c in self.children:
+                out += c.get_params()
+            return out
+        return list(self._params)
+
+    def set_params(self, params):
+        params = list(params)
+        if len(params) != self.num_params():
+            raise ShapeMismatch("expected %d parameters, got %d" % (self.num_params(), len(params)))
+        if self.kind in (L.NODE_SUM, L.NODE_PRODUCT):
+            at = 0
+            for c in self.children:
+                k = c.num_params()
+                c.set_params(params[at:at + k])
+                at += k
+        else:
+            for p in params:
+                _positive(math.exp(p), "parameter")
+            self._params = params
+
+    def nodes(self):
+        """Prefix node list for the C ABI."""
+        if self.kind in (L.NODE_SUM, L.NODE_PRODUCT):
+            out = [(self.kind, len(self.children))]
+            for c in self.children:
+                out += c.nodes()
+            return out
+        return [(self.kind, self.dims)]
+
+    def node_array(self):
+        ns = self.nodes()
+        arr = (L.KernelNode * len(ns))()
+        for i, (k, a) in enumerate(ns):
+            arr[i].kind = k
+            arr[i].arg = a
+        return arr, len(ns)
+
+    def input_dim(self):
+        if self.kind == L.LEAF_RBF_ARD:
+            return self.dims
+        for c in self.children:
+            d = c.input_dim()
+            if d:
+                return d
+        return 0
+
+    def copy(self):
+        k = KernelSpec(self.kind, [c.copy() for c in self.children], self._params, self.dims)
+        return k
+
+
+def RbfKernel(lengthscale):
+    """k = exp(−r²/(2ℓ²)) (src/kernel/rbf.rs:18)."""
+    return KernelSpec(L.LEAF_RBF, params=[math.log(_positive(lengthscale, "lengthscale"))])
+
+
+def RbfArdKernel(lengthscales):
+    """k = exp(−½ Σ_f Δ_f²/ℓ_f²) (src/kernel/rbf_ard.rs:16)."""
+    ls = [_positive(v, "lengthscale") for v in lengthscales]
+    if not ls:
+        raise EmptyInput("RbfArdKernel needs at least one lengthscale")
+    return KernelSpec(L.LEAF_RBF_ARD, params=[math.log(v) for v in ls], dims=len(ls))
+
+
+def ConstantKernel(constant):
+    """k = c (src/kernel/constant.rs:12)."""
+    return KernelSpec(L.LEAF_CONSTANT, params=[math.log(_positive(constant, "constant"))])
+
+
+def PeriodicKernel(lengthscale, period):
+    """k = exp(−2 sin²(π r / p)/ℓ²) (src/kernel/periodic.rs:598)."""
+    return KernelSpec(L.LEAF_PERIODIC, params=[math.log(_positive(lengthscale, "lengthscale")),
+                                               math.log(_positive(period, "period"))])
+
+
+class GaussianLikelihood:
+    """θ = log σn² (src/likelihood.rs:72-194)."""
+
+    def __init__(self, noise_variance):
+        self.log_noise_variance = math.log(_positive(noise_variance, "noise variance"))
+
+    @property
+    def noise_variance(self):
+        return math.exp(self.log_noise_variance)
+
+
+# ---------------------------------------------------------------------------
+# optimizers (src/optimizer/)
+# ---------------------------------------------------------------------------
+class Lbfgs:
+    """L-BFGS with the Moré–Thuente line search (src/optimizer/lbfgs.rs:28-172)."""
+
+    def __init__(self, max_iterations=100, tolerance=math.sqrt(2.220446049250313e-16), history_size=10,
+                 restarts=0, seed=0):
+        if not (math.isfinite(tolerance) and tolerance >= 0.0):
+            raise InvalidConfig("L-BFGS gradient tolerance must be finite and >= 0")
+        self.max_iterations = int(max_iterations)
+        self.tolerance = float(tolerance)
+        self.history_size = int(history_size)
+        self.restarts = int(restarts)
+        self.seed = int(seed)
+
+    def with_max_iterations(self, n):
+        self.max_iterations = int(n)
+        return self
+
+    def with_tolerance(self, tol):
+        return Lbfgs(self.max_iterations, tol, self.history_size, self.restarts, self.seed)
+
+    def with_history_size(self, m):
+        self.history_size = int(m)
+        return self
+
+    def with_restarts(self, n, seed):
+        self.restarts = int(n)
+        self.seed = int(seed)
+        return self
+
+    def _c(self):
+        o = L.LbfgsOptions()
+        L.lib().gprx_lbfgs_options_default(C.byref(o))
+        o.max_iterations = self.max_iterations
+        o.tolerance = self.tolerance
+        o.history_size = self.history_size
+        o.restarts = self.restarts
+        o.seed = self.seed
+        return o
+
+
+class Fixed:
+    """No optimization: factor at the given θ (src/optimizer/mod.rs)."""
+
+
+class VarianceKind(enum.IntEnum):
+    Latent = L.VARIANCE_LATENT
+    Observation = L.VARIANCE_OBSERVATION
+
+
+class PredictOptions:
+    def __init__(self, variance_kind=VarianceKind.Observation):
+        self.variance_kind = VarianceKind(variance_kind)
+
+
+class Prediction:
+    """Predictive mean and diagonal variance (src/prediction.rs)."""
+
+    def __init__(self, mean, variance, variance_kind):
+        self.mean = mean
+        self.variance = variance
+        self.variance_kind = variance_kind
+
+
+class Precision(enum.IntEnum):
+    Fp64 = L.PRECISION_FP64
+    Mixed = L.PRECISION_MIXED
+
+
+def _check_points(x, n_rows, n_cols):
+    x = L.f64(x)
+    if n_rows <= 0:
+        raise EmptyInput("no points")
+    if n_cols <= 0:
+        raise EmptyInput("no features")
+    if x.size != n_rows * n_cols:
+        raise ShapeMismatch("x has %d values, expected %d×%d" % (x.size, n_rows, n_cols))
+    if not np.all(np.isfinite(x)):
+        raise NonFiniteInput("non-finite x")
+    return x
+
+
+# ---------------------------------------------------------------------------
+# exact GPR (src/gpr/)
+# ---------------------------------------------------------------------------
+class Gpr:
+    """Exact GPR trainer (src/gpr/trainer.rs:533-613)."""
+
+    def __init__(self, kernel, likelihood, optimizer=None, precision=Precision.Fp64, device=0):
+        self.kernel = kernel
+        self.likelihood = likelihood
+        self.optimizer = optimizer if optimizer is not None else Lbfgs()
+        self.precision = Precision(precision)
+        self.device = device
+        self.jitter = None  # (kind, initial, multiplier, retries, max); None = fixed(0)
+
+    def with_optimizer(self, opt):
+        g = Gpr(self.kernel, self.likelihood, opt, self.precision, self.device)
+        g.jitter = self.jitter
+        return g
+
+    def with_precision(self, precision):
+        g = Gpr(self.kernel, self.likelihood, self.optimizer, precision, self.device)
+        g.jitter = self.jitter
+        return g
+
+    def with_jitter_fixed(self, jitter):
+        self.jitter = (0, float(jitter), 1.0, 0, float(jitter))
+        return self
+
+    def with_jitter_adaptive(self, initial, multiplier, max_retries, max_jitter):
+        self.jitter = (1, float(initial), float(multiplier), int(max_retries), float(max_jitter))
+        return self
+
+    def _options(self):
+        o = L.Options()
+        L.lib().gprx_options_default(C.byref(o))
+        o.precision = int(self.precision)
+        o.device = int(self.device)
+        if self.jitter is not None:
+            o.jitter_kind, o.jitter_initial, o.jitter_multiplier, o.jitter_max_retries, o.jitter_max = self.jitter
+        return o
+
+    def _create(self, x, n_rows, n_cols, y):
+        x = _check_points(x, n_rows, n_cols)
+        y = L.f64(y)
+        if y.size != n_rows:
+            raise ShapeMismatch("y has %d values, expected %d" % (y.size, n_rows))
+        if not np.all(np.isfinite(y)):
+            raise NonFiniteInput("non-finite y")
+        nodes, nn = self.kernel.node_array()
+        theta = L.f64(self.kernel.get_params() + [self.likelihood.log_noise_variance])
+        h = C.c_void_p()
+        opt = self._options()
+        check(L.lib().gprx_exact_create(L.ptr(x), n_rows, n_cols, L.ptr(y), nodes, nn, L.ptr(theta), theta.size,
+                                        C.byref(opt), C.byref(h)))
+        return FittedGpr(h, n_cols, self.kernel.copy())
+
+    def factor(self, x, n_rows, n_cols, y):
+        """Factor at the given θ (Gpr<Fixed>::factor)."""
+        f = self._create(x, n_rows, n_cols, y)
+        check(L.lib().gprx_exact_factor(f._h))
+        return f
+
+    def fit(self, x, n_rows, n_cols, y):
+        """Optimize θ with the trainer's optimizer, then factor at the best θ."""
+        f = self._create(x, n_rows, n_cols, y)
+        if isinstance(self.optimizer, Fixed):
+            check(L.lib().gprx_exact_factor(f._h))
+            return f
+        rep = L.FitReport()
+        opt = self.optimizer._c()
+        check(L.lib().gprx_exact_fit(f._h, C.byref(opt), C.byref(rep)))
+        f.report = rep
+        return f
+
+
+class FittedGpr:
+    """A factored exact GPR (src/gpr/fitted.rs)."""
+
+    def __init__(self, handle, d, kernel):
+        self._h = handle
+        self.d = d
+        self.kernel = kernel
+        self.report = None
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                L.lib().gprx_exact_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+    def num_params(self):
+        return int(L.lib().gprx_exact_num_params(self._h))
+
+    def get_params(self):
+        p = np.zeros(self.num_params())
+        check(L.lib().gprx_exact_get_params(self._h, L.ptr(p), p.size))
+        return p
+
+    def set_params(self, params):
+        p = L.f64(params)
+        check(L.lib().gprx_exact_set_params(self._h, L.ptr(p), p.size))
+
+    def value_and_gradient(self, params):
+        """NLML and its gradient at `params` (ExactFit::value_and_gradient_into)."""
+        p = L.f64(params)
+        if p.size != self.num_params():
+            raise ShapeMismatch("expected %d parameters" % self.num_params())
+        v = np.zeros(1)
+        g = np.zeros(p.size)
+        check(L.lib().gprx_exact_eval(self._h, L.ptr(p), p.size, L.ptr(v), L.ptr(g)))
+        return float(v[0]), g
+
+    def value(self, params):
+        p = L.f64(params)
+        v = np.zeros(1)
+        check(L.lib().gprx_exact_eval(self._h, L.ptr(p), p.size, L.ptr(v), None))
+        return float(v[0])
+
+    def neg_log_marginal_likelihood(self):
+        v = np.zeros(1)
+        check(L.lib().gprx_exact_nlml(self._h, L.ptr(v)))
+        return float(v[0])
+
+    def factor_jitter(self):
+        v = np.zeros(1)
+        check(L.lib().gprx_exact_factor_jitter(self._h, L.ptr(v)))
+        return float(v[0])
+
+    def alpha(self):
+        n = self.n()
+        out = np.zeros(n)
+        check(L.lib().gprx_exact_alpha(self._h, L.ptr(out), n))
+        return out
+
+    def n(self):
+        return int(L.lib().gprx_online_n(self._h))
+
+    def predict(self, xs, n_rows, n_cols):
+        return self.predict_with(xs, n_rows, n_cols, PredictOptions())
+
+    def predict_with(self, xs, n_rows, n_cols, options):
+        if n_cols != self.d:
+            raise ShapeMismatch("query has %d features, model has %d" % (n_cols, self.d))
+        xs = L.f64(xs)
+        if xs.size != n_rows * n_cols:
+            raise ShapeMismatch("xs has %d values, expected %d×%d" % (xs.size, n_rows, n_cols))
+        mean = np.zeros(n_rows)
+        var = np.zeros(n_rows)
+        check(L.lib().gprx_exact_predict(self._h, L.ptr(xs), n_rows, int(options.variance_kind), L.ptr(mean),
+                                         L.ptr(var)))
+        return Prediction(mean, var, options.variance_kind)
+
+    def stage_times_ms(self):
+        out = np.zeros(5)
+        check(L.lib().gprx_exact_stage_times(self._h, L.ptr(out)))
+        return dict(zip(("fill", "factor", "inverse", "gradient", "total"), out))
+
+    def into_online(self):
+        """FittedGpr::into_online (src/gpr/fitted.rs:757-765)."""
+        check(L.lib().gprx_online_begin(self._h))
+        on = OnlineGpr(self._h, self.d, self.kernel)
+        self._h = None
+        return on
+
+
+class OnlineGpr(FittedGpr):
+    """Exact GPR with O(n²) point insert / delete (src/gpr/online.rs)."""
+
+    def insert(self, x_new, y_new):
+        x = L.f64(x_new)
+        if x.size != self.d:
+            raise ShapeMismatch("point has %d features, model has %d" % (x.size, self.d))
+        pid = C.c_uint64(0)
+        check(L.lib().gprx_online_insert(self._h, L.ptr(x), float(y_new), C.byref(pid)))
+        return int(pid.value)
+
+    def delete(self, point_id):
+        check(L.lib().gprx_online_delete(self._h, int(point_id)))
+
+    def point_ids(self):
+        n = self.n()
+        out = np.zeros(n, dtype=np.uint64)
+        check(L.lib().gprx_online_point_ids(self._h, out.ctypes.data_as(L.U64), n))
+        return out
+
+
+# ---------------------------------------------------------------------------
+# seeded RNG (src/rng.rs)
+# ---------------------------------------------------------------------------
+class SeededRng:
+    """Xoshiro256++ seeded by SplitMix64, the reference's generator."""
+
+    def __init__(self, seed):
+        self._r = L.Rng()
+        L.lib().gprx_rng_seed(C.byref(self._r), int(seed))
+
+    def next_u64(self):
+        return int(L.lib().gprx_rng_next_u64(C.byref(self._r)))
+
+    def unit(self, count=None):
+        if count is None:
+            return float(L.lib().gprx_rng_unit(C.byref(self._r)))
+        out = np.zeros(int(count))
+        L.lib().gprx_rng_fill_unit(C.byref(self._r), L.ptr(out), out.size)
+        return out
+
+    def normal(self, count=None):
+        if count is None:
+            return float(L.lib().gprx_rng_normal(C.byref(self._r)))
+        out = np.zeros(int(count))
+        L.lib().gprx_rng_fill_normal(C.byref(self._r), L.ptr(out), out.size)
+        return out
+
+    def up_to(self, max_value):
+        return int(L.lib().gprx_rng_up_to(C.byref(self._r), int(max_value)))
+
+    def subset(self, n, count):
+        out = np.zeros(int(count), dtype=np.uint64)
+        check(L.lib().gprx_rng_subset(C.byref(self._r), int(n), int(count), out.ctypes.data_as(L.U64)))
+        return out

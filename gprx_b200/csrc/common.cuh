@@ -1,0 +1,225 @@
+// common.cuh — shared device infrastructure of the gprx B200 backend.
+//
+//  * DevStatus: the device-side status word every kernel of a pipeline reads
+//    first and writes on failure (non-positive pivot, non-finite kernel value,
+//    bounded wait that ran out).  Kernels never trap; the host reads the word
+//    after the stream drains and maps it onto a gprx_status.
+//  * KTree: a KernelSpec tree (src/kernel/spec.rs:106) in sum-of-products
+//    form, evaluated per matrix entry with static register indexing.
+//  * launch bookkeeping (gprx_launch_count).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/gprx_cuda.h"
+
+namespace gprx {
+
+// ---------------------------------------------------------------------------
+// status word
+// ---------------------------------------------------------------------------
+struct DevStatus {
+  int code;       // GPRX_OK or a gprx_status
+  int stage;      // GPRX_STAGE_* for CHOLESKY_FAILED
+  long long info; // failing row / index
+};
+
+__device__ __forceinline__ bool dev_failed(const DevStatus* st) {
+  return st != nullptr && *(volatile const int*)&st->code != GPRX_OK;
+}
+
+__device__ __forceinline__ void dev_fail(DevStatus* st, int code, long long info) {
+  if (st == nullptr) return;
+  if (atomicCAS(&st->code, GPRX_OK, code) == GPRX_OK) {
+    st->info = info;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launch accounting
+// ---------------------------------------------------------------------------
+void count_launch(int k = 1);
+uint64_t launches();
+
+#define GPRX_LAUNCH(kernel, grid, block, smem, stream, ...)            \
+  do {                                                                 \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);        \
+    ::gprx::count_launch();                                            \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// kernel tree in sum-of-products form
+// ---------------------------------------------------------------------------
+constexpr int KT_MAX_LEAVES = 8;
+constexpr int KT_MAX_TERMS = 8;
+constexpr int KT_ACC_PER_LEAF = 2;  // ∂/∂ of a non-ARD leaf: ≤ 2 parameters
+
+struct KLeaf {
+  int kind;      // GPRX_LEAF_*
+  int param;     // first θ index
+  double c0;     // RBF: 1/(2ℓ²); CONSTANT: c; PERIODIC: π/p
+  double c1;     // PERIODIC: 1/ℓ²
+};
+
+struct KTree {
+  int n_leaves;
+  int n_terms;
+  int n_params;               // kernel parameters
+  int d;
+  int ard_leaf;               // index of the single RBF_ARD leaf, or -1
+  int ard_param;              // its first θ index
+  unsigned term_mask[KT_MAX_TERMS];
+  KLeaf leaf[KT_MAX_LEAVES];
+  double inv_ell2[GPRX_MAX_DIM];  // ARD 1/ℓ_f²
+  double diag_value;          // k(x, x) (stationary: the same for every x)
+};
+
+// Leaf values at one pair.  dx[f] = x1_f − x2_f.
+template <int ARD_D>
+__device__ __forceinline__ void kt_leaf_values(const KTree& t, const double* dx, double r2,
+                                               double (&v)[KT_MAX_LEAVES], double& ard_q) {
+  ard_q = 0.0;
+  if (ARD_D > 0) {
+#pragma unroll
+    for (int f = 0; f < ARD_D; ++f) {
+      if (f < t.d) ard_q = fma(dx[f] * dx[f], t.inv_ell2[f], ard_q);
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < KT_MAX_LEAVES; ++l) {
+    if (l >= t.n_leaves) { v[l] = 0.0; continue; }
+    const KLeaf& lf = t.leaf[l];
+    double val;
+    switch (lf.kind) {
+      case GPRX_LEAF_CONSTANT: val = lf.c0; break;
+      case GPRX_LEAF_RBF: val = exp(-r2 * lf.c0); break;
+      case GPRX_LEAF_RBF_ARD: val = exp(-0.5 * ard_q); break;
+      case GPRX_LEAF_PERIODIC: {
+        double s = sin(lf.c0 * sqrt(fmax(r2, 0.0)));
+        val = exp(-2.0 * s * s * lf.c1);
+        break;
+      }
+      default: val = 0.0;
+    }
+    v[l] = val;
+  }
+}
+
+__device__ __forceinline__ double kt_combine(const KTree& t, const double (&v)[KT_MAX_LEAVES]) {
+  double k = 0.0;
+#pragma unroll
+  for (int tt = 0; tt < KT_MAX_TERMS; ++tt) {
+    if (tt >= t.n_terms) break;
+    double p = 1.0;
+#pragma unroll
+    for (int l = 0; l < KT_MAX_LEAVES; ++l)
+      if ((t.term_mask[tt] >> l) & 1u) p *= v[l];
+    k += p;
+  }
+  return k;
+}
+
+// k(x1, x2).  x1/x2 are feature-0 pointers with strides s1/s2.
+template <int ARD_D>
+__device__ __forceinline__ double kt_value(const KTree& t, const double* dx, double r2) {
+  double v[KT_MAX_LEAVES];
+  double q;
+  kt_leaf_values<ARD_D>(t, dx, r2, v, q);
+  return kt_combine(t, v);
+}
+
+// Accumulates w · ∂k/∂θ into per-leaf slots (acc_leaf[l][0..1]) and per-dim ARD
+// slots (acc_ard[f]); the host maps slots to θ indices.  A Sum gives each term
+// the same weight; a Product gives a factor the weight times the other factors
+// (src/kernel/compiled/weighted.rs:274-345).
+template <int ARD_D>
+__device__ __forceinline__ void kt_accumulate_grad(const KTree& t, const double* dx, double r2, double w,
+                                                   double (&acc_leaf)[KT_MAX_LEAVES][KT_ACC_PER_LEAF],
+                                                   double (&acc_ard)[ARD_D > 0 ? ARD_D : 1]) {
+  double v[KT_MAX_LEAVES];
+  double q;
+  kt_leaf_values<ARD_D>(t, dx, r2, v, q);
+  double adj[KT_MAX_LEAVES];
+#pragma unroll
+  for (int l = 0; l < KT_MAX_LEAVES; ++l) adj[l] = 0.0;
+#pragma unroll
+  for (int tt = 0; tt < KT_MAX_TERMS; ++tt) {
+    if (tt >= t.n_terms) break;
+    unsigned mask = t.term_mask[tt];
+#pragma unroll
+    for (int l = 0; l < KT_MAX_LEAVES; ++l) {
+      if (!((mask >> l) & 1u)) continue;
+      double others = 1.0;
+#pragma unroll
+      for (int o = 0; o < KT_MAX_LEAVES; ++o)
+        if (o != l && ((mask >> o) & 1u)) others *= v[o];
+      adj[l] += others;
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < KT_MAX_LEAVES; ++l) {
+    if (l >= t.n_leaves) break;
+    const KLeaf& lf = t.leaf[l];
+    double wa = w * adj[l];
+    switch (lf.kind) {
+      case GPRX_LEAF_CONSTANT: acc_leaf[l][0] = fma(wa, lf.c0, acc_leaf[l][0]); break;
+      case GPRX_LEAF_RBF: acc_leaf[l][0] = fma(wa * v[l], 2.0 * lf.c0 * r2, acc_leaf[l][0]); break;
+      case GPRX_LEAF_RBF_ARD:
+        if (ARD_D > 0) {
+          double wv = wa * v[l];
+#pragma unroll
+          for (int f = 0; f < (ARD_D > 0 ? ARD_D : 1); ++f)
+            if (f < t.d) acc_ard[f] = fma(wv, dx[f] * dx[f] * t.inv_ell2[f], acc_ard[f]);
+        }
+        break;
+      case GPRX_LEAF_PERIODIC: {
+        double a = lf.c0 * sqrt(fmax(r2, 0.0));
+        double s, c;
+        sincos(a, &s, &c);
+        double wv = wa * v[l] * 4.0 * lf.c1 * s;
+        acc_leaf[l][0] = fma(wv, s, acc_leaf[l][0]);
+        acc_leaf[l][1] = fma(wv, c * a, acc_leaf[l][1]);
+        break;
+      }
+      default: break;
+    }
+  }
+}
+
+// Number of accumulator slots and the θ index of each (host side).
+int kt_num_slots(int ard_d);
+
+// ---------------------------------------------------------------------------
+// small device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum; `red` holds ≥ 32 doubles of shared memory.  All threads get
+// the result.  Fixed order: deterministic for a fixed block size.
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int nw = (blockDim.x + 31) >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (warp == 0) {
+    s = lane < nw ? red[lane] : 0.0;
+    s = warp_sum(s);
+    if (lane == 0) red[0] = s;
+  }
+  __syncthreads();
+  s = red[0];
+  __syncthreads();
+  return s;
+}
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace gprx

@@ -1,0 +1,65 @@
+// dense_f64.cuh — blocked FP64 dense kernels and drivers (host API).
+#pragma once
+
+#include "common.cuh"
+#include "gemm_f64.cuh"
+
+namespace gprx {
+
+// Panel width of the blocked factor / inverse / solves.  The in-place GEMM
+// steps need it ≤ the 128-wide GEMM tile.
+constexpr int NB = 128;
+
+// C = alpha·opA·opB + beta·C with the 128×128 DMMA tile (see gemm_f64.cuh).
+cudaError_t dgemm(bool ta, bool tb, const GemmParams& p, cudaStream_t s, int batch = 1);
+
+// Small helper building GemmParams.
+GemmParams gemm_params(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
+                       double* C, long long ldc, double alpha, double beta, const DevStatus* st);
+
+// In-place lower Cholesky of A (n×n, ld) by right-looking blocks of NB.
+// linv receives the inverse of every diagonal block (ceil(n/NB) blocks of
+// NB×NB, column-major, ld NB).  A non-positive pivot sets st (CHOLESKY_FAILED,
+// info = global row) and every later kernel of the stream returns at once.
+cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatus* st, cudaStream_t s);
+
+// Inverses of the diagonal NB-blocks of a lower triangle (unit: unit diagonal).
+cudaError_t tri_inv_blocks(const double* L, long long ld, int n, bool unit, double* linv, DevStatus* st,
+                           cudaStream_t s);
+
+// X = L⁻¹ into X (n×n, ldx; zero above the diagonal), from L and its diagonal
+// block inverses.
+cudaError_t trtri_blocked(const double* L, long long ld, int n, const double* linv, double* X, long long ldx,
+                          DevStatus* st, cudaStream_t s);
+
+// C (lower) = Xᵀ X for lower-triangular X: K⁻¹ from X = L⁻¹.
+cudaError_t lauum_lower(const double* X, long long ldx, int n, double* C, long long ldc, DevStatus* st,
+                        cudaStream_t s);
+
+// B (n×q, ldb) := L⁻¹ B   /   := L⁻ᵀ B, with L's diagonal block inverses.
+cudaError_t trsm_lower(const double* L, long long ld, int n, const double* linv, double* B, long long ldb, int q,
+                       DevStatus* st, cudaStream_t s);
+cudaError_t trsm_lower_t(const double* L, long long ld, int n, const double* linv, double* B, long long ldb, int q,
+                         DevStatus* st, cudaStream_t s);
+
+// out = log|det L|² contribution: 2 Σ ln L_ii (lower LLT) or Σ ln D_i (ldlt=true).
+cudaError_t logdet_diag(const double* L, long long ld, int n, bool ldlt, double* out, DevStatus* st,
+                        cudaStream_t s);
+
+// z = X y for lower-triangular X (n×n, ld).
+cudaError_t trmv_lower(const double* X, long long ld, int n, const double* y, double* z, DevStatus* st,
+                       cudaStream_t s);
+// out_j = Σ_{i ≥ (lower ? j : 0)} M(i,j) v_i  for j < ncols (one warp per column).
+cudaError_t gemv_t(const double* M, long long ld, int nrows, int ncols, bool lower, const double* v, double* out,
+                   DevStatus* st, cudaStream_t s);
+// out_j = Σ_i M(i,j)² (/ w_i when w != nullptr) for j < ncols.
+cudaError_t col_sumsq(const double* M, long long ld, int nrows, int ncols, const double* w, double* out,
+                      DevStatus* st, cudaStream_t s);
+
+// out = Σ_i a_i b_i (single block, deterministic).
+cudaError_t dot_dev(const double* a, const double* b, int n, double* out, DevStatus* st, cudaStream_t s);
+
+// Sets X (n×n, ld) to the identity (full columns, zero off the diagonal).
+cudaError_t set_identity(double* X, long long ld, int n, cudaStream_t s);
+
+}  // namespace gprx

@@ -1,0 +1,357 @@
+// exact.cu — exact-GPR objective, factor and prediction on the device.
+//
+// One evaluation (gprx ExactFit::value_and_gradient_into_fit,
+// src/gpr/exact_fit.rs:319-341) is enqueued on the handle's stream as
+//   fill  K + (σn² + j) I                      (factor.rs:515-542)
+//   potrf L                                    (chol.rs:141-167)
+//   logdet 2 Σ ln L_ii                          (factor.rs:555-568)
+//   trtri X = L⁻¹, α = Xᵀ (X y), yᵀα
+//   lauum K⁻¹ = Xᵀ X                            (workspace.rs:395-425)
+//   contraction −½⟨ααᵀ − K⁻¹, ∂K/∂θ⟩, noise −½σn² Σ W_ii (exact_fit.rs:665-729)
+// and drained with one synchronisation.  A non-positive pivot stops every
+// later kernel through the device status word; the host then retries with the
+// next jitter offset (retry_with_jitter, chol.rs:35-58) or restores the
+// previous θ and its factor (exact_fit.rs:196-206).
+
+#include <algorithm>
+#include <cmath>
+
+#include "exact.cuh"
+
+namespace gprx {
+
+ExactState::~ExactState() {
+  if (stream) cudaStreamSynchronize(stream);
+  for (auto& e : ev)
+    if (e) cudaEventDestroy(e);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+static bool in_default_interval(double log_v) {
+  // Interval::DEFAULT_POSITIVE = (1e-5, 1e5), open (src/param.rs:91)
+  double v = std::exp(log_v);
+  return std::isfinite(v) && v > 1e-5 && v < 1e5;
+}
+
+gprx_status ExactState::create(const double* xh, uint64_t nn, uint64_t dd, const double* yh,
+                               const gprx_kernel_node* nodes, int n_nodes, const double* theta, int n_theta,
+                               const gprx_options* o) {
+  if (!xh || !yh || !nodes || (!theta && n_theta > 0)) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (nn == 0) return set_error(GPRX_EMPTY_INPUT, "no training points");
+  if (dd == 0) return set_error(GPRX_EMPTY_INPUT, "no features (d = 0)");
+  if (nn > (uint64_t)INT32_MAX / 2) return set_error(GPRX_CAPACITY, "n too large");
+  if (!all_finite(xh, nn * dd) || !all_finite(yh, nn)) return set_error(GPRX_NONFINITE_INPUT, "non-finite input");
+  if (o) opt = *o;
+  else gprx_options_default(&opt);
+  std::string why;
+  // θ for the kernel comes first, then log σn²
+  if (n_theta < 1) return set_error(GPRX_SHAPE_MISMATCH, "theta must hold the kernel parameters and log noise");
+  gprx_status st = kern.init(nodes, n_nodes, theta, n_theta - 1, (int)dd, &why);
+  if (st != GPRX_OK) return set_error(st, why);
+  for (int i = 0; i < n_theta; ++i)
+    if (!in_default_interval(theta[i]))
+      return set_error(GPRX_INVALID_HYPERPARAMETER, "hyperparameter outside (1e-5, 1e5)");
+  log_noise = theta[n_theta - 1];
+  n = (int)nn;
+  d = (int)dd;
+  cap = n;
+  ld = round_ld(cap);
+  device = opt.device;
+  GPRX_CUDA_TRY(cudaSetDevice(device));
+  GPRX_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  for (auto& e : ev) GPRX_CUDA_TRY(cudaEventCreate(&e));
+  int nblk = ceil_div(cap, NB);
+  if (x.alloc((size_t)cap * d) != cudaSuccess || y.alloc(cap) != cudaSuccess ||
+      A.alloc((size_t)ld * cap) != cudaSuccess || linv.alloc((size_t)nblk * NB * NB) != cudaSuccess ||
+      alpha.alloc(cap) != cudaSuccess || z.alloc(cap) != cudaSuccess || tmpv.alloc(cap) != cudaSuccess ||
+      partials.alloc((size_t)grad_max_blocks() * 64) != cudaSuccess || slot_param.alloc(64) != cudaSuccess ||
+      res.alloc(64) != cudaSuccess || status.alloc(1) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "device allocation failed");
+  GPRX_CUDA_TRY(res_h.ensure(64));
+  GPRX_CUDA_TRY(status_h.ensure(1));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(x.p, xh, sizeof(double) * n * d, cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(y.p, yh, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+  std::vector<int> sp(64, -1);
+  std::copy(kern.slot_param.begin(), kern.slot_param.end(), sp.begin());
+  GPRX_CUDA_TRY(cudaMemcpyAsync(slot_param.p, sp.data(), sizeof(int) * 64, cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(cudaMemsetAsync(status.p, 0, sizeof(DevStatus), stream));
+  GPRX_CUDA_TRY(cudaStreamSynchronize(stream));
+  y_host.assign(yh, yh + n);
+  for (int i = 0; i < n; ++i) ids.push_back(next_id++);
+  return GPRX_OK;
+}
+
+void ExactState::get_params(double* out) const {
+  for (int i = 0; i < kern.n_params; ++i) out[i] = kern.theta[i];
+  out[kern.n_params] = log_noise;
+}
+
+gprx_status ExactState::write_params(const double* params) {
+  int p = num_params();
+  for (int i = 0; i < p; ++i)
+    if (!in_default_interval(params[i]))
+      return set_error(GPRX_INVALID_HYPERPARAMETER, "hyperparameter outside (1e-5, 1e5)");
+  gprx_status st = kern.set_theta(params);
+  if (st != GPRX_OK) return set_error(st, "invalid kernel hyperparameter");
+  log_noise = params[p - 1];
+  factor_ok = false;
+  alpha_ok = false;
+  return GPRX_OK;
+}
+
+gprx_status ExactState::reset_status() {
+  GPRX_CUDA_TRY(cudaMemsetAsync(status.p, 0, sizeof(DevStatus), stream));
+  return GPRX_OK;
+}
+
+gprx_status ExactState::read_status(DevStatus* out) {
+  GPRX_CUDA_TRY(cudaMemcpyAsync(status_h.p, status.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+  GPRX_CUDA_TRY(cudaStreamSynchronize(stream));
+  *out = *status_h.p;
+  return GPRX_OK;
+}
+
+gprx_status ExactState::enqueue_factor(double j) {
+  GPRX_CUDA_TRY(cudaEventRecord(ev[0], stream));
+  GPRX_CUDA_TRY(fill_lower(kern, x.p, n, A.p, ld, noise() + j, status.p, stream));
+  GPRX_CUDA_TRY(cudaEventRecord(ev[1], stream));
+  GPRX_CUDA_TRY(potrf_blocked(A.p, ld, n, linv.p, status.p, stream));
+  GPRX_CUDA_TRY(cudaEventRecord(ev[2], stream));
+  return GPRX_OK;
+}
+
+// JitterPolicy retry offsets after the first attempt (src/policy.rs:306-397).
+static std::vector<double> retry_list(const gprx_options& o) {
+  std::vector<double> out;
+  if (o.jitter_kind == GPRX_JITTER_FIXED) {
+    if (o.jitter_initial > 0.0) out.push_back(o.jitter_initial);
+    return out;
+  }
+  double j = o.jitter_initial;
+  for (int r = 0; r < o.jitter_max_retries; ++r) {
+    if (!(j <= o.jitter_max)) break;
+    out.push_back(j);
+    double g = j * o.jitter_multiplier;
+    if (!std::isfinite(g)) break;
+    j = g;
+  }
+  return out;
+}
+
+gprx_status ExactState::factor_with_retries(int stage) {
+  std::vector<double> js{0.0};
+  auto r = retry_list(opt);
+  js.insert(js.end(), r.begin(), r.end());
+  double last = 0.0;
+  for (double j : js) {
+    last = j;
+    gprx_status st = reset_status();
+    if (st != GPRX_OK) return st;
+    st = enqueue_factor(j);
+    if (st != GPRX_OK) return st;
+    DevStatus ds;
+    st = read_status(&ds);
+    if (st != GPRX_OK) return st;
+    if (ds.code == GPRX_OK) {
+      jitter = j;
+      factor_ok = true;
+      linv_ok = true;
+      online = false;
+      return GPRX_OK;
+    }
+    if (ds.code != GPRX_CHOLESKY_FAILED) return status_to_error(ds, j, n, stage);
+  }
+  factor_ok = false;
+  return set_cholesky_error(last, n, stage);
+}
+
+gprx_status ExactState::solve_alpha_from_l() {
+  GPRX_CUDA_TRY(cudaMemcpyAsync(alpha.p, y.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+  GPRX_CUDA_TRY(trsm_lower(A.p, ld, n, linv.p, alpha.p, n, 1, status.p, stream));
+  GPRX_CUDA_TRY(trsm_lower_t(A.p, ld, n, linv.p, alpha.p, n, 1, status.p, stream));
+  alpha_ok = true;
+  return GPRX_OK;
+}
+
+gprx_status ExactState::factor_current() {
+  gprx_status st = factor_with_retries(GPRX_STAGE_FIT);
+  if (st != GPRX_OK) return st;
+  st = solve_alpha_from_l();
+  if (st != GPRX_OK) return st;
+  DevStatus ds;
+  st = read_status(&ds);
+  if (st != GPRX_OK) return st;
+  if (ds.code != GPRX_OK) return status_to_error(ds, jitter, n, GPRX_STAGE_FIT);
+  return GPRX_OK;
+}
+
+gprx_status ExactState::eval(const double* params, double* nlml_out, double* grad) {
+  const int p = num_params();
+  std::vector<double> prev(p);
+  get_params(prev.data());
+  gprx_status st = write_params(params);
+  if (st != GPRX_OK) return st;
+  if (online) return set_error(GPRX_INVALID_CONFIG, "an online model takes no hyperparameter evaluation");
+  std::vector<double> js{0.0};
+  auto r = retry_list(opt);
+  js.insert(js.end(), r.begin(), r.end());
+  double last = 0.0;
+  const size_t nn = (size_t)ld * cap;
+  if (grad && Xinv.n < nn) {
+    if (Xinv.alloc(nn) != cudaSuccess) {
+      write_params(prev.data());
+      return set_error(GPRX_OUT_OF_MEMORY, "device allocation of the inverse failed");
+    }
+  }
+  for (double j : js) {
+    last = j;
+    if ((st = reset_status()) != GPRX_OK) return st;
+    if ((st = enqueue_factor(j)) != GPRX_OK) return st;
+    GPRX_CUDA_TRY(logdet_diag(A.p, ld, n, false, res.p + 0, status.p, stream));
+    if (grad) {
+      GPRX_CUDA_TRY(trtri_blocked(A.p, ld, n, linv.p, Xinv.p, ld, status.p, stream));
+      GPRX_CUDA_TRY(trmv_lower(Xinv.p, ld, n, y.p, z.p, status.p, stream));
+      GPRX_CUDA_TRY(gemv_t(Xinv.p, ld, n, n, true, z.p, alpha.p, status.p, stream));
+      GPRX_CUDA_TRY(dot_dev(y.p, alpha.p, n, res.p + 1, status.p, stream));
+      GPRX_CUDA_TRY(lauum_lower(Xinv.p, ld, n, A.p, ld, status.p, stream));
+      GPRX_CUDA_TRY(cudaEventRecord(ev[3], stream));
+      int blocks = 0;
+      GPRX_CUDA_TRY(grad_contract(kern, x.p, n, A.p, ld, alpha.p, partials.p, &blocks, status.p, stream));
+      GPRX_CUDA_TRY(grad_finalize(kern, partials.p, blocks, slot_param.p, noise(), res.p + 2, status.p, stream));
+      GPRX_CUDA_TRY(cudaEventRecord(ev[4], stream));
+    } else {
+      GPRX_CUDA_TRY(cudaMemcpyAsync(alpha.p, y.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+      GPRX_CUDA_TRY(trsm_lower(A.p, ld, n, linv.p, alpha.p, n, 1, status.p, stream));
+      GPRX_CUDA_TRY(trsm_lower_t(A.p, ld, n, linv.p, alpha.p, n, 1, status.p, stream));
+      GPRX_CUDA_TRY(dot_dev(y.p, alpha.p, n, res.p + 1, status.p, stream));
+      GPRX_CUDA_TRY(cudaEventRecord(ev[3], stream));
+      GPRX_CUDA_TRY(cudaEventRecord(ev[4], stream));
+    }
+    GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p, sizeof(double) * (2 + p), cudaMemcpyDeviceToHost, stream));
+    DevStatus ds;
+    if ((st = read_status(&ds)) != GPRX_OK) return st;
+    ev_recorded = true;
+    if (ds.code == GPRX_OK) {
+      jitter = j;
+      factor_ok = grad == nullptr;  // the gradient overwrote L with K⁻¹
+      linv_ok = factor_ok;
+      alpha_ok = true;
+      online = false;
+      double logdet = res_h.p[0], quad = res_h.p[1];
+      *nlml_out = 0.5 * (quad + logdet + (double)n * std::log(2.0 * M_PI));
+      if (grad)
+        for (int i = 0; i < p; ++i) grad[i] = res_h.p[2 + i];
+      if (!std::isfinite(*nlml_out)) return set_error(GPRX_NOT_CONVERGED, "non-finite NLML");
+      return GPRX_OK;
+    }
+    if (ds.code != GPRX_CHOLESKY_FAILED) {
+      gprx_status e = status_to_error(ds, j, n, GPRX_STAGE_FIT);
+      write_params(prev.data());
+      factor_current();
+      return set_error(e, last_error().message);
+    }
+  }
+  // every offset failed: restore θ and its factor (exact_fit.rs:196-206)
+  write_params(prev.data());
+  factor_current();
+  return set_cholesky_error(last, n, GPRX_STAGE_FIT);
+}
+
+gprx_status ExactState::nlml(double* out) {
+  gprx_status st;
+  if (online) {
+    if (!alpha_ok && (st = online_alpha()) != GPRX_OK) return st;
+  } else if (!factor_ok || !alpha_ok) {
+    if ((st = factor_current()) != GPRX_OK) return st;
+  }
+  if ((st = reset_status()) != GPRX_OK) return st;
+  GPRX_CUDA_TRY(logdet_diag(A.p, ld, n, online, res.p + 0, status.p, stream));
+  GPRX_CUDA_TRY(dot_dev(y.p, alpha.p, n, res.p + 1, status.p, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+  DevStatus ds;
+  if ((st = read_status(&ds)) != GPRX_OK) return st;
+  if (ds.code != GPRX_OK) return status_to_error(ds, jitter, n, GPRX_STAGE_FIT);
+  *out = 0.5 * (res_h.p[1] + res_h.p[0] + (double)n * std::log(2.0 * M_PI));
+  return GPRX_OK;
+}
+
+// var = max(0, k** − quad) (+ σn² for observation variance); shared.rs:792-806
+__global__ void finish_var_kernel(const double* quad, int q, double kss, double noise, int kind, double* var,
+                                  const DevStatus* st) {
+  if (dev_failed(st)) return;
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= q) return;
+  double lat = kss - quad[j];
+  if (lat < 0.0) lat = 0.0;
+  var[j] = kind == GPRX_VARIANCE_OBSERVATION ? lat + noise : lat;
+}
+
+__global__ void extract_diag_kernel(const double* A, long long ld, int n, double* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = A[i + (long long)i * ld];
+}
+
+gprx_status ExactState::predict(const double* xs, uint64_t q, int kind, double* mean, double* var) {
+  if (!xs || !mean || !var) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (kind != GPRX_VARIANCE_LATENT && kind != GPRX_VARIANCE_OBSERVATION)
+    return set_error(GPRX_INVALID_ARGUMENT, "variance kind");
+  if (q == 0) return GPRX_OK;
+  if (!all_finite(xs, q * d)) return set_error(GPRX_NONFINITE_INPUT, "non-finite query");
+  gprx_status st;
+  if (online) {
+    if (!alpha_ok && (st = online_alpha()) != GPRX_OK) return st;
+    if (!linv_ok) {
+      if ((st = reset_status()) != GPRX_OK) return st;
+      GPRX_CUDA_TRY(tri_inv_blocks(A.p, ld, n, true, linv.p, status.p, stream));
+      linv_ok = true;
+    }
+    GPRX_CUDA_TRY(cudaMemsetAsync(status.p, 0, sizeof(DevStatus), stream));
+    extract_diag_kernel<<<ceil_div(n, 256), 256, 0, stream>>>(A.p, ld, n, tmpv.p);
+    count_launch();
+  } else if (!factor_ok || !alpha_ok) {
+    if ((st = factor_current()) != GPRX_OK) return st;
+  }
+  const int qc_max = (int)std::max<long long>(1, std::min<long long>((long long)q, (1LL << 27) / std::max(n, 1)));
+  if (qbuf.ensure((size_t)ld * qc_max) != cudaSuccess || qx.ensure((size_t)qc_max * (d + 3)) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "predict scratch");
+  HostPinned<double> hm;
+  GPRX_CUDA_TRY(hm.ensure(2 * (size_t)qc_max));
+  const double kss = kern.diag_value();
+  for (uint64_t c0 = 0; c0 < q; c0 += qc_max) {
+    int qc = (int)std::min<uint64_t>(qc_max, q - c0);
+    double* xq = qx.p;                  // qc × d
+    double* mdev = qx.p + (size_t)qc_max * d;
+    double* vdev = mdev + qc_max;
+    double* quad = vdev + qc_max;
+    GPRX_CUDA_TRY(cudaMemcpy2DAsync(xq, sizeof(double) * qc, xs + c0, sizeof(double) * q, sizeof(double) * qc, d,
+                                    cudaMemcpyHostToDevice, stream));
+    GPRX_CUDA_TRY(fill_cross(kern, x.p, cap, n, xq, qc, qc, qbuf.p, ld, status.p, stream));
+    GPRX_CUDA_TRY(gemv_t(qbuf.p, ld, n, qc, false, alpha.p, mdev, status.p, stream));
+    GPRX_CUDA_TRY(trsm_lower(A.p, ld, n, linv.p, qbuf.p, ld, qc, status.p, stream));
+    GPRX_CUDA_TRY(col_sumsq(qbuf.p, ld, n, qc, online ? tmpv.p : nullptr, quad, status.p, stream));
+    finish_var_kernel<<<ceil_div(qc, 256), 256, 0, stream>>>(quad, qc, kss, noise(), kind, vdev, status.p);
+    count_launch();
+    GPRX_CUDA_TRY(cudaMemcpyAsync(hm.p, mdev, sizeof(double) * qc, cudaMemcpyDeviceToHost, stream));
+    GPRX_CUDA_TRY(cudaMemcpyAsync(hm.p + qc_max, vdev, sizeof(double) * qc, cudaMemcpyDeviceToHost, stream));
+    DevStatus ds;
+    if ((st = read_status(&ds)) != GPRX_OK) return st;
+    if (ds.code != GPRX_OK) return status_to_error(ds, jitter, n, GPRX_STAGE_PREDICT);
+    std::copy(hm.p, hm.p + qc, mean + c0);
+    std::copy(hm.p + qc_max, hm.p + qc_max + qc, var + c0);
+  }
+  return GPRX_OK;
+}
+
+gprx_status ExactState::stage_times(double* out5) {
+  if (!ev_recorded) return set_error(GPRX_INVALID_CONFIG, "no evaluation recorded");
+  float ms;
+  for (int i = 0; i < 4; ++i) {
+    GPRX_CUDA_TRY(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+    out5[i] = ms;
+  }
+  GPRX_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[4]));
+  out5[4] = ms;
+  return GPRX_OK;
+}
+
+}  // namespace gprx

@@ -1,0 +1,86 @@
+// exact.cuh — the exact-GPR handle (device state of one Gpr / FittedGpr /
+// OnlineGpr).
+#pragma once
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "dense_f64.cuh"
+#include "kernels.cuh"
+#include "runtime.cuh"
+
+struct gprx_exact;
+
+namespace gprx {
+
+struct ExactState {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int n = 0, d = 0;
+  long long ld = 0;        // leading dimension of the n×n buffers
+  int cap = 0;             // online capacity (rows/cols the buffers hold)
+  gprx_options opt{};
+  HostKernel kern;
+  double log_noise = 0.0;
+  std::vector<double> y_host;  // y in buffer order (online compaction)
+
+  DevBuf<double> x;        // cap×d (column-major, ld = cap)
+  DevBuf<double> y;        // cap
+  DevBuf<double> A;        // ld×cap: K → L (→ K⁻¹ after a gradient; → LDLT online)
+  DevBuf<double> Xinv;     // ld×cap: L⁻¹ (gradient path)
+  DevBuf<double> linv;     // diagonal-block inverses
+  DevBuf<double> alpha, z, tmpv;
+  DevBuf<double> partials;
+  DevBuf<int> slot_param;
+  DevBuf<double> res;      // [0] logdet, [1] yᵀα, [2..] grad
+  DevBuf<DevStatus> status;
+  HostPinned<double> res_h;
+  HostPinned<DevStatus> status_h;
+  DevBuf<double> qbuf, qx;  // predict scratch
+
+  bool factor_ok = false;   // A holds L (LLT) of the current θ
+  bool alpha_ok = false;
+  bool online = false;      // A holds LDLT
+  bool linv_ok = false;     // linv matches A's diagonal blocks
+  double jitter = 0.0;
+  std::vector<uint64_t> ids;
+  uint64_t next_id = 0;
+
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool ev_recorded = false;
+
+  ~ExactState();
+  gprx_status create(const double* x, uint64_t n, uint64_t d, const double* y, const gprx_kernel_node* nodes,
+                     int n_nodes, const double* theta, int n_theta, const gprx_options* o);
+  int num_params() const { return kern.n_params + 1; }
+  void get_params(double* out) const;
+  gprx_status write_params(const double* params);
+  double noise() const { return std::exp(log_noise); }
+
+  // Enqueues fill + potrf for one jitter attempt.
+  gprx_status enqueue_factor(double j);
+  // fill + potrf with the jitter retries; syncs; on success A holds L.
+  gprx_status factor_with_retries(int stage);
+  gprx_status solve_alpha_from_l();
+  gprx_status factor_current();
+  gprx_status eval(const double* params, double* nlml, double* grad);
+  gprx_status nlml(double* out);
+  gprx_status predict(const double* xs, uint64_t q, int kind, double* mean, double* var);
+  gprx_status reset_status();
+  gprx_status read_status(DevStatus* out);
+  gprx_status stage_times(double* out5);
+
+  // online (LDLT)
+  gprx_status online_begin();
+  gprx_status online_insert(const double* xnew, double ynew, uint64_t* id);
+  gprx_status online_delete(uint64_t id);
+  gprx_status online_alpha();
+  gprx_status grow(int needed);
+};
+
+}  // namespace gprx
+
+struct gprx_exact {
+  gprx::ExactState s;
+};
