@@ -1,0 +1,327 @@
+"""Benchmark: exact-GPR NLML + gradient evaluations per second at n = 8192.
+
+Workload (the reference's exact objective, config "Exact Gpr,
+ConstantKernel(2.0) * RbfArdKernel d = 8, n = 8192"): x ~ N(0, I₈), the eight
+lengthscales log-uniform in [0.3, 3], c = 2, σn² = 0.05², y a draw from the
+GP prior at those hyperparameters plus N(0, 0.05²) noise.  One step is one
+NLML + gradient evaluation at a hyperparameter vector perturbed by N(0, 0.1²)
+in log space (100 perturbations, cycled).  All data are synthetic, from the
+restated SeededRng; no dataset is read.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl ours|reference]
+
+N > 1 runs N independent replicas (one exact problem does not shard; launched
+by torchrun, one rank per GPU); `value` is the aggregate evals/s over ranks,
+timed as the maximum over ranks.  `--impl reference` times the CPU
+restatement of the reference's algorithm (oracle/) on the host cores.
+"""
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 8192
+D = 8
+NOISE = 0.05 ** 2
+CONST = 2.0
+
+
+def synth(n, d, seed=0):
+    """x, y, true θ for the C2 workload (seeded Xoshiro256++)."""
+    import gprx_b200 as gx
+
+    rng = gx.SeededRng(seed)
+    x = rng.normal(n * d)                      # column-major n×d, N(0, 1)
+    u = rng.unit(d)
+    ls = np.exp(math.log(0.3) + u * (math.log(3.0) - math.log(0.3)))
+    xm = x.reshape(d, n).T
+    z = xm / ls
+    sq = np.sum(z * z, axis=1)
+    k = CONST * np.exp(-0.5 * np.maximum(sq[:, None] + sq[None, :] - 2.0 * (z @ z.T), 0.0))
+    k[np.diag_indices(n)] = CONST + NOISE
+    chol = np.linalg.cholesky(k)
+    y = chol @ rng.normal(n)                   # prior draw plus noise (the NOISE on the diagonal)
+    theta = np.array([math.log(CONST)] + list(np.log(ls)) + [math.log(NOISE)])
+    return x, y, theta
+
+
+def perturbations(theta, count=100, seed=1):
+    import gprx_b200 as gx
+
+    rng = gx.SeededRng(seed)
+    return [theta + 0.1 * rng.normal(theta.size) for _ in range(count)]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh)
+    return {}
+
+
+def fp64_peak_tflops(torch, dev):
+    """cuBLAS DGEMM throughput on this GPU (the FP64 denominator; measured
+    here because the driver's peak file has no FP64 figure)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh)
+    return None
+
+
+def cpu_reference(n, d, x, y, thetas, steps, warmup, budget_s=6.0):
+    """Times the oracle (a CPU restatement of the reference's algorithm)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    lib = O.lib()
+    cores = int(lib.orc_num_threads())
+    nodes = [[2, 2], [12, 0], [11, d]]
+    # a step is one full evaluation at n when it fits the budget, else one
+    # evaluation at n/2 scaled by 8 (the evaluation is O(n³)).
+    t0 = time.perf_counter()
+    O.exact_eval(nodes, thetas[0], x, n, d, y)
+    t_full = time.perf_counter() - t0
+    if t_full <= budget_s:
+        ns, scale, xs, ys = n, 1.0, x, y
+    else:
+        ns = n // 2
+        xs = x.reshape(d, n)[:, :ns].reshape(-1).copy()
+        ys = y[:ns].copy()
+        scale = (n / ns) ** 3
+    for i in range(warmup):
+        O.exact_eval(nodes, thetas[i % len(thetas)], xs, ns, d, ys)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        O.exact_eval(nodes, thetas[i % len(thetas)], xs, ns, d, ys)
+    dt = (time.perf_counter() - t0) / steps * scale
+    sample = ("one NLML+gradient evaluation per step at n=%d" % ns) + (
+        "" if scale == 1.0 else ", time scaled by (%d/%d)^3 to n=%d" % (n, ns, n))
+    return 1.0 / dt, dt, cores, sample
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    n, d = args.n, D
+    warm = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    workload = "exact_gpr_nlml_grad_n%d_d%d_const_rbfard" % (n, d)
+    config = {"workload": workload, "n": n, "d": d, "kernel": "ConstantKernel(2.0) * RbfArdKernel(d=8)",
+              "noise_variance": NOISE, "perturbations": "100 θ + N(0, 0.1²) in log space, cycled",
+              "l2": "inputs larger than L2 (two n×n FP64 buffers of %d MiB each)" % (n * n * 8 // 2 ** 20),
+              "parallelism": "replicas" if args.gpus > 1 else "single"}
+    metric = "NLML+grad evals/s n=%d (%s)" % (n, "FP64" if args.precision == "fp64" else "mixed")
+
+    x, y, theta = synth(n, d)
+    thetas = perturbations(theta)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        value, dt, cores, sample = cpu_reference(n, d, x, y, thetas, args.steps, args.warmup)
+        line = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config, "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import gprx_b200 as gx
+    from gprx_b200 import _lib as L
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    spec = gx.ConstantKernel(CONST) * gx.RbfArdKernel(list(np.exp(theta[1:1 + d])))
+    prec = gx.Precision.Fp64 if args.precision == "fp64" else gx.Precision.Mixed
+    model = gx.Gpr(spec, gx.GaussianLikelihood(NOISE), precision=prec, device=local) \
+        .with_optimizer(gx.Fixed()).factor(x, n, d, y)
+    stream = torch.cuda.ExternalStream(model.stream_ptr(), device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident timing (value) ----
+    for i in range(warm):
+        model.value_and_gradient(thetas[i % len(thetas)])
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = L.lib().gprx_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stage = np.zeros(5)
+    for i in range(args.steps):
+        model.value_and_gradient(thetas[i % len(thetas)])
+        st = model.stage_times_ms()
+        stage += np.array([st["fill"], st["factor"], st["inverse"], st["gradient"], st["total"]])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = int(L.lib().gprx_launch_count() - l0)
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    barrier()
+    ms_max = ms
+    if dist is not None:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = args.steps * world / (ms_max * 1e-3)
+    stage /= args.steps
+
+    # ---- end to end through the public API with host buffers ----
+    xh = torch.from_numpy(x).pin_memory().numpy()
+    yh = torch.from_numpy(y).pin_memory().numpy()
+    p = theta.size
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        model.set_data(xh, yh)
+        model.value_and_gradient(thetas[i % len(thetas)])
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": args.steps * world / e2e_s, "unit": "evals/s",
+           "h2d_bytes_per_step": int((n * d + n + p) * 8), "d2h_bytes_per_step": int((1 + p) * 8)}
+
+    # ---- roofline: the DMMA-driven stages (factor + inverse), n³ flops ----
+    peaks = measured_peaks()
+    fp64_peak = fp64_peak_tflops(torch, dev) if rank == 0 else None
+    dmma_ms = stage[1] + stage[2]
+    achieved = (n ** 3) / (dmma_ms * 1e-3) / 1e12
+    traffic = load_traffic()
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak if fp64_peak else None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)",
+                "kernel": "dgemm_kernel (DMMA m16n8k4 f64) inside potrf/trtri/lauum",
+                "work": "n^3 flops per evaluation (potrf n^3/3 + trtri n^3/3 + lauum n^3/3)",
+                "traffic": traffic.get("bytes_per_eval") if traffic else None,
+                "stage_ms": {"fill": stage[0], "factor": stage[1], "inverse": stage[2], "gradient": stage[3],
+                             "total": stage[4]}}
+
+    line = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": warm, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config, "e2e": e2e,
+            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
+            "bf16_peak_reference": peaks.get("bf16_tflops")}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, dt, cores, sample = cpu_reference(n, d, x, y, thetas, steps=1, warmup=0, budget_s=30.0)
+        line["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del model
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

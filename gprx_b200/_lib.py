@@ -98,11 +98,14 @@ _SIGS = {
     "gprx_exact_alpha": (C.c_int32, [C.c_void_p, D, C.c_uint64]),
     "gprx_exact_fit": (C.c_int32, [C.c_void_p, C.POINTER(LbfgsOptions), C.POINTER(FitReport)]),
     "gprx_exact_stage_times": (C.c_int32, [C.c_void_p, D]),
+    "gprx_exact_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "gprx_online_begin": (C.c_int32, [C.c_void_p]),
     "gprx_online_insert": (C.c_int32, [C.c_void_p, D, C.c_double, U64]),
     "gprx_online_delete": (C.c_int32, [C.c_void_p, C.c_uint64]),
     "gprx_online_n": (C.c_uint64, [C.c_void_p]),
     "gprx_online_point_ids": (C.c_int32, [C.c_void_p, U64, C.c_uint64]),
+    "gprx_probe_dgemm": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
+    "gprx_probe_potrf": (C.c_int32, [C.c_int32, C.c_int32, D]),
     "gprx_rng_seed": (None, [C.POINTER(Rng), C.c_uint64]),
     "gprx_rng_next_u64": (C.c_uint64, [C.POINTER(Rng)]),
     "gprx_rng_unit": (C.c_double, [C.POINTER(Rng)]),

@@ -494,6 +494,18 @@ class FittedGpr:
                                          L.ptr(var)))
         return Prediction(mean, var, options.variance_kind)
 
+    def stream_ptr(self):
+        """The cudaStream_t this model's kernels run on (for event timing)."""
+        s = C.c_void_p()
+        check(L.lib().gprx_exact_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def set_data(self, x, y):
+        """Re-uploads X and y of the same shape (gprx_exact_set_data)."""
+        x = L.f64(x)
+        y = L.f64(y)
+        check(L.lib().gprx_exact_set_data(self._h, L.ptr(x), L.ptr(y)))
+
     def stage_times_ms(self):
         out = np.zeros(5)
         check(L.lib().gprx_exact_stage_times(self._h, L.ptr(out)))

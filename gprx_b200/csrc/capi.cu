@@ -346,6 +346,13 @@ gprx_status gprx_exact_stage_times(gprx_exact* h, double* out5) {
   return h->s.stage_times(out5);
 }
 
+gprx_status gprx_exact_stream(gprx_exact* h, void** stream) {
+  CHECK_HANDLE(h);
+  if (!stream) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  *stream = (void*)h->s.stream;
+  return GPRX_OK;
+}
+
 gprx_status gprx_online_begin(gprx_exact* h) {
   CHECK_HANDLE(h);
   return h->s.online_begin();

@@ -111,24 +111,200 @@ __device__ void blk_store_full(double* dst, int ldd, const double* s, int ls, in
   }
 }
 
-__global__ void __launch_bounds__(DIAG_THREADS) potrf_diag_kernel(double* A, long long lda, long long k0, int nb,
-                                                                   double* linv, DevStatus* st) {
-  extern __shared__ double s[];
-  if (dev_failed(st)) return;
-  const int ls = nb + 1;
-  double* tmp = s + nb * ls;
-  blk_load_lower(s, ls, A, lda, k0, nb);
-  int f = blk_potf2(s, ls, nb);
-  if (f >= 0) {
-    if (threadIdx.x == 0) dev_fail(st, GPRX_CHOLESKY_FAILED, k0 + f);
+// ---------------------------------------------------------------------------
+// Fast diagonal block (nb ≤ 128): LLT by 32-column sub-panels and the block's
+// inverse, all in shared memory.
+//   per sub-panel p:  one warp factors the 32×32 diagonal sub-block in
+//                     registers (lane = row, pivots broadcast by shuffles) and
+//                     inverts it (lane = column);
+//                     all warps: P = A_below · L_pp⁻ᵀ, then A22 −= P Pᵀ.
+//   inverse:          column blocks right to left from X L = I:
+//                     X_ij = −(Σ_{k=j+1..i} X_ik L_kj) X_jj, in place.
+// ---------------------------------------------------------------------------
+constexpr int FD_THREADS = 512;
+constexpr int SB = 32;         // sub-panel width
+constexpr int SBL = SB + 1;    // ld of a 32×32 scratch block
+
+__device__ __forceinline__ void warp_factor_inv(double* s, int ls, int c0, int w, double* xd, int* fail) {
+  // lane r holds row r of the diagonal sub-block (columns ≤ r)
+  const int lane = threadIdx.x & 31;
+  double d[SB];
+#pragma unroll
+  for (int c = 0; c < SB; ++c) d[c] = (lane < w && c <= lane) ? s[(c0 + lane) + (c0 + c) * ls] : 0.0;
+  int bad = -1;
+#pragma unroll
+  for (int j = 0; j < SB; ++j) {
+    if (j < w && bad < 0) {
+      double piv = __shfl_sync(0xffffffffu, d[j], j);
+      if (!(piv > 0.0)) {
+        bad = j;
+      } else {
+        double ljj = sqrt(piv);
+        if (lane == j) d[j] = ljj;
+        else if (lane > j) d[j] = d[j] / ljj;
+#pragma unroll
+        for (int c = j + 1; c < SB; ++c) {
+          double lcj = __shfl_sync(0xffffffffu, d[j], c);
+          if (lane >= c) d[c] = fma(-d[j], lcj, d[c]);
+        }
+      }
+    }
+  }
+  if (bad >= 0) {
+    if (lane == 0) *fail = c0 + bad;
     return;
   }
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+  if (lane < w) {
+#pragma unroll
+    for (int c = 0; c < SB; ++c)
+      if (c <= lane) s[(c0 + lane) + (c0 + c) * ls] = d[c];
+  }
+  __syncwarp();
+  // inverse of the sub-block: lane c computes column c
+  if (lane < w) {
+    const int c = lane;
+    for (int r = 0; r < c; ++r) xd[r + c * SBL] = 0.0;
+    xd[c + c * SBL] = 1.0 / s[(c0 + c) + (c0 + c) * ls];
+    for (int r = c + 1; r < w; ++r) {
+      double acc = 0.0;
+      for (int t = c; t < r; ++t) acc = fma(s[(c0 + r) + (c0 + t) * ls], xd[t + c * SBL], acc);
+      xd[r + c * SBL] = -acc / s[(c0 + r) + (c0 + r) * ls];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long long lda, long long k0, int nb,
+                                                                 double* linv, DevStatus* st) {
+  extern __shared__ double smem[];
+  __shared__ int fail;
+  if (dev_failed(st)) return;
+  const int ls = nb + 1;
+  double* s = smem;                       // nb × ls
+  double* xd = s + nb * ls;               // 4 × (32 × 33) diagonal sub-block inverses
+  double* tmp = xd + 4 * SB * SBL;        // 3 × (32 × 33)
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) fail = -1;
+  for (int e = tid; e < nb * nb; e += nt) {
+    int i = e % nb, j = e / nb;
+    s[i + j * ls] = (i >= j) ? A[(k0 + i) + (k0 + j) * lda] : 0.0;
+  }
+  __syncthreads();
+  const int np = (nb + SB - 1) / SB;
+  for (int p = 0; p < np; ++p) {
+    const int c0 = p * SB, w = min(SB, nb - c0);
+    if (tid < 32) warp_factor_inv(s, ls, c0, w, xd + p * SB * SBL, &fail);
+    __syncthreads();
+    if (fail >= 0) {
+      if (tid == 0) dev_fail(st, GPRX_CHOLESKY_FAILED, k0 + fail);
+      return;
+    }
+    const int r0 = c0 + w, cnt = nb - r0;
+    if (cnt <= 0) break;
+    // P = A_below · X_ppᵀ  (P(r, c) = Σ_{t ≤ c} A(r, t) X(c, t))
+    const double* X = xd + p * SB * SBL;
+    const int items = cnt * (SB / 4);  // ≤ 96 · 8 = 768 ≤ 2 · FD_THREADS
+    // each thread: up to two items, results held until all reads finish
+    double res0[4] = {0, 0, 0, 0}, res1[4] = {0, 0, 0, 0};
+    auto item = [&](int it, double (&acc)[4]) {
+      int r = r0 + it % cnt, cg = (it / cnt) * 4;
+      for (int t = 0; t < w; ++t) {
+        double a = s[r + (c0 + t) * ls];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] = fma(a, X[(cg + q) + t * SBL], acc[q]);
+      }
+    };
+    auto put = [&](int it, const double (&acc)[4]) {
+      int r = r0 + it % cnt, cg = (it / cnt) * 4;
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (cg + q < w) s[r + (c0 + cg + q) * ls] = acc[q];
+    };
+    if (tid < items) item(tid, res0);
+    if (tid + nt < items) item(tid + nt, res1);
+    __syncthreads();
+    if (tid < items) put(tid, res0);
+    if (tid + nt < items) put(tid + nt, res1);
+    __syncthreads();
+    // A22 −= P Pᵀ over 4×4 blocks of the lower triangle
+    const int nb4 = (cnt + 3) / 4;
+    const int nblk = nb4 * (nb4 + 1) / 2;
+    for (int b = tid; b < nblk; b += nt) {
+      int bi = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+      while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
+      while (bi * (bi + 1) / 2 > b) --bi;
+      int bj = b - bi * (bi + 1) / 2;
+      int i0 = r0 + bi * 4, j0 = r0 + bj * 4;
+      double a4[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) a4[u][v] = 0.0;
+      for (int t = 0; t < w; ++t) {
+        double pi[4], pj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          pi[u] = (i0 + u < nb) ? s[(i0 + u) + (c0 + t) * ls] : 0.0;
+          pj[u] = (j0 + u < nb) ? s[(j0 + u) + (c0 + t) * ls] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) a4[u][v] = fma(pi[u], pj[v], a4[u][v]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          int i = i0 + u, j = j0 + v;
+          if (i < nb && j < nb && i >= j) s[i + j * ls] -= a4[u][v];
+        }
+    }
+    __syncthreads();
+  }
+  // L back to global
+  for (int e = tid; e < nb * nb; e += nt) {
     int i = e % nb, j = e / nb;
     if (i >= j) A[(k0 + i) + (k0 + j) * lda] = s[i + j * ls];
   }
   __syncthreads();
-  blk_trti2(s, ls, nb, false, tmp);
+  // block inverse in place, column blocks right to left
+  for (int jb = np - 1; jb >= 0; --jb) {
+    const int j0 = jb * SB, wj = min(SB, nb - j0);
+    const double* Xjj = xd + jb * SB * SBL;
+    // T_ib = Σ_{k=jb+1..ib} X_ik L_kj  for ib > jb (X_ik already in s for k > jb)
+    const int nout = np - 1 - jb;
+    for (int e = tid; e < nout * SB * SB; e += nt) {
+      int ib = jb + 1 + e / (SB * SB);
+      int rr = (e % (SB * SB)) % SB, cc = (e % (SB * SB)) / SB;
+      int i = ib * SB + rr, j = j0 + cc;
+      double acc = 0.0;
+      if (i < nb && cc < wj) {
+        // X (columns > jb, including the inverted diagonal blocks, zero above
+        // their diagonals) is already in s; column block jb still holds L.
+        const int kend = min(nb, (ib + 1) * SB);
+        for (int k = (jb + 1) * SB; k < kend; ++k) acc = fma(s[i + k * ls], s[k + j * ls], acc);
+      }
+      tmp[(ib - jb - 1) * SB * SBL + rr + cc * SBL] = acc;
+    }
+    __syncthreads();
+    // X_ib,jb = −T X_jj ; then X_jj onto the diagonal block
+    for (int e = tid; e < nout * SB * SB; e += nt) {
+      int ib = jb + 1 + e / (SB * SB);
+      int rr = (e % (SB * SB)) % SB, cc = (e % (SB * SB)) / SB;
+      int i = ib * SB + rr, j = j0 + cc;
+      if (i < nb && cc < wj) {
+        const double* T = tmp + (ib - jb - 1) * SB * SBL;
+        double acc = 0.0;
+        for (int k = cc; k < wj; ++k) acc = fma(T[rr + k * SBL], Xjj[k + cc * SBL], acc);
+        s[i + j * ls] = -acc;
+      }
+    }
+    for (int e = tid; e < SB * SB; e += nt) {
+      int rr = e % SB, cc = e / SB;
+      if (rr < wj && cc < wj) s[(j0 + rr) + (j0 + cc) * ls] = (rr >= cc) ? Xjj[rr + cc * SBL] : 0.0;
+    }
+    __syncthreads();
+  }
   blk_store_full(linv, NB, s, ls, nb);
 }
 
@@ -146,12 +322,13 @@ __global__ void __launch_bounds__(DIAG_THREADS) tri_inv_blocks_kernel(const doub
 }
 
 static size_t diag_smem(int nb) { return (size_t)(nb * (nb + 1) + nb) * sizeof(double); }
+static size_t fast_diag_smem(int nb) { return (size_t)(nb * (nb + 1) + 7 * SB * SBL) * sizeof(double); }
 
 static cudaError_t diag_attrs() {
   static bool done = false;
   if (done) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(potrf_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)diag_smem(NB));
+                                       (int)fast_diag_smem(NB));
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(tri_inv_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem(NB));
   if (e != cudaSuccess) return e;
@@ -170,7 +347,7 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
   for (int k0 = 0; k0 < n; k0 += NB) {
     int nbk = min(NB, n - k0);
     double* lk = linv + (long long)(k0 / NB) * NB * NB;
-    GPRX_LAUNCH(potrf_diag_kernel, 1, DIAG_THREADS, diag_smem(nbk), s, A, ld, (long long)k0, nbk, lk, st);
+    GPRX_LAUNCH(potrf_diag_kernel, 1, FD_THREADS, fast_diag_smem(nbk), s, A, ld, (long long)k0, nbk, lk, st);
     int rest = n - k0 - nbk;
     if (rest <= 0) break;
     double* P = A + (k0 + nbk) + (long long)k0 * ld;

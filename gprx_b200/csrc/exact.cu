@@ -216,8 +216,9 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
       GPRX_CUDA_TRY(lauum_lower(Xinv.p, ld, n, A.p, ld, status.p, stream));
       GPRX_CUDA_TRY(cudaEventRecord(ev[3], stream));
       int blocks = 0;
-      GPRX_CUDA_TRY(grad_contract(kern, x.p, n, A.p, ld, alpha.p, partials.p, &blocks, status.p, stream));
-      GPRX_CUDA_TRY(grad_finalize(kern, partials.p, blocks, slot_param.p, noise(), res.p + 2, status.p, stream));
+      GPRX_CUDA_TRY(grad_contract(kern, x.p, cap, n, A.p, ld, alpha.p, partials.p, &blocks, status.p, stream));
+      GPRX_CUDA_TRY(grad_finalize(kern, partials.p, blocks, slot_param.p, -0.5, -0.5 * noise(), res.p + 2,
+                                  status.p, stream));
       GPRX_CUDA_TRY(cudaEventRecord(ev[4], stream));
     } else {
       GPRX_CUDA_TRY(cudaMemcpyAsync(alpha.p, y.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));

@@ -354,8 +354,29 @@ constexpr int GRAD_MAX_BLOCKS = 148 * 4;
 
 int grad_max_blocks() { return GRAD_MAX_BLOCKS; }
 
+// Writes one block's slot sums (warp shuffles, then warps in a fixed order).
+template <int NS>
+__device__ __forceinline__ void store_slots(double (&vals)[NS], double (*red)[NS], double* out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    double v = warp_sum(vals[s]);
+    if (lane == 0) red[warp][s] = v;
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < NS; s += blockDim.x) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][s];
+    out[s] = v;
+  }
+}
+
+// Lower-triangle contraction Σ_{i≥j} c_ij W_ij ∂K_ij/∂θ (c = 1 diagonal, 2 off).
+// With alpha: W_ij = α_i α_j − M_ij (the exact-GPR weight, M = K⁻¹) and the
+// last slot collects Σ W_ii; without: W_ij = M_ij.
 template <int ARD_D>
-__global__ void __launch_bounds__(GRAD_THREADS) grad_contract_kernel(KTree t, const double* x, int n,
+__global__ void __launch_bounds__(GRAD_THREADS) grad_contract_kernel(KTree t, const double* x, long long ldx, int n,
                                                                      const double* kinv, long long ld,
                                                                      const double* alpha, double* partials,
                                                                      const DevStatus* st) {
@@ -367,6 +388,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) grad_contract_kernel(KTree t, co
   __shared__ double red[GRAD_THREADS / 32][NS];
   if (dev_failed(st)) return;
   const int d = t.d;
+  const bool amode = alpha != nullptr;
   double acc_leaf[KT_MAX_LEAVES][KT_ACC_PER_LEAF];
   double acc_ard[AD];
   double acc_noise = 0.0;
@@ -384,10 +406,10 @@ __global__ void __launch_bounds__(GRAD_THREADS) grad_contract_kernel(KTree t, co
     __syncthreads();
     for (int e = threadIdx.x; e < d * FT; e += blockDim.x) {
       int r = e % FT, f = e / FT;
-      xi[f * FT + r] = (i0 + r < n) ? x[(i0 + r) + (long long)f * n] : 0.0;
-      xj[f * FT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * n] : 0.0;
+      xi[f * FT + r] = (i0 + r < n) ? x[(i0 + r) + (long long)f * ldx] : 0.0;
+      xj[f * FT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * ldx] : 0.0;
     }
-    if (threadIdx.x < FT) {
+    if (amode && threadIdx.x < FT) {
       int r = threadIdx.x;
       ai[r] = (i0 + r < n) ? alpha[i0 + r] : 0.0;
       aj[r] = (j0 + r < n) ? alpha[j0 + r] : 0.0;
@@ -398,7 +420,8 @@ __global__ void __launch_bounds__(GRAD_THREADS) grad_contract_kernel(KTree t, co
     for (int c = threadIdx.x / FT; c < FT; c += GRAD_THREADS / FT) {
       int j = j0 + c;
       if (i >= n || j >= n || i < j) continue;
-      double w = fma(ai[r], aj[c], -kinv[i + (long long)j * ld]);
+      double m = kinv[i + (long long)j * ld];
+      double w = amode ? fma(ai[r], aj[c], -m) : m;
       double cw = (i == j) ? w : 2.0 * w;
       if (i == j) acc_noise += w;
       double dx[AD];
@@ -415,34 +438,84 @@ __global__ void __launch_bounds__(GRAD_THREADS) grad_contract_kernel(KTree t, co
       kt_accumulate_grad<ARD_D>(t, dx, r2, cw, acc_leaf, acc_ard);
     }
   }
-  // reduce: warp shuffles, then across warps in fixed order
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __syncthreads();
+  double vals[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
-    double v;
-    if (s < GRAD_SLOTS_LEAF) v = acc_leaf[s / 2][s % 2];
-    else if (s < GRAD_SLOTS_LEAF + AD) v = acc_ard[s - GRAD_SLOTS_LEAF];
-    else v = acc_noise;
-    v = warp_sum(v);
-    if (lane == 0) red[warp][s] = v;
+    if (s < GRAD_SLOTS_LEAF) vals[s] = acc_leaf[s / 2][s % 2];
+    else if (s < GRAD_SLOTS_LEAF + AD) vals[s] = acc_ard[s - GRAD_SLOTS_LEAF];
+    else vals[s] = acc_noise;
   }
-  __syncthreads();
-  for (int s = threadIdx.x; s < NS; s += blockDim.x) {
-    double v = 0.0;
-    for (int w = 0; w < GRAD_THREADS / 32; ++w) v += red[w][s];
-    partials[(long long)blockIdx.x * NS + s] = v;
-  }
+  store_slots<NS>(vals, red, partials + (long long)blockIdx.x * NS);
 }
 
-cudaError_t grad_contract(const HostKernel& k, const double* x, int n, const double* kinv, long long ld,
+// Rectangle contraction Σ_{i,c} W_ic ∂k(z_i, x_c)/∂θ (W is m×n, ldw).
+template <int ARD_D>
+__global__ void __launch_bounds__(GRAD_THREADS) cross_contract_kernel(KTree t, const double* z, long long ldz, int m,
+                                                                      const double* x, long long ldx, int n,
+                                                                      const double* W, long long ldw, double* partials,
+                                                                      const DevStatus* st) {
+  constexpr int AD = ARD_D > 0 ? ARD_D : 1;
+  constexpr int NS = GRAD_SLOTS_LEAF + AD + 1;
+  __shared__ double xi[GPRX_MAX_DIM * FT];
+  __shared__ double xj[GPRX_MAX_DIM * FT];
+  __shared__ double red[GRAD_THREADS / 32][NS];
+  if (dev_failed(st)) return;
+  const int d = t.d;
+  double acc_leaf[KT_MAX_LEAVES][KT_ACC_PER_LEAF];
+  double acc_ard[AD];
+#pragma unroll
+  for (int l = 0; l < KT_MAX_LEAVES; ++l) acc_leaf[l][0] = acc_leaf[l][1] = 0.0;
+#pragma unroll
+  for (int f = 0; f < AD; ++f) acc_ard[f] = 0.0;
+  const int tm = (m + FT - 1) / FT, tn = (n + FT - 1) / FT;
+  const long long ntiles = (long long)tm * tn;
+  for (long long idx = blockIdx.x; idx < ntiles; idx += gridDim.x) {
+    const int i0 = (int)(idx % tm) * FT, j0 = (int)(idx / tm) * FT;
+    __syncthreads();
+    for (int e = threadIdx.x; e < d * FT; e += blockDim.x) {
+      int r = e % FT, f = e / FT;
+      xi[f * FT + r] = (i0 + r < m) ? z[(i0 + r) + (long long)f * ldz] : 0.0;
+      xj[f * FT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * ldx] : 0.0;
+    }
+    __syncthreads();
+    const int r = threadIdx.x % FT;
+    const int i = i0 + r;
+    for (int c = threadIdx.x / FT; c < FT; c += GRAD_THREADS / FT) {
+      int j = j0 + c;
+      if (i >= m || j >= n) continue;
+      double w = W[i + (long long)j * ldw];
+      double dx[AD];
+      double r2 = 0.0;
+      for (int f = 0; f < d; ++f) {
+        double v = xi[f * FT + r] - xj[f * FT + c];
+        r2 = fma(v, v, r2);
+        if (ARD_D > 0) {
+#pragma unroll
+          for (int g = 0; g < AD; ++g)
+            if (g == f) dx[g] = v;
+        }
+      }
+      kt_accumulate_grad<ARD_D>(t, dx, r2, w, acc_leaf, acc_ard);
+    }
+  }
+  double vals[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    if (s < GRAD_SLOTS_LEAF) vals[s] = acc_leaf[s / 2][s % 2];
+    else if (s < GRAD_SLOTS_LEAF + AD) vals[s] = acc_ard[s - GRAD_SLOTS_LEAF];
+    else vals[s] = 0.0;
+  }
+  store_slots<NS>(vals, red, partials + (long long)blockIdx.x * NS);
+}
+
+cudaError_t grad_contract(const HostKernel& k, const double* x, long long ldx, int n, const double* kinv, long long ld,
                           const double* alpha, double* partials, int* blocks_out, DevStatus* st, cudaStream_t s) {
   int nt = (n + FT - 1) / FT;
   long long ntiles = (long long)nt * (nt + 1) / 2;
   int grid = (int)std::max<long long>(1, std::min<long long>(ntiles, GRAD_MAX_BLOCKS));
   *blocks_out = grid;
 #define GPRX_GRAD(D) \
-  GPRX_LAUNCH(grad_contract_kernel<D>, grid, GRAD_THREADS, 0, s, k.tree, x, n, kinv, ld, alpha, partials, st)
+  GPRX_LAUNCH(grad_contract_kernel<D>, grid, GRAD_THREADS, 0, s, k.tree, x, ldx, n, kinv, ld, alpha, partials, st)
   switch (k.ard_d) {
     case 0: GPRX_GRAD(0); break;
     case 4: GPRX_GRAD(4); break;
@@ -454,8 +527,29 @@ cudaError_t grad_contract(const HostKernel& k, const double* x, int n, const dou
   return cudaGetLastError();
 }
 
+cudaError_t cross_contract(const HostKernel& k, const double* z, long long ldz, int m, const double* x, long long ldx,
+                           int n, const double* W, long long ldw, double* partials, int* blocks_out, DevStatus* st,
+                           cudaStream_t s) {
+  long long ntiles = (long long)((m + FT - 1) / FT) * ((n + FT - 1) / FT);
+  int grid = (int)std::max<long long>(1, std::min<long long>(ntiles, GRAD_MAX_BLOCKS));
+  *blocks_out = grid;
+#define GPRX_CC(D)                                                                                                  \
+  GPRX_LAUNCH(cross_contract_kernel<D>, grid, GRAD_THREADS, 0, s, k.tree, z, ldz, m, x, ldx, n, W, ldw, partials, \
+              st)
+  switch (k.ard_d) {
+    case 0: GPRX_CC(0); break;
+    case 4: GPRX_CC(4); break;
+    case 8: GPRX_CC(8); break;
+    case 16: GPRX_CC(16); break;
+    default: GPRX_CC(32); break;
+  }
+#undef GPRX_CC
+  return cudaGetLastError();
+}
+
+// grad[p] = scale · Σ_slots(p); grad[n_kernel] = noise_coef · Σ (last slot).
 __global__ void grad_finalize_kernel(const double* partials, int blocks, int ns, const int* slot_param, int n_kernel,
-                                     double noise, double* grad, const DevStatus* st) {
+                                     double scale, double noise_coef, double* grad, const DevStatus* st) {
   __shared__ double tot[64];
   if (dev_failed(st)) return;
   for (int s = threadIdx.x; s < ns; s += blockDim.x) {
@@ -470,15 +564,16 @@ __global__ void grad_finalize_kernel(const double* partials, int blocks, int ns,
       int p = slot_param[s];
       if (p >= 0) grad[p] += tot[s];
     }
-    for (int p = 0; p < n_kernel; ++p) grad[p] *= -0.5;
-    grad[n_kernel] = -0.5 * noise * tot[ns - 1];
+    for (int p = 0; p < n_kernel; ++p) grad[p] *= scale;
+    grad[n_kernel] = noise_coef * tot[ns - 1];
   }
 }
 
 cudaError_t grad_finalize(const HostKernel& k, const double* partials, int blocks, const int* slot_param_dev,
-                          double noise, double* grad, DevStatus* st, cudaStream_t s) {
+                          double scale, double noise_coef, double* grad, DevStatus* st, cudaStream_t s) {
   int ns = grad_slots(k.ard_d);
-  GPRX_LAUNCH(grad_finalize_kernel, 1, 64, 0, s, partials, blocks, ns, slot_param_dev, k.n_params, noise, grad, st);
+  GPRX_LAUNCH(grad_finalize_kernel, 1, 64, 0, s, partials, blocks, ns, slot_param_dev, k.n_params, scale,
+              noise_coef, grad, st);
   return cudaGetLastError();
 }
 

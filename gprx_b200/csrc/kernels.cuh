@@ -38,14 +38,19 @@ cudaError_t fill_lower(const HostKernel& k, const double* x, int n, double* K, l
 cudaError_t fill_cross(const HostKernel& k, const double* x1, long long ldx1, int n1, const double* x2,
                        long long ldx2, int n2, double* out, long long ld, DevStatus* st, cudaStream_t s);
 
-// Partial sums of Σ_{i≥j} c_ij · ∂K_ij/∂θ (c = 1 on the diagonal, 2 off it) with
-// weights W_ij = α_i α_j − Kinv_ij (Kinv lower in ld), plus the diagonal Σ W_ii.
-// Writes `blocks × grad_slots(ard_d)` partials; returns the block count.
-cudaError_t grad_contract(const HostKernel& k, const double* x, int n, const double* kinv, long long ld,
+// Partial sums of Σ_{i≥j} c_ij · W_ij · ∂K_ij/∂θ (c = 1 on the diagonal, 2 off
+// it).  With alpha: W_ij = α_i α_j − M_ij (M = K⁻¹ lower in ld) and the last
+// slot collects Σ W_ii; with alpha == nullptr: W_ij = M_ij.  x is n×d with
+// leading dimension ldx.  Writes `blocks × grad_slots(ard_d)` partials.
+cudaError_t grad_contract(const HostKernel& k, const double* x, long long ldx, int n, const double* kinv, long long ld,
                           const double* alpha, double* partials, int* blocks_out, DevStatus* st, cudaStream_t s);
-// grad[p] (p = n_params + 1 values): −½ (slot sums mapped to θ), noise −½ σn² Σ W_ii.
+// Partial sums of Σ_{i,c} W_ic ∂k(z_i, x_c)/∂θ over the m×n rectangle.
+cudaError_t cross_contract(const HostKernel& k, const double* z, long long ldz, int m, const double* x, long long ldx,
+                           int n, const double* W, long long ldw, double* partials, int* blocks_out, DevStatus* st,
+                           cudaStream_t s);
+// grad[p] = scale · (slot sums mapped to θ), grad[n_params] = noise_coef · Σ W_ii.
 cudaError_t grad_finalize(const HostKernel& k, const double* partials, int blocks, const int* slot_param_dev,
-                          double noise, double* grad, DevStatus* st, cudaStream_t s);
+                          double scale, double noise_coef, double* grad, DevStatus* st, cudaStream_t s);
 
 // Maximum partial-block count of grad_contract (sizes the partials buffer).
 int grad_max_blocks();

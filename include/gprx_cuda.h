@@ -194,6 +194,10 @@ gprx_status gprx_exact_fit(gprx_exact* h, const gprx_lbfgs_options* opt, gprx_fi
  * [fill, factor, inverse, gradient, total] (the reference's insert-stages idea). */
 gprx_status gprx_exact_stage_times(gprx_exact* h, double* out5);
 
+/* The CUDA stream (a cudaStream_t) the handle enqueues its work on, so a
+ * caller can time the handle's kernels with events on that stream. */
+gprx_status gprx_exact_stream(gprx_exact* h, void** stream);
+
 /* ---- online exact GPR (src/gpr/online.rs) ---- */
 /* FittedGpr::into_online: LLT → LDLT (src/gpr/fitted.rs:757-765,
  * src/gpr/factor_store.rs:157-179); assigns PointIds 0..n-1. */
@@ -205,6 +209,15 @@ gprx_status gprx_online_delete(gprx_exact* h, uint64_t id);
 uint64_t gprx_online_n(const gprx_exact* h);
 /* PointIds in buffer order (src/points.rs:76). */
 gprx_status gprx_online_point_ids(gprx_exact* h, uint64_t* out, uint64_t n);
+
+/* ------------------------------------------------------------------ */
+/* device microbenchmarks (diagnostics; no gprx counterpart)            */
+/* ------------------------------------------------------------------ */
+/* ms per launch of the FP64 DMMA GEMM C(m×n) = op(A)·op(B), k deep. */
+gprx_status gprx_probe_dgemm(int32_t m, int32_t n, int32_t k, int32_t trans_a, int32_t trans_b, int32_t reps,
+                             double* ms_per_launch);
+/* ms per blocked Cholesky factor of an n×n SPD matrix. */
+gprx_status gprx_probe_potrf(int32_t n, int32_t reps, double* ms_per_factor);
 
 /* ------------------------------------------------------------------ */
 /* seeded random numbers (src/rng.rs): Xoshiro256++ seeded by SplitMix64 */

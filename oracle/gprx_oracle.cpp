@@ -348,16 +348,32 @@ void trsm_lower_t(const double* l, int64_t n, int64_t ld, double* b, int64_t q, 
 // (src/workspace.rs:395-425), written as X = L⁻¹ then K⁻¹ = Xᵀ X.
 void llt_inverse(const double* l, int64_t n, int64_t ld, double* kinv, int64_t ldk) {
   Mat x((size_t)n * n, 0.0);
-  // X = L⁻¹, column by column (independent columns).
-#pragma omp parallel for schedule(dynamic, 8)
-  for (int64_t j = 0; j < n; ++j) {
-    double* col = &x[(size_t)j * n];
-    col[j] = 1.0 / AT(l, ld, j, j);
-    for (int64_t i = j + 1; i < n; ++i) {
-      double s = 0.0;
-      for (int64_t t = j; t < i; ++t) s += AT(l, ld, i, t) * col[t];
-      col[i] = -s / AT(l, ld, i, i);
+  // X = L⁻¹ by block rows: X_k = L_kk⁻¹ B_k (forward substitution), then
+  // B_{>k, ≤k} −= L_{>k,k} X_{k, ≤k}; B starts as the identity.
+  for (int64_t i = 0; i < n; ++i) x[(size_t)i * n + i] = 1.0;
+  const int NB = 64;
+  std::vector<double> pa, pb;
+  for (int64_t k = 0; k < n; k += NB) {
+    int nb = (int)std::min<int64_t>(NB, n - k);
+    int64_t cols = k + nb;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < cols; ++c) {
+      double* col = &x[(size_t)c * n];
+      for (int i = 0; i < nb; ++i) {
+        double s = col[k + i];
+        for (int t = 0; t < i; ++t) s -= AT(l, ld, k + i, k + t) * col[k + t];
+        col[k + i] = s / AT(l, ld, k + i, k + i);
+      }
     }
+    int64_t rest = n - cols;
+    if (rest <= 0) break;
+    pa.assign((size_t)rest * nb, 0.0);
+    for (int64_t i = 0; i < rest; ++i)
+      for (int t = 0; t < nb; ++t) pa[(size_t)i * nb + t] = AT(l, ld, cols + i, k + t);
+    pb.assign((size_t)cols * nb, 0.0);
+    for (int64_t c = 0; c < cols; ++c)
+      for (int t = 0; t < nb; ++t) pb[(size_t)c * nb + t] = x[(size_t)c * n + k + t];
+    packed_update(&x[(size_t)cols], n, pa.data(), (int)rest, pb.data(), (int)cols, nb, 0, 0, false);
   }
   // K⁻¹_ij = Σ_{t ≥ i} X_ti X_tj for i ≥ j (columns of X are contiguous).
 #pragma omp parallel for schedule(dynamic, 8)
