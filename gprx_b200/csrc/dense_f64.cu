@@ -112,200 +112,199 @@ __device__ void blk_store_full(double* dst, int ldd, const double* s, int ls, in
 }
 
 // ---------------------------------------------------------------------------
-// Fast diagonal block (nb ≤ 128): LLT by 32-column sub-panels and the block's
-// inverse, all in shared memory.
-//   per sub-panel p:  one warp factors the 32×32 diagonal sub-block in
-//                     registers (lane = row, pivots broadcast by shuffles) and
-//                     inverts it (lane = column);
-//                     all warps: P = A_below · L_pp⁻ᵀ, then A22 −= P Pᵀ.
-//   inverse:          column blocks right to left from X L = I:
-//                     X_ij = −(Σ_{k=j+1..i} X_ik L_kj) X_jj, in place.
+// Diagonal block (nb ≤ 128): LLT and the block's inverse in shared memory.
+// The block is padded to a multiple of 32 with an identity tail.
+//   per 32-column sub-panel p:
+//     warp 0 factors the 32×32 diagonal sub-block in registers (lane = row,
+//     pivots broadcast by shuffles) and inverts it (lane = column);
+//     all warps (DMMA m16n8k4): P = A_below · L_pp⁻ᵀ, then A22 −= P Pᵀ.
+//   inverse, column blocks right to left from X L = I (DMMA):
+//     X_ij = −(Σ_{k=j+1..i} X_ik L_kj) X_jj, in place.
 // ---------------------------------------------------------------------------
-constexpr int FD_THREADS = 512;
-constexpr int SB = 32;         // sub-panel width
-constexpr int SBL = SB + 1;    // ld of a 32×32 scratch block
+constexpr int FD_THREADS = 256;
+constexpr int SB = 32;          // sub-panel width
+constexpr int FLS = NB + 4;     // ld of the block (≡ 4 mod 16: conflict-free fragments)
+constexpr int XLD = SB + 4;     // ld of a 32×32 scratch block
 
-__device__ __forceinline__ void warp_factor_inv(double* s, int ls, int c0, int w, double* xd, int* fail) {
-  // lane r holds row r of the diagonal sub-block (columns ≤ r)
+// C(16×8) += A(16×K) · B(K×8) with A(i,k) = a[i·ai + k·ak], B(k,j) = b[k·bk + j·bj].
+__device__ __forceinline__ void mma_tile_smem(double (&c)[4], const double* a, int ai, int ak, const double* b, int bk,
+                                              int bj, int K) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  for (int kk = 0; kk < K; kk += 4) {
+    double a0 = a[g * ai + (kk + t) * ak];
+    double a1 = a[(g + 8) * ai + (kk + t) * ak];
+    double b0 = b[(kk + t) * bk + g * bj];
+    dmma_16x8x4(c, a0, a1, b0);
+  }
+}
+
+// Factor + invert the 32×32 sub-block at (c0, c0) of s; L goes back to s, L⁻¹
+// to xd (ld XLD).  Returns the failing column or −1 (uniform over the warp).
+__device__ __forceinline__ int warp_factor_inv32(double* s, int c0, double* xd) {
   const int lane = threadIdx.x & 31;
   double d[SB];
 #pragma unroll
-  for (int c = 0; c < SB; ++c) d[c] = (lane < w && c <= lane) ? s[(c0 + lane) + (c0 + c) * ls] : 0.0;
+  for (int c = 0; c < SB; ++c) d[c] = (c <= lane) ? s[(c0 + lane) + (c0 + c) * FLS] : 0.0;
   int bad = -1;
 #pragma unroll
   for (int j = 0; j < SB; ++j) {
-    if (j < w && bad < 0) {
-      double piv = __shfl_sync(0xffffffffu, d[j], j);
-      if (!(piv > 0.0)) {
-        bad = j;
-      } else {
-        double ljj = sqrt(piv);
-        if (lane == j) d[j] = ljj;
-        else if (lane > j) d[j] = d[j] / ljj;
+    double piv = __shfl_sync(0xffffffffu, d[j], j);
+    if (!(piv > 0.0) && bad < 0) bad = j;
+    double ljj = sqrt(fmax(piv, 1e-300));
+    if (lane == j) d[j] = ljj;
+    else if (lane > j) d[j] = d[j] / ljj;
 #pragma unroll
-        for (int c = j + 1; c < SB; ++c) {
-          double lcj = __shfl_sync(0xffffffffu, d[j], c);
-          if (lane >= c) d[c] = fma(-d[j], lcj, d[c]);
-        }
+    for (int c = 0; c < SB; ++c) {  // constant trip count keeps d[] in registers
+      if (c > j) {
+        double lcj = __shfl_sync(0xffffffffu, d[j], c);
+        if (lane >= c) d[c] = fma(-d[j], lcj, d[c]);
       }
     }
   }
-  if (bad >= 0) {
-    if (lane == 0) *fail = c0 + bad;
-    return;
-  }
-  if (lane < w) {
+  if (bad >= 0) return bad;
 #pragma unroll
-    for (int c = 0; c < SB; ++c)
-      if (c <= lane) s[(c0 + lane) + (c0 + c) * ls] = d[c];
+  for (int c = 0; c < SB; ++c)
+    if (c <= lane) s[(c0 + lane) + (c0 + c) * FLS] = d[c];
+  // X = L⁻¹: lane c holds column c; row r of L lives in lane r
+  double x[SB];
+#pragma unroll
+  for (int r = 0; r < SB; ++r) {
+    double acc = (r == lane) ? 1.0 : 0.0;
+#pragma unroll
+    for (int t = 0; t < SB; ++t)
+      if (t < r) acc = fma(-__shfl_sync(0xffffffffu, d[t], r), x[t], acc);
+    x[r] = acc / __shfl_sync(0xffffffffu, d[r], r);
   }
-  __syncwarp();
-  // inverse of the sub-block: lane c computes column c
-  if (lane < w) {
-    const int c = lane;
-    for (int r = 0; r < c; ++r) xd[r + c * SBL] = 0.0;
-    xd[c + c * SBL] = 1.0 / s[(c0 + c) + (c0 + c) * ls];
-    for (int r = c + 1; r < w; ++r) {
-      double acc = 0.0;
-      for (int t = c; t < r; ++t) acc = fma(s[(c0 + r) + (c0 + t) * ls], xd[t + c * SBL], acc);
-      xd[r + c * SBL] = -acc / s[(c0 + r) + (c0 + r) * ls];
-    }
-  }
+#pragma unroll
+  for (int r = 0; r < SB; ++r) xd[r + lane * XLD] = x[r];
+  return -1;
 }
 
 __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long long lda, long long k0, int nb,
                                                                  double* linv, DevStatus* st) {
-  extern __shared__ double smem[];
+  extern __shared__ __align__(16) double smem[];
   __shared__ int fail;
   if (dev_failed(st)) return;
-  const int ls = nb + 1;
-  double* s = smem;                       // nb × ls
-  double* xd = s + nb * ls;               // 4 × (32 × 33) diagonal sub-block inverses
-  double* tmp = xd + 4 * SB * SBL;        // 3 × (32 × 33)
-  const int tid = threadIdx.x, nt = blockDim.x;
+  double* s = smem;                       // NB × FLS
+  double* xd = s + NB * FLS;              // 4 × (32 × XLD) sub-block inverses
+  double* tmp = xd + 4 * SB * XLD;        // 3 × (32 × XLD)
+  const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, nw = nt >> 5;
+  const int lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+  const int npad = (nb + SB - 1) / SB * SB;
   if (tid == 0) fail = -1;
-  for (int e = tid; e < nb * nb; e += nt) {
-    int i = e % nb, j = e / nb;
-    s[i + j * ls] = (i >= j) ? A[(k0 + i) + (k0 + j) * lda] : 0.0;
+  for (int e = tid; e < npad * npad; e += nt) {
+    int i = e % npad, j = e / npad;
+    double v;
+    if (i < nb && j < nb) v = (i >= j) ? A[(k0 + i) + (k0 + j) * lda] : 0.0;
+    else v = (i == j) ? 1.0 : 0.0;
+    s[i + j * FLS] = v;
   }
   __syncthreads();
-  const int np = (nb + SB - 1) / SB;
+  const int np = npad / SB;
   for (int p = 0; p < np; ++p) {
-    const int c0 = p * SB, w = min(SB, nb - c0);
-    if (tid < 32) warp_factor_inv(s, ls, c0, w, xd + p * SB * SBL, &fail);
+    const int c0 = p * SB;
+    if (warp == 0) {
+      int f = warp_factor_inv32(s, c0, xd + p * SB * XLD);
+      if (f >= 0 && lane == 0) fail = c0 + f;
+    }
     __syncthreads();
     if (fail >= 0) {
       if (tid == 0) dev_fail(st, GPRX_CHOLESKY_FAILED, k0 + fail);
       return;
     }
-    const int r0 = c0 + w, cnt = nb - r0;
+    const int r0 = c0 + SB, cnt = npad - r0;
     if (cnt <= 0) break;
-    // P = A_below · X_ppᵀ  (P(r, c) = Σ_{t ≤ c} A(r, t) X(c, t))
-    const double* X = xd + p * SB * SBL;
-    const int items = cnt * (SB / 4);  // ≤ 96 · 8 = 768 ≤ 2 · FD_THREADS
-    // each thread: up to two items, results held until all reads finish
-    double res0[4] = {0, 0, 0, 0}, res1[4] = {0, 0, 0, 0};
-    auto item = [&](int it, double (&acc)[4]) {
-      int r = r0 + it % cnt, cg = (it / cnt) * 4;
-      for (int t = 0; t < w; ++t) {
-        double a = s[r + (c0 + t) * ls];
+    // P = A_below · X_ppᵀ: tiles (cnt/16) × 4, held in registers until all read
+    const double* X = xd + p * SB * XLD;
+    const int tiles = (cnt / 16) * 4;
+    double pc[2][4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = fma(a, X[(cg + q) + t * SBL], acc[q]);
+    for (int q = 0; q < 2; ++q) {
+      int tile = warp + q * nw;
+      for (int r = 0; r < 4; ++r) pc[q][r] = 0.0;
+      if (tile < tiles) {
+        int tm = tile % (cnt / 16), tn = tile / (cnt / 16);
+        // A(i, k) = s[(r0 + 16 tm + i) + (c0 + k) FLS]; B(k, j) = X(8 tn + j, k) = X[(8tn + j) + k XLD]
+        mma_tile_smem(pc[q], s + (r0 + 16 * tm) + c0 * FLS, 1, FLS, X + 8 * tn, XLD, 1, SB);
       }
-    };
-    auto put = [&](int it, const double (&acc)[4]) {
-      int r = r0 + it % cnt, cg = (it / cnt) * 4;
-#pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (cg + q < w) s[r + (c0 + cg + q) * ls] = acc[q];
-    };
-    if (tid < items) item(tid, res0);
-    if (tid + nt < items) item(tid + nt, res1);
+    }
     __syncthreads();
-    if (tid < items) put(tid, res0);
-    if (tid + nt < items) put(tid + nt, res1);
-    __syncthreads();
-    // A22 −= P Pᵀ over 4×4 blocks of the lower triangle
-    const int nb4 = (cnt + 3) / 4;
-    const int nblk = nb4 * (nb4 + 1) / 2;
-    for (int b = tid; b < nblk; b += nt) {
-      int bi = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
-      while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
-      while (bi * (bi + 1) / 2 > b) --bi;
-      int bj = b - bi * (bi + 1) / 2;
-      int i0 = r0 + bi * 4, j0 = r0 + bj * 4;
-      double a4[4][4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) a4[u][v] = 0.0;
-      for (int t = 0; t < w; ++t) {
-        double pi[4], pj[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          pi[u] = (i0 + u < nb) ? s[(i0 + u) + (c0 + t) * ls] : 0.0;
-          pj[u] = (j0 + u < nb) ? s[(j0 + u) + (c0 + t) * ls] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-          for (int v = 0; v < 4; ++v) a4[u][v] = fma(pi[u], pj[v], a4[u][v]);
+    for (int q = 0; q < 2; ++q) {
+      int tile = warp + q * nw;
+      if (tile < tiles) {
+        int tm = tile % (cnt / 16), tn = tile / (cnt / 16);
+        int row = r0 + 16 * tm + g, col = c0 + 8 * tn + 2 * t4;
+        s[row + col * FLS] = pc[q][0];
+        s[row + (col + 1) * FLS] = pc[q][1];
+        s[(row + 8) + col * FLS] = pc[q][2];
+        s[(row + 8) + (col + 1) * FLS] = pc[q][3];
       }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          int i = i0 + u, j = j0 + v;
-          if (i < nb && j < nb && i >= j) s[i + j * ls] -= a4[u][v];
-        }
+    }
+    __syncthreads();
+    // A22 −= P Pᵀ: 16×8 tiles not strictly above the diagonal
+    const int tm_n = cnt / 16, tn_n = cnt / 8;
+    for (int tile = warp; tile < tm_n * tn_n; tile += nw) {
+      int tm = tile % tm_n, tn = tile / tm_n;
+      int rbeg = 16 * tm, cbeg = 8 * tn;
+      if (rbeg + 15 < cbeg) continue;
+      double c[4] = {0, 0, 0, 0};
+      // A(i, k) = P(r0 + rbeg + i, k) ; B(k, j) = P(r0 + cbeg + j, k)
+      mma_tile_smem(c, s + (r0 + rbeg) + c0 * FLS, 1, FLS, s + (r0 + cbeg) + c0 * FLS, FLS, 1, SB);
+      int row = r0 + rbeg + g, col = r0 + cbeg + 2 * t4;
+      if (row >= col) s[row + col * FLS] -= c[0];
+      if (row >= col + 1) s[row + (col + 1) * FLS] -= c[1];
+      if (row + 8 >= col) s[(row + 8) + col * FLS] -= c[2];
+      if (row + 8 >= col + 1) s[(row + 8) + (col + 1) * FLS] -= c[3];
     }
     __syncthreads();
   }
   // L back to global
   for (int e = tid; e < nb * nb; e += nt) {
     int i = e % nb, j = e / nb;
-    if (i >= j) A[(k0 + i) + (k0 + j) * lda] = s[i + j * ls];
+    if (i >= j) A[(k0 + i) + (k0 + j) * lda] = s[i + j * FLS];
   }
   __syncthreads();
   // block inverse in place, column blocks right to left
   for (int jb = np - 1; jb >= 0; --jb) {
-    const int j0 = jb * SB, wj = min(SB, nb - j0);
-    const double* Xjj = xd + jb * SB * SBL;
-    // T_ib = Σ_{k=jb+1..ib} X_ik L_kj  for ib > jb (X_ik already in s for k > jb)
+    const int j0 = jb * SB;
     const int nout = np - 1 - jb;
-    for (int e = tid; e < nout * SB * SB; e += nt) {
-      int ib = jb + 1 + e / (SB * SB);
-      int rr = (e % (SB * SB)) % SB, cc = (e % (SB * SB)) / SB;
-      int i = ib * SB + rr, j = j0 + cc;
-      double acc = 0.0;
-      if (i < nb && cc < wj) {
-        // X (columns > jb, including the inverted diagonal blocks, zero above
-        // their diagonals) is already in s; column block jb still holds L.
-        const int kend = min(nb, (ib + 1) * SB);
-        for (int k = (jb + 1) * SB; k < kend; ++k) acc = fma(s[i + k * ls], s[k + j * ls], acc);
-      }
-      tmp[(ib - jb - 1) * SB * SBL + rr + cc * SBL] = acc;
+    // T_ib = Σ_{k=(jb+1)·32}^{(ib+1)·32−1} X(i, k) L(k, j): tiles (ib, 2 m-tiles, 4 n-tiles)
+    for (int tile = warp; tile < nout * 8; tile += nw) {
+      int ib = jb + 1 + tile / 8, tm = (tile % 8) / 4, tn = tile % 4;
+      double c[4] = {0, 0, 0, 0};
+      int kbeg = (jb + 1) * SB, kcnt = (ib - jb) * SB;
+      mma_tile_smem(c, s + (ib * SB + 16 * tm) + kbeg * FLS, 1, FLS, s + kbeg + (j0 + 8 * tn) * FLS, 1, FLS, kcnt);
+      double* T = tmp + (ib - jb - 1) * SB * XLD;
+      int row = 16 * tm + g, col = 8 * tn + 2 * t4;
+      T[row + col * XLD] = c[0];
+      T[row + (col + 1) * XLD] = c[1];
+      T[(row + 8) + col * XLD] = c[2];
+      T[(row + 8) + (col + 1) * XLD] = c[3];
     }
     __syncthreads();
-    // X_ib,jb = −T X_jj ; then X_jj onto the diagonal block
-    for (int e = tid; e < nout * SB * SB; e += nt) {
-      int ib = jb + 1 + e / (SB * SB);
-      int rr = (e % (SB * SB)) % SB, cc = (e % (SB * SB)) / SB;
-      int i = ib * SB + rr, j = j0 + cc;
-      if (i < nb && cc < wj) {
-        const double* T = tmp + (ib - jb - 1) * SB * SBL;
-        double acc = 0.0;
-        for (int k = cc; k < wj; ++k) acc = fma(T[rr + k * SBL], Xjj[k + cc * SBL], acc);
-        s[i + j * ls] = -acc;
-      }
+    const double* Xjj = xd + jb * SB * XLD;
+    for (int tile = warp; tile < nout * 8; tile += nw) {
+      int ib = jb + 1 + tile / 8, tm = (tile % 8) / 4, tn = tile % 4;
+      const double* T = tmp + (ib - jb - 1) * SB * XLD;
+      double c[4] = {0, 0, 0, 0};
+      mma_tile_smem(c, T + 16 * tm, 1, XLD, Xjj + 8 * tn * XLD, 1, XLD, SB);
+      int row = ib * SB + 16 * tm + g, col = j0 + 8 * tn + 2 * t4;
+      s[row + col * FLS] = -c[0];
+      s[row + (col + 1) * FLS] = -c[1];
+      s[(row + 8) + col * FLS] = -c[2];
+      s[(row + 8) + (col + 1) * FLS] = -c[3];
     }
     for (int e = tid; e < SB * SB; e += nt) {
       int rr = e % SB, cc = e / SB;
-      if (rr < wj && cc < wj) s[(j0 + rr) + (j0 + cc) * ls] = (rr >= cc) ? Xjj[rr + cc * SBL] : 0.0;
+      s[(j0 + rr) + (j0 + cc) * FLS] = (rr >= cc) ? Xjj[rr + cc * XLD] : 0.0;
     }
     __syncthreads();
   }
-  blk_store_full(linv, NB, s, ls, nb);
+  for (int e = tid; e < nb * nb; e += nt) {
+    int i = e % nb, j = e / nb;
+    linv[i + j * NB] = (i >= j) ? s[i + j * FLS] : 0.0;
+  }
 }
 
 __global__ void __launch_bounds__(DIAG_THREADS) tri_inv_blocks_kernel(const double* L, long long ld, int n,
@@ -322,7 +321,7 @@ __global__ void __launch_bounds__(DIAG_THREADS) tri_inv_blocks_kernel(const doub
 }
 
 static size_t diag_smem(int nb) { return (size_t)(nb * (nb + 1) + nb) * sizeof(double); }
-static size_t fast_diag_smem(int nb) { return (size_t)(nb * (nb + 1) + 7 * SB * SBL) * sizeof(double); }
+static size_t fast_diag_smem(int nb) { (void)nb; return (size_t)(NB * FLS + 7 * SB * XLD) * sizeof(double); }
 
 static cudaError_t diag_attrs() {
   static bool done = false;
@@ -392,23 +391,60 @@ cudaError_t set_identity(double* X, long long ld, int n, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-// Solves L X = I right-looking over block rows: X_k = L_kk⁻¹ B_k, then
-// B_{>k} −= L_{>k,k} X_k (columns ≤ the block only; the rest stays zero).
+// X = L⁻¹ by recursive doubling over the NB-blocks: the diagonal blocks are
+// the inverses the factor left in linv; at each level every pair of sibling
+// blocks gets X21 = −X22 (L21 X11), two batched triangular products with the
+// k-ranges cut to the nonzero triangles.  X's strict upper triangle must be
+// zero on entry (it is never written).  scratch holds ceil(n/2)² doubles.
+__global__ void copy_diag_blocks_kernel(const double* linv, int n, double* X, long long ldx) {
+  long long k0 = (long long)blockIdx.x * NB;
+  int nb = (int)min((long long)NB, n - k0);
+  const double* src = linv + (long long)blockIdx.x * NB * NB;
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    int i = e % nb, j = e / nb;
+    X[(k0 + i) + (k0 + j) * ldx] = src[i + j * NB];
+  }
+}
+
 cudaError_t trtri_blocked(const double* L, long long ld, int n, const double* linv, double* X, long long ldx,
-                          DevStatus* st, cudaStream_t s) {
-  CK(set_identity(X, ldx, n, s));
-  for (int k0 = 0; k0 < n; k0 += NB) {
-    int nbk = min(NB, n - k0);
-    int cols = k0 + nbk;
-    const double* lk = linv + (long long)(k0 / NB) * NB * NB;
-    double* Xk = X + k0;
-    GemmParams p1 = gemm_params(nbk, cols, nbk, lk, NB, Xk, ldx, Xk, ldx, 1.0, 0.0, st);
-    CK(dgemm(false, false, p1, s));
-    int rest = n - cols;
-    if (rest <= 0) break;
-    GemmParams p2 = gemm_params(rest, cols, nbk, L + cols + (long long)k0 * ld, ld, Xk, ldx, X + cols, ldx, -1.0,
-                                1.0, st);
-    CK(dgemm(false, false, p2, s));
+                          double* scratch, DevStatus* st, cudaStream_t s) {
+  int nblk = ceil_div(n, NB);
+  GPRX_LAUNCH(copy_diag_blocks_kernel, nblk, 256, 0, s, linv, n, X, ldx);
+  for (long long b = 2LL * NB; b < 2LL * n; b *= 2) {
+    long long h = b / 2;
+    if (h >= n) break;
+    long long full = n / b;            // pairs with both halves of size h
+    long long r = n - full * b;        // tail: a pair when it reaches past h
+    for (int part = 0; part < 2; ++part) {
+      long long s0, cnt, h2;
+      if (part == 0) {
+        if (full == 0) continue;
+        s0 = 0;
+        cnt = full;
+        h2 = h;
+      } else {
+        if (r <= h) continue;
+        s0 = full * b;
+        cnt = 1;
+        h2 = r - h;
+      }
+      // T = L21 · X11   (h2 × h, K = h; X11 lower → k from the column)
+      GemmParams p1 = gemm_params((int)h2, (int)h, (int)h, L + (s0 + h) + s0 * ld, ld, X + s0 + s0 * ldx, ldx,
+                                  scratch, h2, 1.0, 0.0, st);
+      p1.mode = GEMM_K_FROM_COL;
+      p1.strideA = b + b * ld;
+      p1.strideB = b + b * ldx;
+      p1.strideC = h2 * h;
+      CK(dgemm(false, false, p1, s, (int)cnt));
+      // X21 = −X22 · T   (h2 × h, K = h2; X22 lower → k up to the row)
+      GemmParams p2 = gemm_params((int)h2, (int)h, (int)h2, X + (s0 + h) + (s0 + h) * ldx, ldx, scratch, h2,
+                                  X + (s0 + h) + s0 * ldx, ldx, -1.0, 0.0, st);
+      p2.mode = GEMM_K_TO_ROW;
+      p2.strideA = b + b * ldx;
+      p2.strideB = h2 * h;
+      p2.strideC = b + b * ldx;
+      CK(dgemm(false, false, p2, s, (int)cnt));
+    }
   }
   return cudaGetLastError();
 }

@@ -27,10 +27,11 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
 cudaError_t tri_inv_blocks(const double* L, long long ld, int n, bool unit, double* linv, DevStatus* st,
                            cudaStream_t s);
 
-// X = L⁻¹ into X (n×n, ldx; zero above the diagonal), from L and its diagonal
-// block inverses.
+// X = L⁻¹ into X (n×n, ldx), from L and its diagonal block inverses.  X's
+// strict upper triangle must be zero on entry; scratch holds ceil(n/2)²
+// doubles.
 cudaError_t trtri_blocked(const double* L, long long ld, int n, const double* linv, double* X, long long ldx,
-                          DevStatus* st, cudaStream_t s);
+                          double* scratch, DevStatus* st, cudaStream_t s);
 
 // C (lower) = Xᵀ X for lower-triangular X: K⁻¹ from X = L⁻¹.
 cudaError_t lauum_lower(const double* X, long long ldx, int n, double* C, long long ldc, DevStatus* st,

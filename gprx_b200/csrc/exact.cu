@@ -198,10 +198,13 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
   double last = 0.0;
   const size_t nn = (size_t)ld * cap;
   if (grad && Xinv.n < nn) {
-    if (Xinv.alloc(nn) != cudaSuccess) {
+    size_t half = (size_t)((n + 1) / 2) * ((n + 1) / 2);
+    if (Xinv.alloc(nn) != cudaSuccess || scratch.alloc(std::max<size_t>(half, 1)) != cudaSuccess) {
+      Xinv.reset();
       write_params(prev.data());
       return set_error(GPRX_OUT_OF_MEMORY, "device allocation of the inverse failed");
     }
+    GPRX_CUDA_TRY(cudaMemsetAsync(Xinv.p, 0, sizeof(double) * nn, stream));
   }
   for (double j : js) {
     last = j;
@@ -209,7 +212,7 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
     if ((st = enqueue_factor(j)) != GPRX_OK) return st;
     GPRX_CUDA_TRY(logdet_diag(A.p, ld, n, false, res.p + 0, status.p, stream));
     if (grad) {
-      GPRX_CUDA_TRY(trtri_blocked(A.p, ld, n, linv.p, Xinv.p, ld, status.p, stream));
+      GPRX_CUDA_TRY(trtri_blocked(A.p, ld, n, linv.p, Xinv.p, ld, scratch.p, status.p, stream));
       GPRX_CUDA_TRY(trmv_lower(Xinv.p, ld, n, y.p, z.p, status.p, stream));
       GPRX_CUDA_TRY(gemv_t(Xinv.p, ld, n, n, true, z.p, alpha.p, status.p, stream));
       GPRX_CUDA_TRY(dot_dev(y.p, alpha.p, n, res.p + 1, status.p, stream));

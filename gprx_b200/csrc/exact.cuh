@@ -28,7 +28,8 @@ struct ExactState {
   DevBuf<double> x;        // cap×d (column-major, ld = cap)
   DevBuf<double> y;        // cap
   DevBuf<double> A;        // ld×cap: K → L (→ K⁻¹ after a gradient; → LDLT online)
-  DevBuf<double> Xinv;     // ld×cap: L⁻¹ (gradient path)
+  DevBuf<double> Xinv;     // ld×cap: L⁻¹ (gradient path; strict upper triangle kept zero)
+  DevBuf<double> scratch;  // ceil(n/2)² doubles for the recursive triangular inverse
   DevBuf<double> linv;     // diagonal-block inverses
   DevBuf<double> alpha, z, tmpv;
   DevBuf<double> partials;

@@ -26,6 +26,7 @@ enum GemmMode : int {
   GEMM_K_FROM_ROW = 2,
   GEMM_SPLIT_K = 4,
   GEMM_K_TO_ROW = 8,   // k-loop stops at the tile's last global row + 1 (lower-triangular A)
+  GEMM_K_FROM_COL = 16, // k-loop starts at the tile's first global column (lower-triangular B)
 };
 
 struct GemmParams {
@@ -137,6 +138,11 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES, TA, TB>::T
   if (p.mode & GEMM_K_FROM_ROW) {
     long long first_row = p.row0 + m0;  // global row of this tile
     long long kb = first_row - p.krow0;
+    if (kb > kbeg) kbeg = (int)(kb / BK * BK);
+  }
+  if (p.mode & GEMM_K_FROM_COL) {
+    long long first_col = p.col0 + n0;
+    long long kb = first_col - p.krow0;
     if (kb > kbeg) kbeg = (int)(kb / BK * BK);
   }
   if (p.mode & GEMM_K_TO_ROW) {
