@@ -217,9 +217,9 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
     // P = A_below · X_ppᵀ: tiles (cnt/16) × 4, held in registers until all read
     const double* X = xd + p * SB * XLD;
     const int tiles = (cnt / 16) * 4;
-    double pc[2][4];
+    double pc[3][4];  // ≤ 24 tiles over 8 warps
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < 3; ++q) {
       int tile = warp + q * nw;
       for (int r = 0; r < 4; ++r) pc[q][r] = 0.0;
       if (tile < tiles) {
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < 3; ++q) {
       int tile = warp + q * nw;
       if (tile < tiles) {
         int tm = tile % (cnt / 16), tn = tile / (cnt / 16);
