@@ -130,6 +130,7 @@ constexpr int XLD = SB + 4;     // ld of a 32×32 scratch block
 __device__ __forceinline__ void mma_tile_smem(double (&c)[4], const double* a, int ai, int ak, const double* b, int bk,
                                               int bj, int K) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll 4
   for (int kk = 0; kk < K; kk += 4) {
     double a0 = a[g * ai + (kk + t) * ak];
     double a1 = a[(g + 8) * ai + (kk + t) * ak];
@@ -140,19 +141,25 @@ __device__ __forceinline__ void mma_tile_smem(double (&c)[4], const double* a, i
 
 // Factor + invert the 32×32 sub-block at (c0, c0) of s; L goes back to s, L⁻¹
 // to xd (ld XLD).  Returns the failing column or −1 (uniform over the warp).
+// Pivot step: L_jj = piv·rsqrt(piv), the column below scaled by rsqrt(piv).
 __device__ __forceinline__ int warp_factor_inv32(double* s, int c0, double* xd) {
   const int lane = threadIdx.x & 31;
   double d[SB];
 #pragma unroll
   for (int c = 0; c < SB; ++c) d[c] = (c <= lane) ? s[(c0 + lane) + (c0 + c) * FLS] : 0.0;
   int bad = -1;
+  double my_inv = 1.0;  // 1 / L_{lane,lane}
 #pragma unroll
   for (int j = 0; j < SB; ++j) {
     double piv = __shfl_sync(0xffffffffu, d[j], j);
     if (!(piv > 0.0) && bad < 0) bad = j;
-    double ljj = sqrt(fmax(piv, 1e-300));
-    if (lane == j) d[j] = ljj;
-    else if (lane > j) d[j] = d[j] / ljj;
+    double rs = rsqrt(fmax(piv, 1e-300));
+    if (lane == j) {
+      d[j] = piv * rs;
+      my_inv = rs;
+    } else if (lane > j) {
+      d[j] = d[j] * rs;
+    }
 #pragma unroll
     for (int c = 0; c < SB; ++c) {  // constant trip count keeps d[] in registers
       if (c > j) {
@@ -173,11 +180,31 @@ __device__ __forceinline__ int warp_factor_inv32(double* s, int c0, double* xd) 
 #pragma unroll
     for (int t = 0; t < SB; ++t)
       if (t < r) acc = fma(-__shfl_sync(0xffffffffu, d[t], r), x[t], acc);
-    x[r] = acc / __shfl_sync(0xffffffffu, d[r], r);
+    x[r] = acc * __shfl_sync(0xffffffffu, my_inv, r);
   }
 #pragma unroll
   for (int r = 0; r < SB; ++r) xd[r + lane * XLD] = x[r];
   return -1;
+}
+
+// A22 −= P Pᵀ on the 16×8 tiles of rows [rlo, npad) × columns [clo, chi) that
+// are not strictly above the diagonal; tiles dealt to warps w0.. in steps of nws.
+__device__ __forceinline__ void diag_syrk_tiles(double* s, int c0, int rlo, int clo, int chi, int npad, int w0,
+                                                int nws) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+  const int tm_n = (npad - rlo) / 16, tn_n = (chi - clo) / 8;
+  for (int tile = warp - w0; tile < tm_n * tn_n; tile += nws) {
+    int tm = tile % tm_n, tn = tile / tm_n;
+    int rbeg = rlo + 16 * tm, cbeg = clo + 8 * tn;
+    if (rbeg + 15 < cbeg) continue;
+    double c[4] = {0, 0, 0, 0};
+    mma_tile_smem(c, s + rbeg + c0 * FLS, 1, FLS, s + cbeg + c0 * FLS, FLS, 1, SB);
+    int row = rbeg + g, col = cbeg + 2 * t4;
+    if (row >= col) s[row + col * FLS] -= c[0];
+    if (row >= col + 1) s[row + (col + 1) * FLS] -= c[1];
+    if (row + 8 >= col) s[(row + 8) + col * FLS] -= c[2];
+    if (row + 8 >= col + 1) s[(row + 8) + (col + 1) * FLS] -= c[3];
+  }
 }
 
 __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long long lda, long long k0, int nb,
@@ -192,26 +219,29 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
   const int lane = tid & 31, g = lane >> 2, t4 = lane & 3;
   const int npad = (nb + SB - 1) / SB * SB;
   if (tid == 0) fail = -1;
+  // block load: every lower entry in flight at once (cp.async), padding after
+  for (int j = warp; j < nb; j += nw)
+    for (int i = j + lane; i < nb; i += 32) cp_async8(s + i + j * FLS, A + (k0 + i) + (k0 + j) * lda, true);
+  cp_async_commit();
   for (int e = tid; e < npad * npad; e += nt) {
     int i = e % npad, j = e / npad;
-    double v;
-    if (i < nb && j < nb) v = (i >= j) ? A[(k0 + i) + (k0 + j) * lda] : 0.0;
-    else v = (i == j) ? 1.0 : 0.0;
-    s[i + j * FLS] = v;
+    if (i < j) s[i + j * FLS] = 0.0;
+    else if (i >= nb || j >= nb) s[i + j * FLS] = (i == j) ? 1.0 : 0.0;
   }
+  cp_async_wait<0>();
   __syncthreads();
   const int np = npad / SB;
+  if (warp == 0) {
+    int f = warp_factor_inv32(s, 0, xd);
+    if (f >= 0 && lane == 0) fail = f;
+  }
+  __syncthreads();
   for (int p = 0; p < np; ++p) {
-    const int c0 = p * SB;
-    if (warp == 0) {
-      int f = warp_factor_inv32(s, c0, xd + p * SB * XLD);
-      if (f >= 0 && lane == 0) fail = c0 + f;
-    }
-    __syncthreads();
     if (fail >= 0) {
       if (tid == 0) dev_fail(st, GPRX_CHOLESKY_FAILED, k0 + fail);
       return;
     }
+    const int c0 = p * SB;
     const int r0 = c0 + SB, cnt = npad - r0;
     if (cnt <= 0) break;
     // P = A_below · X_ppᵀ: tiles (cnt/16) × 4, held in registers until all read
@@ -221,10 +251,10 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       int tile = warp + q * nw;
+#pragma unroll
       for (int r = 0; r < 4; ++r) pc[q][r] = 0.0;
       if (tile < tiles) {
         int tm = tile % (cnt / 16), tn = tile / (cnt / 16);
-        // A(i, k) = s[(r0 + 16 tm + i) + (c0 + k) FLS]; B(k, j) = X(8 tn + j, k) = X[(8tn + j) + k XLD]
         mma_tile_smem(pc[q], s + (r0 + 16 * tm) + c0 * FLS, 1, FLS, X + 8 * tn, XLD, 1, SB);
       }
     }
@@ -242,29 +272,25 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
       }
     }
     __syncthreads();
-    // A22 −= P Pᵀ: 16×8 tiles not strictly above the diagonal
-    const int tm_n = cnt / 16, tn_n = cnt / 8;
-    for (int tile = warp; tile < tm_n * tn_n; tile += nw) {
-      int tm = tile % tm_n, tn = tile / tm_n;
-      int rbeg = 16 * tm, cbeg = 8 * tn;
-      if (rbeg + 15 < cbeg) continue;
-      double c[4] = {0, 0, 0, 0};
-      // A(i, k) = P(r0 + rbeg + i, k) ; B(k, j) = P(r0 + cbeg + j, k)
-      mma_tile_smem(c, s + (r0 + rbeg) + c0 * FLS, 1, FLS, s + (r0 + cbeg) + c0 * FLS, FLS, 1, SB);
-      int row = r0 + rbeg + g, col = r0 + cbeg + 2 * t4;
-      if (row >= col) s[row + col * FLS] -= c[0];
-      if (row >= col + 1) s[row + (col + 1) * FLS] -= c[1];
-      if (row + 8 >= col) s[(row + 8) + col * FLS] -= c[2];
-      if (row + 8 >= col + 1) s[(row + 8) + (col + 1) * FLS] -= c[3];
+    // the next sub-panel's columns first (all warps) ...
+    diag_syrk_tiles(s, c0, r0, r0, r0 + SB, npad, 0, nw);
+    __syncthreads();
+    // ... then warp 0 factors it while the other warps update the rest
+    if (warp == 0) {
+      int f = warp_factor_inv32(s, r0, xd + (p + 1) * SB * XLD);
+      if (f >= 0 && lane == 0) fail = r0 + f;
+    } else if (r0 + SB < npad) {
+      diag_syrk_tiles(s, c0, r0 + SB, r0 + SB, npad, npad, 1, nw - 1);
     }
     __syncthreads();
   }
-  // L back to global
-  for (int e = tid; e < nb * nb; e += nt) {
-    int i = e % nb, j = e / nb;
-    if (i >= j) A[(k0 + i) + (k0 + j) * lda] = s[i + j * FLS];
+  if (fail >= 0) {
+    if (tid == 0) dev_fail(st, GPRX_CHOLESKY_FAILED, k0 + fail);
+    return;
   }
-  __syncthreads();
+  // L back to global
+  for (int j = warp; j < nb; j += nw)
+    for (int i = j + lane; i < nb; i += 32) A[(k0 + i) + (k0 + j) * lda] = s[i + j * FLS];
   // block inverse in place, column blocks right to left
   for (int jb = np - 1; jb >= 0; --jb) {
     const int j0 = jb * SB;
@@ -301,10 +327,8 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
     }
     __syncthreads();
   }
-  for (int e = tid; e < nb * nb; e += nt) {
-    int i = e % nb, j = e / nb;
-    linv[i + j * NB] = (i >= j) ? s[i + j * FLS] : 0.0;
-  }
+  for (int j = warp; j < NB; j += nw)
+    for (int i = lane; i < NB; i += 32) linv[i + j * NB] = (i < nb && j < nb && i >= j) ? s[i + j * FLS] : 0.0;
 }
 
 __global__ void __launch_bounds__(DIAG_THREADS) tri_inv_blocks_kernel(const double* L, long long ld, int n,
@@ -341,24 +365,96 @@ static cudaError_t diag_attrs() {
     if (e_ != cudaSuccess) return e_;        \
   } while (0)
 
-cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatus* st, cudaStream_t s) {
-  CK(diag_attrs());
-  for (int k0 = 0; k0 < n; k0 += NB) {
-    int nbk = min(NB, n - k0);
-    double* lk = linv + (long long)(k0 / NB) * NB * NB;
-    GPRX_LAUNCH(potrf_diag_kernel, 1, FD_THREADS, fast_diag_smem(nbk), s, A, ld, (long long)k0, nbk, lk, st);
-    int rest = n - k0 - nbk;
-    if (rest <= 0) break;
+FactorCtx::~FactorCtx() {
+  for (auto e : ev) cudaEventDestroy(e);
+  if (aux) cudaStreamDestroy(aux);
+}
+
+cudaError_t FactorCtx::ensure(int nblk) {
+  if (!aux) {
+    int lo, hi;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&aux, cudaStreamNonBlocking, hi));
+  }
+  while ((int)ev.size() < 2 * nblk + 2) {
+    cudaEvent_t e;
+    CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ev.push_back(e);
+  }
+  return cudaSuccess;
+}
+
+static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double* linv, DevStatus* st,
+                                  cudaStream_t s) {
+  int nbk = min(NB, n - k0);
+  double* lk = linv + (long long)(k0 / NB) * NB * NB;
+  GPRX_LAUNCH(potrf_diag_kernel, 1, FD_THREADS, fast_diag_smem(nbk), s, A, ld, (long long)k0, nbk, lk, st);
+  int rest = n - k0 - nbk;
+  if (rest > 0) {
     double* P = A + (k0 + nbk) + (long long)k0 * ld;
     // panel: P := P · L_kk⁻ᵀ (in place; the 128-wide tile covers all nbk columns)
     GemmParams pp = gemm_params(rest, nbk, nbk, P, ld, lk, NB, P, ld, 1.0, 0.0, st);
     CK(dgemm(false, true, pp, s));
-    // trailing: A22 −= P Pᵀ (lower tiles)
-    double* A22 = A + (k0 + nbk) + (long long)(k0 + nbk) * ld;
-    GemmParams ps = gemm_params(rest, rest, nbk, P, ld, P, ld, A22, ld, -1.0, 1.0, st);
-    ps.mode = GEMM_LOWER_TILES;
-    CK(dgemm(false, true, ps, s));
   }
+  return cudaGetLastError();
+}
+
+cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatus* st, cudaStream_t s,
+                          FactorCtx* ctx) {
+  CK(diag_attrs());
+  const int nblk = ceil_div(n, NB);
+  if (!ctx) {
+    for (int k0 = 0; k0 < n; k0 += NB) {
+      CK(diag_and_panel(A, ld, n, k0, linv, st, s));
+      int nbk = min(NB, n - k0), rest = n - k0 - nbk;
+      if (rest <= 0) break;
+      double* P = A + (k0 + nbk) + (long long)k0 * ld;
+      double* A22 = A + (k0 + nbk) + (long long)(k0 + nbk) * ld;
+      GemmParams ps = gemm_params(rest, rest, nbk, P, ld, P, ld, A22, ld, -1.0, 1.0, st);
+      ps.mode = GEMM_LOWER_TILES;
+      CK(dgemm(false, true, ps, s));
+    }
+    return cudaGetLastError();
+  }
+  CK(ctx->ensure(nblk));
+  cudaStream_t X = ctx->aux;
+  cudaEvent_t* Ep = ctx->ev.data();          // panel k done (on X)
+  cudaEvent_t* Es = ctx->ev.data() + nblk;   // trailing update of step k done (on s)
+  cudaEvent_t Ein = ctx->ev[2 * nblk];
+  CK(cudaEventRecord(Ein, s));
+  CK(cudaStreamWaitEvent(X, Ein, 0));
+  CK(diag_and_panel(A, ld, n, 0, linv, st, X));
+  CK(cudaEventRecord(Ep[0], X));
+  int last = 0;
+  for (int k = 0; k < nblk; ++k) {
+    const int c1 = (k + 1) * NB;  // first column of block k+1
+    if (c1 >= n) break;
+    const int k0 = k * NB;
+    const double* Pk = A + c1 + (long long)k0 * ld;  // panel k, rows from c1
+    // critical chain of block k+1 (side stream)
+    if (k >= 1) CK(cudaStreamWaitEvent(X, Es[k - 1], 0));
+    {
+      int m = n - c1, w = min(NB, n - c1);
+      GemmParams pc = gemm_params(m, w, NB, Pk, ld, Pk, ld, A + c1 + (long long)c1 * ld, ld, -1.0, 1.0, st);
+      pc.mode = GEMM_LOWER_TILES;
+      CK(dgemm(false, true, pc, X));
+    }
+    CK(diag_and_panel(A, ld, n, c1, linv, st, X));
+    CK(cudaEventRecord(Ep[k + 1], X));
+    last = k + 1;
+    // bulk trailing update of step k (main stream): columns from c2
+    CK(cudaStreamWaitEvent(s, Ep[k], 0));
+    const int c2 = c1 + NB;
+    if (c2 < n) {
+      int m = n - c2;
+      const double* Pk2 = A + c2 + (long long)k0 * ld;
+      GemmParams ps = gemm_params(m, m, NB, Pk2, ld, Pk2, ld, A + c2 + (long long)c2 * ld, ld, -1.0, 1.0, st);
+      ps.mode = GEMM_LOWER_TILES;
+      CK(dgemm(false, true, ps, s));
+    }
+    CK(cudaEventRecord(Es[k], s));
+  }
+  CK(cudaStreamWaitEvent(s, Ep[last], 0));
   return cudaGetLastError();
 }
 

@@ -2,6 +2,8 @@
 #pragma once
 
 #include "common.cuh"
+#include <vector>
+
 #include "gemm_f64.cuh"
 
 namespace gprx {
@@ -17,11 +19,24 @@ cudaError_t dgemm(bool ta, bool tb, const GemmParams& p, cudaStream_t s, int bat
 GemmParams gemm_params(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
                        double* C, long long ldc, double alpha, double beta, const DevStatus* st);
 
+// Side stream and events of the look-ahead factorization (one per handle).
+struct FactorCtx {
+  int device = -1;
+  cudaStream_t aux = nullptr;
+  std::vector<cudaEvent_t> ev;
+  ~FactorCtx();
+  cudaError_t ensure(int nblk);
+};
+
 // In-place lower Cholesky of A (n×n, ld) by right-looking blocks of NB.
 // linv receives the inverse of every diagonal block (ceil(n/NB) blocks of
 // NB×NB, column-major, ld NB).  A non-positive pivot sets st (CHOLESKY_FAILED,
 // info = global row) and every later kernel of the stream returns at once.
-cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatus* st, cudaStream_t s);
+// With ctx, the chain column update → diagonal block → panel solve of step
+// k+1 runs on ctx->aux (high priority) while the trailing update of step k
+// runs on s; on return all work is ordered before later work on s.
+cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatus* st, cudaStream_t s,
+                          FactorCtx* ctx = nullptr);
 
 // Inverses of the diagonal NB-blocks of a lower triangle (unit: unit diagonal).
 cudaError_t tri_inv_blocks(const double* L, long long ld, int n, bool unit, double* linv, DevStatus* st,

@@ -36,6 +36,7 @@ struct ExactState {
   DevBuf<int> slot_param;
   DevBuf<double> res;      // [0] logdet, [1] yᵀα, [2..] grad
   DevBuf<DevStatus> status;
+  FactorCtx fctx;          // side stream + events of the look-ahead factor
   HostPinned<double> res_h;
   HostPinned<DevStatus> status_h;
   DevBuf<double> qbuf, qx;  // predict scratch

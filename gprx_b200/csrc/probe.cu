@@ -89,11 +89,12 @@ gprx_status gprx_probe_potrf(int32_t n, int32_t reps, double* ms_per_factor) {
   cudaEventCreate(&e1);
   float total = 0.f;
   cudaError_t e = cudaSuccess;
+  FactorCtx ctx;
   for (int r = 0; r < reps + 1 && e == cudaSuccess; ++r) {
     cudaMemsetAsync(st.p, 0, sizeof(DevStatus), s);
     fill_spd_kernel<<<1184, 256, 0, s>>>(A.p, ld, n);
     cudaEventRecord(e0, s);
-    e = potrf_blocked(A.p, ld, n, linv.p, st.p, s);
+    e = potrf_blocked(A.p, ld, n, linv.p, st.p, s, &ctx);
     cudaEventRecord(e1, s);
     cudaStreamSynchronize(s);
     float ms;
