@@ -43,6 +43,8 @@ GemmParams gemm_params(int M, int N, int K, const double* A, long long lda, cons
   p.split_stride = 0;
   p.status = st;
   p.strideA = p.strideB = p.strideC = 0;
+  p.max_ctas = 0;
+  p.splits_tiles = 0;
   return p;
 }
 
@@ -139,51 +141,125 @@ __device__ __forceinline__ void mma_tile_smem(double (&c)[4], const double* a, i
   }
 }
 
-// Factor + invert the 32×32 sub-block at (c0, c0) of s; L goes back to s, L⁻¹
-// to xd (ld XLD).  Returns the failing column or −1 (uniform over the warp).
-// Pivot step: L_jj = piv·rsqrt(piv), the column below scaled by rsqrt(piv).
-__device__ __forceinline__ int warp_factor_inv32(double* s, int c0, double* xd) {
-  const int lane = threadIdx.x & 31;
-  double d[SB];
+// 16×16 leaf, one warp: lanes r and r+16 both hold row r of the block at
+// (off, off) of s in registers; pivots are broadcast by shuffles.  Writes L
+// back to s and L⁻¹ (column-major, ld XLD) to xo.  Returns the failing column
+// or −1.  Kept out of line so one compact copy serves every call (the fully
+// unrolled 32-wide form overflowed the instruction cache).
+__device__ __noinline__ int leaf16_factor_inv(double* s, int off, double* xo) {
+  const int lane = threadIdx.x & 31, r = lane & 15;
+  double d[16];
 #pragma unroll
-  for (int c = 0; c < SB; ++c) d[c] = (c <= lane) ? s[(c0 + lane) + (c0 + c) * FLS] : 0.0;
+  for (int c = 0; c < 16; ++c) d[c] = (c <= r) ? s[(off + r) + (off + c) * FLS] : 0.0;
   int bad = -1;
-  double my_inv = 1.0;  // 1 / L_{lane,lane}
+  double my_inv = 1.0;
 #pragma unroll
-  for (int j = 0; j < SB; ++j) {
+  for (int j = 0; j < 16; ++j) {
     double piv = __shfl_sync(0xffffffffu, d[j], j);
     if (!(piv > 0.0) && bad < 0) bad = j;
     double rs = rsqrt(fmax(piv, 1e-300));
-    if (lane == j) {
+    if (r == j) {
       d[j] = piv * rs;
       my_inv = rs;
-    } else if (lane > j) {
+    } else if (r > j) {
       d[j] = d[j] * rs;
     }
 #pragma unroll
-    for (int c = 0; c < SB; ++c) {  // constant trip count keeps d[] in registers
+    for (int c = 0; c < 16; ++c) {
       if (c > j) {
         double lcj = __shfl_sync(0xffffffffu, d[j], c);
-        if (lane >= c) d[c] = fma(-d[j], lcj, d[c]);
+        if (r >= c) d[c] = fma(-d[j], lcj, d[c]);
       }
     }
   }
   if (bad >= 0) return bad;
+  if (lane < 16) {
 #pragma unroll
-  for (int c = 0; c < SB; ++c)
-    if (c <= lane) s[(c0 + lane) + (c0 + c) * FLS] = d[c];
-  // X = L⁻¹: lane c holds column c; row r of L lives in lane r
-  double x[SB];
-#pragma unroll
-  for (int r = 0; r < SB; ++r) {
-    double acc = (r == lane) ? 1.0 : 0.0;
-#pragma unroll
-    for (int t = 0; t < SB; ++t)
-      if (t < r) acc = fma(-__shfl_sync(0xffffffffu, d[t], r), x[t], acc);
-    x[r] = acc * __shfl_sync(0xffffffffu, my_inv, r);
+    for (int c = 0; c < 16; ++c)
+      if (c <= r) s[(off + r) + (off + c) * FLS] = d[c];
   }
+  double x[16];
 #pragma unroll
-  for (int r = 0; r < SB; ++r) xd[r + lane * XLD] = x[r];
+  for (int q = 0; q < 16; ++q) {
+    double acc = (q == r) ? 1.0 : 0.0;
+#pragma unroll
+    for (int t = 0; t < 16; ++t)
+      if (t < q) acc = fma(-__shfl_sync(0xffffffffu, d[t], q), x[t], acc);
+    x[q] = acc * __shfl_sync(0xffffffffu, my_inv, q);
+  }
+  if (lane < 16) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) xo[q + r * XLD] = x[q];
+  }
+  __syncwarp();
+  return -1;
+}
+
+// Factor + invert the 32×32 sub-block at (c0, c0) of s with one warp, as two
+// 16×16 leaves: L21 = A21 X11ᵀ, A22 −= L21 L21ᵀ, then X21 = −X22 (L21 X11),
+// the products on DMMA.  L goes back to s, L⁻¹ to xd (ld XLD, zero above the
+// diagonal).  Returns the failing column or −1 (uniform over the warp).
+__device__ __forceinline__ int warp_factor_inv32(double* s, int c0, double* xd) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
+  int f = leaf16_factor_inv(s, c0, xd);
+  if (f >= 0) return f;
+  // L21 = A21 · X11ᵀ  (B(k, j) = X11(j, k))
+  double c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+#pragma unroll
+  for (int tn = 0; tn < 2; ++tn) mma_tile_smem(c[tn], s + (c0 + 16) + c0 * FLS, 1, FLS, xd + 8 * tn, XLD, 1, 16);
+  __syncwarp();
+#pragma unroll
+  for (int tn = 0; tn < 2; ++tn) {
+    int row = c0 + 16 + g, col = c0 + 8 * tn + 2 * t4;
+    s[row + col * FLS] = c[tn][0];
+    s[row + (col + 1) * FLS] = c[tn][1];
+    s[(row + 8) + col * FLS] = c[tn][2];
+    s[(row + 8) + (col + 1) * FLS] = c[tn][3];
+  }
+  __syncwarp();
+  // A22 −= L21 L21ᵀ (lower part)
+#pragma unroll
+  for (int tn = 0; tn < 2; ++tn) {
+    double u[4] = {0, 0, 0, 0};
+    mma_tile_smem(u, s + (c0 + 16) + c0 * FLS, 1, FLS, s + (c0 + 16 + 8 * tn) + c0 * FLS, FLS, 1, 16);
+    int i = g, j = 8 * tn + 2 * t4;  // within the 16×16 block
+    double* b = s + (c0 + 16) + (c0 + 16) * FLS;
+    if (i >= j) b[i + j * FLS] -= u[0];
+    if (i >= j + 1) b[i + (j + 1) * FLS] -= u[1];
+    if (i + 8 >= j) b[(i + 8) + j * FLS] -= u[2];
+    if (i + 8 >= j + 1) b[(i + 8) + (j + 1) * FLS] -= u[3];
+  }
+  __syncwarp();
+  f = leaf16_factor_inv(s, c0 + 16, xd + 16 + 16 * XLD);
+  if (f >= 0) return 16 + f;
+  // T = L21 · X11 into the (zero) upper-right quarter of xd, then
+  // X21 = −X22 · T, and the quarter back to zero
+  double* T = xd + 16 * XLD;  // rows 0..15, columns 16..31
+#pragma unroll
+  for (int tn = 0; tn < 2; ++tn) {
+    double u[4] = {0, 0, 0, 0};
+    mma_tile_smem(u, s + (c0 + 16) + c0 * FLS, 1, FLS, xd + 8 * tn * XLD, 1, XLD, 16);
+    int i = g, j = 8 * tn + 2 * t4;
+    T[i + j * XLD] = u[0];
+    T[i + (j + 1) * XLD] = u[1];
+    T[(i + 8) + j * XLD] = u[2];
+    T[(i + 8) + (j + 1) * XLD] = u[3];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int tn = 0; tn < 2; ++tn) {
+    double u[4] = {0, 0, 0, 0};
+    mma_tile_smem(u, xd + 16 + 16 * XLD, 1, XLD, T + 8 * tn * XLD, 1, XLD, 16);
+    int i = g, j = 8 * tn + 2 * t4;
+    double* X21 = xd + 16;
+    X21[i + j * XLD] = -u[0];
+    X21[i + (j + 1) * XLD] = -u[1];
+    X21[(i + 8) + j * XLD] = -u[2];
+    X21[(i + 8) + (j + 1) * XLD] = -u[3];
+  }
+  __syncwarp();
+  for (int e = lane; e < 256; e += 32) T[(e % 16) + (e / 16) * XLD] = 0.0;
+  __syncwarp();
   return -1;
 }
 
@@ -219,16 +295,31 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
   const int lane = tid & 31, g = lane >> 2, t4 = lane & 3;
   const int npad = (nb + SB - 1) / SB * SB;
   if (tid == 0) fail = -1;
-  // block load: every lower entry in flight at once (cp.async), padding after
-  for (int j = warp; j < nb; j += nw)
-    for (int i = j + lane; i < nb; i += 32) cp_async8(s + i + j * FLS, A + (k0 + i) + (k0 + j) * lda, true);
+  // block load: every lower entry in flight at once (16-byte cp.async pairs
+  // from the even row at or above the diagonal), then zero / pad
+  const bool vec = ((lda & 1) == 0) && ((((unsigned long long)(A + k0 + k0 * lda)) & 15) == 0);
+  for (int j = warp; j < nb; j += nw) {
+    if (vec) {
+      for (int i = (j & ~1) + 2 * lane; i < nb; i += 64) {
+        if (i + 1 < nb) {
+          unsigned sa = (unsigned)__cvta_generic_to_shared(s + i + j * FLS);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(A + (k0 + i) + (k0 + j) * lda));
+        } else {
+          cp_async8(s + i + j * FLS, A + (k0 + i) + (k0 + j) * lda, true);
+        }
+      }
+    } else {
+      for (int i = j + lane; i < nb; i += 32) cp_async8(s + i + j * FLS, A + (k0 + i) + (k0 + j) * lda, true);
+    }
+  }
   cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
   for (int e = tid; e < npad * npad; e += nt) {
     int i = e % npad, j = e / npad;
     if (i < j) s[i + j * FLS] = 0.0;
     else if (i >= nb || j >= nb) s[i + j * FLS] = (i == j) ? 1.0 : 0.0;
   }
-  cp_async_wait<0>();
   __syncthreads();
   const int np = npad / SB;
   if (warp == 0) {
@@ -272,15 +363,14 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
       }
     }
     __syncthreads();
-    // the next sub-panel's columns first (all warps) ...
-    diag_syrk_tiles(s, c0, r0, r0, r0 + SB, npad, 0, nw);
+    // trailing update (all warps), then warp 0 factors the next sub-panel
+    // alone: overlapping the two made the factor's dependent FP64 chain wait
+    // behind the other warps' DMMAs on the shared FP64 pipe
+    diag_syrk_tiles(s, c0, r0, r0, npad, npad, 0, nw);
     __syncthreads();
-    // ... then warp 0 factors it while the other warps update the rest
     if (warp == 0) {
       int f = warp_factor_inv32(s, r0, xd + (p + 1) * SB * XLD);
       if (f >= 0 && lane == 0) fail = r0 + f;
-    } else if (r0 + SB < npad) {
-      diag_syrk_tiles(s, c0, r0 + SB, r0 + SB, npad, npad, 1, nw - 1);
     }
     __syncthreads();
   }
@@ -399,6 +489,9 @@ static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double
   return cudaGetLastError();
 }
 
+// CTAs of the bulk trailing update in the look-ahead factor (of 148 SMs).
+constexpr int BULK_CTAS = 132;
+
 cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatus* st, cudaStream_t s,
                           FactorCtx* ctx) {
   CK(diag_attrs());
@@ -450,6 +543,7 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
       const double* Pk2 = A + c2 + (long long)k0 * ld;
       GemmParams ps = gemm_params(m, m, NB, Pk2, ld, Pk2, ld, A + c2 + (long long)c2 * ld, ld, -1.0, 1.0, st);
       ps.mode = GEMM_LOWER_TILES;
+      ps.max_ctas = BULK_CTAS;  // leave SMs free for the side stream's chain
       CK(dgemm(false, true, ps, s));
     }
     CK(cudaEventRecord(Es[k], s));

@@ -46,6 +46,8 @@ struct GemmParams {
   const DevStatus* status;
   // batched: pointer strides per blockIdx.z when splits == 1 and batch > 1
   long long strideA, strideB, strideC;
+  int max_ctas;             // > 0: at most this many CTAs, each looping over tiles
+  int splits_tiles;         // set by the launcher: tile count when max_ctas > 0
 };
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
@@ -88,14 +90,23 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES, TA, TB>::T
   using Cfg = GemmCfg<BM, BN, BK, WM, WN, STAGES, TA, TB>;
   extern __shared__ __align__(16) double smem[];
   if (dev_failed(p.status)) return;
+  const int ntiles_total = p.max_ctas > 0 ? p.max_ctas : 0;  // set by the launcher when capped
+  for (int tile_idx = blockIdx.x;; tile_idx += gridDim.x) {
+  if (p.max_ctas > 0) {
+    if (tile_idx >= p.splits_tiles) break;
+    __syncthreads();  // the previous tile's shared-memory reads are done
+  } else if (tile_idx != (int)blockIdx.x) {
+    break;
+  }
+  (void)ntiles_total;
 
   // ---- which output tile ----
   int tile_m, tile_n;
   const int tiles_m = (p.M + BM - 1) / BM;
   if (p.mode & GEMM_LOWER_TILES) {
-    // blockIdx.x enumerates (tm, tn) with the tile not strictly above the
+    // tile_idx enumerates (tm, tn) with the tile not strictly above the
     // diagonal; when row0 == col0 and BM == BN that is tn ≤ tm.
-    int idx = blockIdx.x;
+    int idx = tile_idx;
     // general enumeration: walk columns; tile (tm, tn) is kept when its last
     // global row ≥ its first global column.
     const int tiles_n = (p.N + BN - 1) / BN;
@@ -113,8 +124,8 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES, TA, TB>::T
     }
     if (tile_m < 0) return;
   } else {
-    tile_m = blockIdx.x % tiles_m;
-    tile_n = blockIdx.x / tiles_m;
+    tile_m = tile_idx % tiles_m;
+    tile_n = tile_idx / tiles_m;
   }
   const int m0 = tile_m * BM;
   const int n0 = tile_n * BN;
@@ -259,6 +270,7 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES, TA, TB>::T
         if (!split && p.beta != 0.0) v = fma(p.beta, *dst, v);
         *dst = v;
       }
+  }  // tile loop
 }
 
 // Host-side launcher for one configuration.
@@ -287,8 +299,11 @@ cudaError_t launch_dgemm(const GemmParams& p, int batch, cudaStream_t stream) {
   } else {
     nblocks = tiles_m * tiles_n;
   }
+  GemmParams q = p;
+  q.splits_tiles = nblocks;
+  if (p.max_ctas > 0 && nblocks > p.max_ctas) nblocks = p.max_ctas;
   dim3 grid(nblocks, 1, (p.mode & GEMM_SPLIT_K) ? p.splits : batch);
-  kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(p);
+  kern<<<grid, Cfg::THREADS, Cfg::SMEM, stream>>>(q);
   count_launch();
   return cudaGetLastError();
 }
