@@ -322,17 +322,16 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
   }
   __syncthreads();
   const int np = npad / SB;
-  if (warp == 0) {
-    int f = warp_factor_inv32(s, 0, xd);
-    if (f >= 0 && lane == 0) fail = f;
-  }
-  __syncthreads();
+  // one call site of the warp factor (a second inlined copy ran several times
+  // slower)
   for (int p = 0; p < np; ++p) {
-    if (fail >= 0) {
-      if (tid == 0) dev_fail(st, GPRX_CHOLESKY_FAILED, k0 + fail);
-      return;
-    }
     const int c0 = p * SB;
+    if (warp == 0) {
+      int f = warp_factor_inv32(s, c0, xd + p * SB * XLD);
+      if (f >= 0 && lane == 0) fail = c0 + f;
+    }
+    __syncthreads();
+    if (fail >= 0) break;
     const int r0 = c0 + SB, cnt = npad - r0;
     if (cnt <= 0) break;
     // P = A_below · X_ppᵀ: tiles (cnt/16) × 4, held in registers until all read
@@ -363,15 +362,8 @@ __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long 
       }
     }
     __syncthreads();
-    // trailing update (all warps), then warp 0 factors the next sub-panel
-    // alone: overlapping the two made the factor's dependent FP64 chain wait
-    // behind the other warps' DMMAs on the shared FP64 pipe
+    // trailing update of the rest of the block (all warps)
     diag_syrk_tiles(s, c0, r0, r0, npad, npad, 0, nw);
-    __syncthreads();
-    if (warp == 0) {
-      int f = warp_factor_inv32(s, r0, xd + (p + 1) * SB * XLD);
-      if (f >= 0 && lane == 0) fail = r0 + f;
-    }
     __syncthreads();
   }
   if (fail >= 0) {
