@@ -253,23 +253,37 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES, TA, TB>::T
   cp_async_wait<0>();
 
   // ---- epilogue ----
+  // Per m16 row group, every C value is loaded before any store of the group
+  // (a load after a store to a possibly aliasing address cannot be hoisted,
+  // and each would pay the full memory latency).
   const bool lower = (p.mode & GEMM_LOWER_TILES) != 0;
   const bool split = (p.mode & GEMM_SPLIT_K) != 0;
+  const bool use_beta = !split && p.beta != 0.0;
 #pragma unroll
-  for (int i = 0; i < Cfg::MT; ++i)
+  for (int i = 0; i < Cfg::MT; ++i) {
+    double cv[Cfg::NT][4];
+    bool ok[Cfg::NT][4];
 #pragma unroll
     for (int j = 0; j < Cfg::NT; ++j)
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         int row = m0 + wm * WM + i * 16 + g + ((r & 2) ? 8 : 0);
         int col = n0 + wn * WN + j * 8 + t4 * 2 + (r & 1);
-        if (row >= p.M || col >= p.N) continue;
-        if (lower && p.row0 + row < p.col0 + col) continue;
-        double* dst = C + row + (long long)col * p.ldc;
-        double v = p.alpha * acc[i][j][r];
-        if (!split && p.beta != 0.0) v = fma(p.beta, *dst, v);
-        *dst = v;
+        ok[j][r] = row < p.M && col < p.N && !(lower && p.row0 + row < p.col0 + col);
+        cv[j][r] = (use_beta && ok[j][r]) ? C[row + (long long)col * p.ldc] : 0.0;
       }
+#pragma unroll
+    for (int j = 0; j < Cfg::NT; ++j)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (!ok[j][r]) continue;
+        int row = m0 + wm * WM + i * 16 + g + ((r & 2) ? 8 : 0);
+        int col = n0 + wn * WN + j * 8 + t4 * 2 + (r & 1);
+        double v = p.alpha * acc[i][j][r];
+        if (use_beta) v = fma(p.beta, cv[j][r], v);
+        C[row + (long long)col * p.ldc] = v;
+      }
+  }
   }  // tile loop
 }
 
