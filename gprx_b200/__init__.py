@@ -16,6 +16,7 @@ from .api import (  # noqa: F401
     EmptyInput,
     Fixed,
     FittedGpr,
+    FittedSgpr,
     GaussianLikelihood,
     Gpr,
     GprError,
@@ -28,6 +29,7 @@ from .api import (  # noqa: F401
     NonFiniteInput,
     NonFiniteKernelValue,
     OnlineGpr,
+    OnlineSgpr,
     OptimizationNotConverged,
     OutOfDeviceMemory,
     PeriodicKernel,
@@ -37,6 +39,7 @@ from .api import (  # noqa: F401
     RbfArdKernel,
     RbfKernel,
     SeededRng,
+    Sgpr,
     ShapeMismatch,
     VarianceKind,
 )

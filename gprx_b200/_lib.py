@@ -104,6 +104,25 @@ _SIGS = {
     "gprx_online_delete": (C.c_int32, [C.c_void_p, C.c_uint64]),
     "gprx_online_n": (C.c_uint64, [C.c_void_p]),
     "gprx_online_point_ids": (C.c_int32, [C.c_void_p, U64, C.c_uint64]),
+    "gprx_sgpr_create": (C.c_int32, [D, C.c_uint64, C.c_uint64, D, D, C.c_uint64, C.POINTER(KernelNode), C.c_int32,
+                                     D, C.c_int32, C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    "gprx_sgpr_destroy": (C.c_int32, [C.c_void_p]),
+    "gprx_sgpr_num_params": (C.c_uint64, [C.c_void_p]),
+    "gprx_sgpr_get_params": (C.c_int32, [C.c_void_p, D, C.c_uint64]),
+    "gprx_sgpr_factor": (C.c_int32, [C.c_void_p]),
+    "gprx_sgpr_eval": (C.c_int32, [C.c_void_p, D, C.c_uint64, D, D]),
+    "gprx_sgpr_nlml": (C.c_int32, [C.c_void_p, D]),
+    "gprx_sgpr_predict": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
+    "gprx_sgpr_fit": (C.c_int32, [C.c_void_p, C.POINTER(LbfgsOptions), C.POINTER(FitReport)]),
+    "gprx_sgpr_insert": (C.c_int32, [C.c_void_p, D, C.c_double, U64]),
+    "gprx_sgpr_delete": (C.c_int32, [C.c_void_p, C.c_uint64]),
+    "gprx_sgpr_n": (C.c_uint64, [C.c_void_p]),
+    "gprx_sgpr_last_step_in_place": (C.c_int32, [C.c_void_p]),
+    "gprx_sgpr_point_ids": (C.c_int32, [C.c_void_p, U64, C.c_uint64]),
+    "gprx_sgpr_set_inducing": (C.c_int32, [C.c_void_p, D, C.c_uint64]),
+    "gprx_sgpr_kmm_jitter": (C.c_int32, [C.c_void_p, D]),
+    "gprx_sgpr_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "gprx_sgpr_stage_times": (C.c_int32, [C.c_void_p, D]),
     "gprx_probe_dgemm": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
     "gprx_probe_potrf": (C.c_int32, [C.c_int32, C.c_int32, D]),
     "gprx_rng_seed": (None, [C.POINTER(Rng), C.c_uint64]),

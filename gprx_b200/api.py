@@ -541,6 +541,168 @@ class OnlineGpr(FittedGpr):
 
 
 # ---------------------------------------------------------------------------
+# VFE sparse GPR (src/sgpr/)
+# ---------------------------------------------------------------------------
+class Sgpr:
+    """VFE sparse GPR trainer (src/sgpr/model.rs:448-579).  The K_mm factor
+    retries with JitterPolicy::adaptive(1e-8, 10, 5, 1e-3) by default."""
+
+    def __init__(self, kernel, likelihood, optimizer=None, precision=Precision.Fp64, device=0):
+        self.kernel = kernel
+        self.likelihood = likelihood
+        self.optimizer = optimizer if optimizer is not None else Lbfgs()
+        self.precision = Precision(precision)
+        self.device = device
+
+    def with_optimizer(self, opt):
+        return Sgpr(self.kernel, self.likelihood, opt, self.precision, self.device)
+
+    def _create(self, x, n_rows, n_cols, y, z, m):
+        x = _check_points(x, n_rows, n_cols)
+        z = _check_points(z, m, n_cols)
+        y = L.f64(y)
+        if y.size != n_rows:
+            raise ShapeMismatch("y has %d values, expected %d" % (y.size, n_rows))
+        if not np.all(np.isfinite(y)):
+            raise NonFiniteInput("non-finite y")
+        nodes, nn = self.kernel.node_array()
+        theta = L.f64(self.kernel.get_params() + [self.likelihood.log_noise_variance])
+        o = L.Options()
+        L.lib().gprx_options_default_sparse(C.byref(o))
+        o.precision = int(self.precision)
+        o.device = int(self.device)
+        h = C.c_void_p()
+        check(L.lib().gprx_sgpr_create(L.ptr(x), n_rows, n_cols, L.ptr(y), L.ptr(z), m, nodes, nn, L.ptr(theta),
+                                       theta.size, C.byref(o), C.byref(h)))
+        return FittedSgpr(h, n_cols)
+
+    def factor(self, x, n_rows, n_cols, y, z, m):
+        f = self._create(x, n_rows, n_cols, y, z, m)
+        check(L.lib().gprx_sgpr_factor(f._h))
+        return f
+
+    def fit(self, x, n_rows, n_cols, y, z, m):
+        f = self._create(x, n_rows, n_cols, y, z, m)
+        if isinstance(self.optimizer, Fixed):
+            check(L.lib().gprx_sgpr_factor(f._h))
+            return f
+        rep = L.FitReport()
+        opt = self.optimizer._c()
+        check(L.lib().gprx_sgpr_fit(f._h, C.byref(opt), C.byref(rep)))
+        f.report = rep
+        return f
+
+
+class FittedSgpr:
+    """An assembled VFE model (src/sgpr/fitted.rs)."""
+
+    def __init__(self, handle, d):
+        self._h = handle
+        self.d = d
+        self.report = None
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            try:
+                L.lib().gprx_sgpr_destroy(self._h)
+            except Exception:
+                pass
+            self._h = None
+
+    def num_params(self):
+        return int(L.lib().gprx_sgpr_num_params(self._h))
+
+    def get_params(self):
+        p = np.zeros(self.num_params())
+        check(L.lib().gprx_sgpr_get_params(self._h, L.ptr(p), p.size))
+        return p
+
+    def value_and_gradient(self, params):
+        p = L.f64(params)
+        v = np.zeros(1)
+        g = np.zeros(p.size)
+        check(L.lib().gprx_sgpr_eval(self._h, L.ptr(p), p.size, L.ptr(v), L.ptr(g)))
+        return float(v[0]), g
+
+    def value(self, params):
+        p = L.f64(params)
+        v = np.zeros(1)
+        check(L.lib().gprx_sgpr_eval(self._h, L.ptr(p), p.size, L.ptr(v), None))
+        return float(v[0])
+
+    def neg_log_marginal_likelihood(self):
+        v = np.zeros(1)
+        check(L.lib().gprx_sgpr_nlml(self._h, L.ptr(v)))
+        return float(v[0])
+
+    def kmm_jitter(self):
+        v = np.zeros(1)
+        check(L.lib().gprx_sgpr_kmm_jitter(self._h, L.ptr(v)))
+        return float(v[0])
+
+    def n(self):
+        return int(L.lib().gprx_sgpr_n(self._h))
+
+    def predict(self, xs, n_rows, n_cols):
+        return self.predict_with(xs, n_rows, n_cols, PredictOptions())
+
+    def predict_with(self, xs, n_rows, n_cols, options):
+        if n_cols != self.d:
+            raise ShapeMismatch("query has %d features, model has %d" % (n_cols, self.d))
+        xs = L.f64(xs)
+        mean = np.zeros(n_rows)
+        var = np.zeros(n_rows)
+        check(L.lib().gprx_sgpr_predict(self._h, L.ptr(xs), n_rows, int(options.variance_kind), L.ptr(mean),
+                                        L.ptr(var)))
+        return Prediction(mean, var, options.variance_kind)
+
+    def stream_ptr(self):
+        s = C.c_void_p()
+        check(L.lib().gprx_sgpr_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    def stage_times_ms(self):
+        out = np.zeros(3)
+        check(L.lib().gprx_sgpr_stage_times(self._h, L.ptr(out)))
+        return dict(zip(("kmm_and_a", "b_and_sums", "gradient"), out))
+
+    def into_online(self):
+        """FittedSgpr::into_online: the same device state, now updatable."""
+        on = OnlineSgpr(self._h, self.d)
+        self._h = None
+        return on
+
+
+class OnlineSgpr(FittedSgpr):
+    """VFE model with O(m²) point insert / delete (src/sgpr/online/mod.rs)."""
+
+    def insert(self, x_new, y_new):
+        x = L.f64(x_new)
+        if x.size != self.d:
+            raise ShapeMismatch("point has %d features, model has %d" % (x.size, self.d))
+        pid = C.c_uint64(0)
+        check(L.lib().gprx_sgpr_insert(self._h, L.ptr(x), float(y_new), C.byref(pid)))
+        return int(pid.value)
+
+    def delete(self, point_id):
+        check(L.lib().gprx_sgpr_delete(self._h, int(point_id)))
+
+    def point_ids(self):
+        n = self.n()
+        out = np.zeros(n, dtype=np.uint64)
+        check(L.lib().gprx_sgpr_point_ids(self._h, out.ctypes.data_as(L.U64), n))
+        return out
+
+    def last_step_in_place(self):
+        return bool(L.lib().gprx_sgpr_last_step_in_place(self._h))
+
+    def set_inducing(self, z, m):
+        """Replace the inducing set (inducing insert / delete by reassembly)."""
+        z = _check_points(z, m, self.d)
+        check(L.lib().gprx_sgpr_set_inducing(self._h, L.ptr(z), m))
+
+
+# ---------------------------------------------------------------------------
 # seeded RNG (src/rng.rs)
 # ---------------------------------------------------------------------------
 class SeededRng:

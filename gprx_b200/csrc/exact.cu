@@ -113,7 +113,7 @@ gprx_status ExactState::read_status(DevStatus* out) {
 
 gprx_status ExactState::enqueue_factor(double j) {
   GPRX_CUDA_TRY(cudaEventRecord(ev[0], stream));
-  GPRX_CUDA_TRY(fill_lower(kern, x.p, n, A.p, ld, noise() + j, status.p, stream));
+  GPRX_CUDA_TRY(fill_lower(kern, x.p, cap, n, A.p, ld, noise() + j, status.p, stream));
   GPRX_CUDA_TRY(cudaEventRecord(ev[1], stream));
   GPRX_CUDA_TRY(potrf_blocked(A.p, ld, n, linv.p, status.p, stream, &fctx));
   GPRX_CUDA_TRY(cudaEventRecord(ev[2], stream));

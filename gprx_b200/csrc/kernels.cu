@@ -242,8 +242,9 @@ __device__ __forceinline__ double pair_value(const KTree& t, const double* xi, c
 }
 
 template <int ARD_D>
-__global__ void __launch_bounds__(FILL_THREADS) fill_lower_kernel(KTree t, const double* x, int n, double* K,
-                                                                  long long ld, double diag_add, DevStatus* st) {
+__global__ void __launch_bounds__(FILL_THREADS) fill_lower_kernel(KTree t, const double* x, long long ldx, int n,
+                                                                  double* K, long long ld, double diag_add,
+                                                                  DevStatus* st) {
   __shared__ double xi[GPRX_MAX_DIM * FT];
   __shared__ double xj[GPRX_MAX_DIM * FT];
   if (dev_failed(st)) return;
@@ -258,8 +259,8 @@ __global__ void __launch_bounds__(FILL_THREADS) fill_lower_kernel(KTree t, const
     __syncthreads();
     for (int e = threadIdx.x; e < d * FT; e += blockDim.x) {
       int r = e % FT, f = e / FT;
-      xi[f * FT + r] = (i0 + r < n) ? x[(i0 + r) + (long long)f * n] : 0.0;
-      xj[f * FT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * n] : 0.0;
+      xi[f * FT + r] = (i0 + r < n) ? x[(i0 + r) + (long long)f * ldx] : 0.0;
+      xj[f * FT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * ldx] : 0.0;
     }
     __syncthreads();
     const int r = threadIdx.x % FT;
@@ -314,16 +315,16 @@ static int fill_grid(long long ntiles) {
   return (int)std::max<long long>(1, std::min(ntiles, cap));
 }
 
-cudaError_t fill_lower(const HostKernel& k, const double* x, int n, double* K, long long ld, double diag_add,
-                       DevStatus* st, cudaStream_t s) {
+cudaError_t fill_lower(const HostKernel& k, const double* x, long long ldx, int n, double* K, long long ld,
+                       double diag_add, DevStatus* st, cudaStream_t s) {
   int nt = (n + FT - 1) / FT;
   int grid = fill_grid((long long)nt * (nt + 1) / 2);
   switch (k.ard_d) {
-    case 0: GPRX_LAUNCH(fill_lower_kernel<0>, grid, FILL_THREADS, 0, s, k.tree, x, n, K, ld, diag_add, st); break;
-    case 4: GPRX_LAUNCH(fill_lower_kernel<4>, grid, FILL_THREADS, 0, s, k.tree, x, n, K, ld, diag_add, st); break;
-    case 8: GPRX_LAUNCH(fill_lower_kernel<8>, grid, FILL_THREADS, 0, s, k.tree, x, n, K, ld, diag_add, st); break;
-    case 16: GPRX_LAUNCH(fill_lower_kernel<16>, grid, FILL_THREADS, 0, s, k.tree, x, n, K, ld, diag_add, st); break;
-    default: GPRX_LAUNCH(fill_lower_kernel<32>, grid, FILL_THREADS, 0, s, k.tree, x, n, K, ld, diag_add, st); break;
+    case 0: GPRX_LAUNCH(fill_lower_kernel<0>, grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
+    case 4: GPRX_LAUNCH(fill_lower_kernel<4>, grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
+    case 8: GPRX_LAUNCH(fill_lower_kernel<8>, grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
+    case 16: GPRX_LAUNCH(fill_lower_kernel<16>, grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
+    default: GPRX_LAUNCH(fill_lower_kernel<32>, grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
   }
   return cudaGetLastError();
 }

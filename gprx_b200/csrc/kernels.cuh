@@ -30,9 +30,10 @@ struct HostKernel {
 constexpr int GRAD_SLOTS_LEAF = KT_MAX_LEAVES * KT_ACC_PER_LEAF;  // 16
 inline int grad_slots(int ard_d) { return GRAD_SLOTS_LEAF + (ard_d > 0 ? ard_d : 1) + 1; }  // + noise slot
 
-// K(X, X) lower triangle (+ diag_add on the diagonal) into K (n×n, ld).
-cudaError_t fill_lower(const HostKernel& k, const double* x, int n, double* K, long long ld, double diag_add,
-                       DevStatus* st, cudaStream_t s);
+// K(X, X) lower triangle (+ diag_add on the diagonal) into K (n×n, ld); X is
+// n×d with leading dimension ldx.
+cudaError_t fill_lower(const HostKernel& k, const double* x, long long ldx, int n, double* K, long long ld,
+                       double diag_add, DevStatus* st, cudaStream_t s);
 // K(X1, X2): n1×n2 into out (ld ≥ n1).  X1 is n1×d, X2 is n2×d (column-major,
 // leading dimensions ldx1 / ldx2).
 cudaError_t fill_cross(const HostKernel& k, const double* x1, long long ldx1, int n1, const double* x2,

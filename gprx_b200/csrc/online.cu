@@ -54,7 +54,7 @@ __global__ void ldlt_border_kernel(double* A, long long ld, int n, const double*
 
 // Rank-1 update L D Lᵀ + a·w wᵀ of the trailing block starting at row/col r0
 // (size m), with w = L[r0.., idx] and a = D_idx.  Single CTA, 1024 threads.
-constexpr int R1_THREADS = 1024;
+constexpr int R1_THREADS = 256;
 __global__ void __launch_bounds__(R1_THREADS) ldlt_rank1_kernel(double* A, long long ld, int r0, int m, int idx,
                                                                  DevStatus* st) {
   __shared__ double P[32], Bt[32];

@@ -211,6 +211,55 @@ uint64_t gprx_online_n(const gprx_exact* h);
 gprx_status gprx_online_point_ids(gprx_exact* h, uint64_t* out, uint64_t n);
 
 /* ------------------------------------------------------------------ */
+/* VFE sparse GPR (src/sgpr/)                                           */
+/* ------------------------------------------------------------------ */
+typedef struct gprx_sgpr gprx_sgpr;
+
+/* Uploads X (n×d), y and the inducing points Z (m×d); SparseCore::prepare
+ * (src/sparse/core.rs:314).  No assembly yet. */
+gprx_status gprx_sgpr_create(const double* x, uint64_t n, uint64_t d, const double* y,
+                             const double* z, uint64_t m,
+                             const gprx_kernel_node* nodes, int32_t n_nodes,
+                             const double* theta, int32_t n_theta,
+                             const gprx_options* options, gprx_sgpr** out);
+gprx_status gprx_sgpr_destroy(gprx_sgpr* h);
+uint64_t gprx_sgpr_num_params(const gprx_sgpr* h);
+gprx_status gprx_sgpr_get_params(gprx_sgpr* h, double* out, uint64_t p);
+/* assemble_vfe at the stored θ (src/sgpr/factor/vfe.rs:191-277). */
+gprx_status gprx_sgpr_factor(gprx_sgpr* h);
+/* FittedSgpr::value_and_gradient_into (src/sgpr/fitted.rs:306-326):
+ * reassembly, vfe_neg_log_marginal_likelihood (vfe.rs:338-369) and
+ * analytic_gradient (derivatives.rs:283-366).  `grad` may be NULL. */
+gprx_status gprx_sgpr_eval(gprx_sgpr* h, const double* params, uint64_t p, double* nlml, double* grad);
+gprx_status gprx_sgpr_nlml(gprx_sgpr* h, double* nlml);
+/* vfe_predict_into / vfe_latent (src/sgpr/factor/predict.rs:102-262). */
+gprx_status gprx_sgpr_predict(gprx_sgpr* h, const double* xs, uint64_t q, int32_t variance_kind,
+                              double* mean, double* var);
+gprx_status gprx_sgpr_fit(gprx_sgpr* h, const gprx_lbfgs_options* opt, gprx_fit_report* report);
+/* OnlineSgpr::insert → append_point (src/sgpr/online/mod.rs:1695-1810). */
+gprx_status gprx_sgpr_insert(gprx_sgpr* h, const double* x_new, double y_new, uint64_t* id);
+/* OnlineSgpr::delete (src/sgpr/online/mod.rs:903-1000): rank-1 downdate of L_B,
+ * reassembly when the downdate fails or the pivot gate does not hold. */
+gprx_status gprx_sgpr_delete(gprx_sgpr* h, uint64_t id);
+uint64_t gprx_sgpr_n(const gprx_sgpr* h);
+/* 1 when the last insert/delete updated in place, 0 when it reassembled. */
+int32_t gprx_sgpr_last_step_in_place(const gprx_sgpr* h);
+/* PointIds in registry order (src/points.rs:76). */
+gprx_status gprx_sgpr_point_ids(gprx_sgpr* h, uint64_t* out, uint64_t n);
+/* Replaces the inducing set Z (m×d) and reassembles: an inducing insert or
+ * delete (OnlineSgpr::insert_inducing / delete_inducing, src/sgpr/online/mod.rs:1301,1943)
+ * taken by reassembly. */
+gprx_status gprx_sgpr_set_inducing(gprx_sgpr* h, const double* z, uint64_t m);
+/* jitter j the K_mm factor took. */
+gprx_status gprx_sgpr_kmm_jitter(gprx_sgpr* h, double* jitter);
+/* The CUDA stream (a cudaStream_t) of the handle, for event timing. */
+gprx_status gprx_sgpr_stream(gprx_sgpr* h, void** stream);
+/* Device time of the last assembly / gradient in ms: [K_mm + A, B + sums, gradient]. */
+gprx_status gprx_sgpr_stage_times(gprx_sgpr* h, double* out3);
+
+
+
+/* ------------------------------------------------------------------ */
 /* device microbenchmarks (diagnostics; no gprx counterpart)            */
 /* ------------------------------------------------------------------ */
 /* ms per launch of the FP64 DMMA GEMM C(m×n) = op(A)·op(B), k deep. */
