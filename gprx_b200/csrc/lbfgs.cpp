@@ -157,6 +157,22 @@ bool MoreThuente::start(double f0, double g0, double stp) {
 
 MoreThuente::Result MoreThuente::step(double f, double g) {
   ++nfev_;
+  if (!(f < 0.5 * BARRIER_COST)) {
+    // A point that cannot be evaluated: its cost carries no slope to
+    // interpolate (the cubic step cancels to zero), so the interval closes on
+    // it and the next trial moves a quarter of the way back toward the best
+    // point so far.
+    if (nfev_ >= max_evals) return STOP;
+    brackt_ = true;
+    sty_ = stp_;
+    fy_ = f;
+    gy_ = 0.0;
+    stmin_ = std::min(stx_, sty_);
+    stmax_ = std::max(stx_, sty_);
+    stp_ = stx_ + 0.25 * (stp_ - stx_);
+    if (std::fabs(stp_ - stx_) <= xtol * std::max(std::fabs(stx_), 1e-300)) return STOP;
+    return CONTINUE;
+  }
   double ftest = finit_ + stp_ * gtest_;
   if (stage_ == 1 && f <= ftest && g >= 0.0) stage_ = 2;
   if (brackt_ && (stp_ <= stmin_ || stp_ >= stmax_)) return STOP;
