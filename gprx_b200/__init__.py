@@ -10,6 +10,7 @@ and a CUDA device, and fails loudly otherwise.
 from .api import (  # noqa: F401
     CholeskyFailed,
     CholeskyStage,
+    BatchFit,
     ConstantKernel,
     CudaError,
     DeviceTimeout,
@@ -19,6 +20,7 @@ from .api import (  # noqa: F401
     FittedSgpr,
     GaussianLikelihood,
     Gpr,
+    GprBatch,
     GprError,
     IndexOutOfRange,
     InsufficientData,

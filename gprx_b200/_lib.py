@@ -123,6 +123,13 @@ _SIGS = {
     "gprx_sgpr_kmm_jitter": (C.c_int32, [C.c_void_p, D]),
     "gprx_sgpr_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "gprx_sgpr_stage_times": (C.c_int32, [C.c_void_p, D]),
+    "gprx_batch_create": (C.c_int32, [D, D, U64, C.c_uint64, C.c_uint64, C.POINTER(KernelNode), C.c_int32,
+                                      C.c_int32, C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    "gprx_batch_destroy": (C.c_int32, [C.c_void_p]),
+    "gprx_batch_num_params": (C.c_uint64, [C.c_void_p]),
+    "gprx_batch_eval": (C.c_int32, [C.c_void_p, D, C.c_uint64, D, D, I32]),
+    "gprx_batch_fit": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.POINTER(LbfgsOptions), D, C.POINTER(FitReport),
+                                   I32]),
     "gprx_probe_dgemm": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
     "gprx_probe_potrf": (C.c_int32, [C.c_int32, C.c_int32, D]),
     "gprx_rng_seed": (None, [C.POINTER(Rng), C.c_uint64]),

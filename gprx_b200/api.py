@@ -703,6 +703,94 @@ class OnlineSgpr(FittedSgpr):
 
 
 # ---------------------------------------------------------------------------
+# batched exact GPR: many independent problems sharing one kernel tree
+# ---------------------------------------------------------------------------
+class BatchFit:
+    """Per-problem results of GprBatch.fit."""
+
+    def __init__(self, params, nlml, iterations, evaluations, grad_norm, converged, status):
+        self.params = params            # n_problems × p, log space
+        self.nlml = nlml
+        self.iterations = iterations
+        self.evaluations = evaluations
+        self.grad_norm = grad_norm
+        self.converged = converged
+        self.status = status            # gprx_status per problem (0 = ok)
+
+
+class GprBatch:
+    """Independent exact GPs that share a kernel tree and d, evaluated in one
+    persistent device launch per round; each problem is what Gpr does for one
+    model (value_and_gradient, fit by L-BFGS).
+
+    xs, ys: lists of per-problem arrays (x_i column-major n_i × d, y_i of n_i).
+    """
+
+    def __init__(self, kernel, xs, ys, d, jitter=None, device=0):
+        self.kernel = kernel.copy()
+        self.d = int(d)
+        if len(xs) != len(ys) or len(xs) == 0:
+            raise ShapeMismatch("xs and ys must be non-empty lists of the same length")
+        ns = np.array([np.asarray(y).size for y in ys], dtype=np.uint64)
+        x = np.concatenate([_check_points(xi, int(n), self.d) for xi, n in zip(xs, ns)])
+        y = np.concatenate([L.f64(yi) for yi in ys])
+        self.n = ns
+        o = L.Options()
+        L.lib().gprx_options_default(C.byref(o))
+        o.device = int(device)
+        if jitter is not None:
+            o.jitter_kind, o.jitter_initial, o.jitter_multiplier, o.jitter_max_retries, o.jitter_max = jitter
+        nodes, nn = self.kernel.node_array()
+        self.p = self.kernel.num_params() + 1
+        h = C.c_void_p()
+        check(L.lib().gprx_batch_create(L.ptr(x), L.ptr(y), ns.ctypes.data_as(L.U64), ns.size, self.d, nodes, nn,
+                                        self.p, C.byref(o), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                L.lib().gprx_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def n_problems(self):
+        return int(self.n.size)
+
+    def _params(self, params):
+        a = np.ascontiguousarray(np.asarray(params, dtype=np.float64))
+        if a.shape != (self.n_problems, self.p):
+            raise ShapeMismatch("params must be n_problems × %d" % self.p)
+        return a
+
+    def value_and_gradient(self, params):
+        """NLML, gradient and status of every problem at its own θ (row i)."""
+        a = self._params(params)
+        nl = np.zeros(self.n_problems)
+        g = np.zeros((self.n_problems, self.p))
+        st = np.zeros(self.n_problems, dtype=np.int32)
+        check(L.lib().gprx_batch_eval(self._h, L.ptr(a), self.p, L.ptr(nl), g.ctypes.data_as(L.D),
+                                      st.ctypes.data_as(L.I32)))
+        return nl, g, st
+
+    def fit(self, params0, optimizer=None):
+        """Fits every problem by L-BFGS (the optimizers run on the device)."""
+        a = self._params(params0)
+        opt = (optimizer if optimizer is not None else Lbfgs())._c()
+        out = np.zeros_like(a)
+        reps = (L.FitReport * self.n_problems)()
+        st = np.zeros(self.n_problems, dtype=np.int32)
+        check(L.lib().gprx_batch_fit(self._h, L.ptr(a), self.p, C.byref(opt), out.ctypes.data_as(L.D), reps,
+                                     st.ctypes.data_as(L.I32)))
+        return BatchFit(out, np.array([r.nlml for r in reps]), np.array([r.iterations for r in reps]),
+                        np.array([r.evaluations for r in reps]), np.array([r.grad_norm for r in reps]),
+                        np.array([r.converged for r in reps], dtype=bool), st)
+
+
+# ---------------------------------------------------------------------------
 # seeded RNG (src/rng.rs)
 # ---------------------------------------------------------------------------
 class SeededRng:

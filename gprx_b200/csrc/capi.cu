@@ -6,7 +6,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <new>
+#include <string>
 
 #include "exact.cuh"
 #include "lbfgs.h"
@@ -76,14 +78,17 @@ gprx_status fit_lbfgs(void* ctx, EvalFn eval, int p, const double* theta0, const
     return set_error(GPRX_INVALID_CONFIG, "parameter interval must be 0 < lo < hi");
   if (!(opt.tolerance >= 0.0) || !std::isfinite(opt.tolerance))
     return set_error(GPRX_INVALID_CONFIG, "L-BFGS gradient tolerance must be finite and >= 0");
+  if (p > LBFGS_HOST_VARS) return set_error(GPRX_INVALID_CONFIG, "too many parameters for the optimizer");
+  if (opt.history_size > LBFGS_HOST_HISTORY)
+    return set_error(GPRX_INVALID_CONFIG, "L-BFGS history must be at most " + std::to_string(LBFGS_HOST_HISTORY));
   LogitMap map;
-  map.init(p, opt.interval_lo, opt.interval_hi);
+  map.init(opt.interval_lo, opt.interval_hi);
   LbfgsConfig cfg;
   cfg.history = opt.history_size > 0 ? opt.history_size : 10;
   cfg.max_iterations = opt.max_iterations;
   cfg.tol_grad = opt.tolerance;
   std::vector<double> z0(p);
-  if (!map.from_log(theta0, z0.data())) return set_error(GPRX_INVALID_HYPERPARAMETER, "initial θ outside the interval");
+  if (!map.from_log(theta0, p, z0.data())) return set_error(GPRX_INVALID_HYPERPARAMETER, "initial θ outside the interval");
   std::vector<double> logt(p), jac(p), g(p);
   double best_f = BARRIER_COST;
   std::vector<double> best_z;
@@ -103,15 +108,16 @@ gprx_status fit_lbfgs(void* ctx, EvalFn eval, int p, const double* theta0, const
         double u = gprx_rng_unit(&rng);
         const double eps = 1.0 / 9007199254740992.0;
         u = std::min(std::max(u, eps), 1.0 - eps);
-        double lt = map.ln_lo[i] + u * (map.ln_hi[i] - map.ln_lo[i]);
-        map.from_log(&lt, &zs[i]);
+        double lt = map.ln_lo + u * (map.ln_hi - map.ln_lo);
+        map.from_log(&lt, 1, &zs[i]);
       }
     }
-    LbfgsRC lb;
+    std::unique_ptr<HostLbfgs> lbp(new HostLbfgs());
+    HostLbfgs& lb = *lbp;
     lb.start(cfg, zs.data(), p);
     gprx_status last = GPRX_OK;
-    while (lb.task() == LbfgsRC::EVALUATE) {
-      map.to_log(lb.point().data(), logt.data(), jac.data());
+    while (lb.task() == HostLbfgs::EVALUATE) {
+      map.to_log(lb.point(), p, logt.data(), jac.data());
       double f;
       gprx_status st = eval(ctx, logt.data(), &f, g.data());
       if (st == GPRX_CUDA_ERROR || st == GPRX_OUT_OF_MEMORY || st == GPRX_TIMEOUT) return st;
@@ -127,7 +133,7 @@ gprx_status fit_lbfgs(void* ctx, EvalFn eval, int p, const double* theta0, const
     total_evals += lb.evaluations();
     if (lb.best_value() < best_f) {
       best_f = lb.best_value();
-      best_z = lb.best();
+      best_z.assign(lb.best(), lb.best() + p);
       iters = lb.iterations();
       gnorm = lb.grad_norm();
       conv = lb.converged();
@@ -141,7 +147,7 @@ gprx_status fit_lbfgs(void* ctx, EvalFn eval, int p, const double* theta0, const
     return st;
   }
   best_theta.resize(p);
-  map.to_log(best_z.data(), best_theta.data(), nullptr);
+  map.to_log(best_z.data(), p, best_theta.data(), nullptr);
   if (rep) {
     rep->nlml = best_f;
     rep->iterations = iters;

@@ -75,6 +75,62 @@ struct KTree {
   double diag_value;          // k(x, x) (stationary: the same for every x)
 };
 
+#ifndef GPRX_HD
+#define GPRX_HD __host__ __device__
+#endif
+
+// Derived constants of every leaf from θ (log space, depth-first order) and
+// k(x, x).  Returns GPRX_OK or GPRX_INVALID_HYPERPARAMETER.  Host and device
+// use the same formulas (rbf.rs:18, constant.rs:12, periodic.rs:598-638,
+// rbf_ard.rs:16).
+GPRX_HD inline int kt_set_theta(KTree& t, const double* th) {
+  for (int i = 0; i < t.n_params; ++i)
+    if (!isfinite(th[i])) return GPRX_INVALID_HYPERPARAMETER;
+  double v0[KT_MAX_LEAVES];
+  for (int l = 0; l < t.n_leaves; ++l) {
+    KLeaf& lf = t.leaf[l];
+    const double* p = th + lf.param;
+    switch (lf.kind) {
+      case GPRX_LEAF_RBF: {
+        double ell = exp(p[0]);
+        lf.c0 = 0.5 / (ell * ell);
+        v0[l] = 1.0;
+        break;
+      }
+      case GPRX_LEAF_CONSTANT:
+        lf.c0 = exp(p[0]);
+        v0[l] = lf.c0;
+        break;
+      case GPRX_LEAF_PERIODIC: {
+        double ell = exp(p[0]), per = exp(p[1]);
+        lf.c0 = M_PI / per;
+        lf.c1 = 1.0 / (ell * ell);
+        v0[l] = 1.0;
+        break;
+      }
+      case GPRX_LEAF_RBF_ARD:
+        for (int f = 0; f < t.d; ++f) {
+          double ell = exp(p[f]);
+          t.inv_ell2[f] = 1.0 / (ell * ell);
+        }
+        v0[l] = 1.0;
+        break;
+      default:
+        v0[l] = 0.0;
+    }
+    if (!isfinite(lf.c0) || !isfinite(lf.c1)) return GPRX_INVALID_HYPERPARAMETER;
+  }
+  double k0 = 0.0;
+  for (int tt = 0; tt < t.n_terms; ++tt) {
+    double pr = 1.0;
+    for (int l = 0; l < t.n_leaves; ++l)
+      if ((t.term_mask[tt] >> l) & 1u) pr *= v0[l];
+    k0 += pr;
+  }
+  t.diag_value = k0;
+  return GPRX_OK;
+}
+
 // Leaf values at one pair.  dx[f] = x1_f − x2_f.
 template <int ARD_D>
 __device__ __forceinline__ void kt_leaf_values(const KTree& t, const double* dx, double r2,

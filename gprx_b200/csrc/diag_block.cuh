@@ -42,7 +42,7 @@ __device__ __forceinline__ void mma_tile_smem(double (&c)[4], const double* a, i
 // back to s and L⁻¹ (column-major, ld XLD) to xo.  Returns the failing column
 // or −1.  Kept out of line so one compact copy serves every call (the fully
 // unrolled 32-wide form overflowed the instruction cache).
-__device__ __noinline__ int leaf16_factor_inv(double* s, int off, double* xo) {
+static __device__ __noinline__ int leaf16_factor_inv(double* s, int off, double* xo) {
   const int lane = threadIdx.x & 31, r = lane & 15;
   double d[16];
 #pragma unroll
@@ -184,7 +184,7 @@ __device__ __forceinline__ void diag_syrk_tiles(double* s, int c0, int rlo, int 
 // (L⁻¹ into linv, ld NB_DIAG, zero above the diagonal; it also stays in smem[0 ..
 // NB_DIAG·FLS) with ld FLS).  fail_sh is a shared int.  Returns the failing column
 // (uniform over the CTA) or −1.
-__device__ int diag_block_factor_inv(double* A, long long lda, long long k0, int nb, double* linv, double* smem,
+static __device__ int diag_block_factor_inv(double* A, long long lda, long long k0, int nb, double* linv, double* smem,
                                      int* fail_sh) {
   int& fail = *fail_sh;
   double* s = smem;                       // NB_DIAG × FLS

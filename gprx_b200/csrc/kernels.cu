@@ -163,50 +163,7 @@ gprx_status HostKernel::set_theta(const double* th) {
   for (int i = 0; i < n_params; ++i)
     if (!std::isfinite(th[i])) return GPRX_INVALID_HYPERPARAMETER;
   theta.assign(th, th + n_params);
-  double v0[KT_MAX_LEAVES];
-  for (int l = 0; l < tree.n_leaves; ++l) {
-    KLeaf& lf = tree.leaf[l];
-    const double* p = theta.data() + lf.param;
-    switch (lf.kind) {
-      case GPRX_LEAF_RBF: {
-        double ell = std::exp(p[0]);
-        lf.c0 = 0.5 / (ell * ell);
-        v0[l] = 1.0;
-        break;
-      }
-      case GPRX_LEAF_CONSTANT:
-        lf.c0 = std::exp(p[0]);
-        v0[l] = lf.c0;
-        break;
-      case GPRX_LEAF_PERIODIC: {
-        double ell = std::exp(p[0]), per = std::exp(p[1]);
-        lf.c0 = M_PI / per;
-        lf.c1 = 1.0 / (ell * ell);
-        v0[l] = 1.0;
-        break;
-      }
-      case GPRX_LEAF_RBF_ARD:
-        for (int f = 0; f < d; ++f) {
-          double ell = std::exp(p[f]);
-          tree.inv_ell2[f] = 1.0 / (ell * ell);
-        }
-        v0[l] = 1.0;
-        break;
-    }
-    for (int f = 0; f < 2; ++f) {
-      (void)f;
-    }
-    if (!std::isfinite(lf.c0) || !std::isfinite(lf.c1)) return GPRX_INVALID_HYPERPARAMETER;
-  }
-  double k0 = 0.0;
-  for (int t = 0; t < tree.n_terms; ++t) {
-    double pr = 1.0;
-    for (int l = 0; l < tree.n_leaves; ++l)
-      if ((tree.term_mask[t] >> l) & 1u) pr *= v0[l];
-    k0 += pr;
-  }
-  tree.diag_value = k0;
-  return GPRX_OK;
+  return (gprx_status)kt_set_theta(tree, theta.data());
 }
 
 // ---------------------------------------------------------------------------

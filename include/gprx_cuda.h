@@ -260,6 +260,39 @@ gprx_status gprx_sgpr_stage_times(gprx_sgpr* h, double* out3);
 
 
 /* ------------------------------------------------------------------ */
+/* batched exact GPR: many independent problems, one kernel tree        */
+/* (no single reference counterpart: each problem is what Gpr::fit /    */
+/* ExactFit::value_and_gradient_into_fit does for one model,            */
+/* src/gpr/exact_fit.rs:319-341, src/optimizer/lbfgs.rs:28-172)         */
+/* ------------------------------------------------------------------ */
+typedef struct gprx_batch gprx_batch;
+
+/* Largest n of one batched problem. */
+#define GPRX_BATCH_MAX_N 2048
+
+/* Uploads n_problems problems that share the kernel tree and d.  Problem i
+ * has n[i] points; x holds the problems' n[i]×d column-major blocks one after
+ * another and y their targets likewise.  n_theta = kernel parameters + 1. */
+gprx_status gprx_batch_create(const double* x, const double* y, const uint64_t* n, uint64_t n_problems,
+                              uint64_t d, const gprx_kernel_node* nodes, int32_t n_nodes, int32_t n_theta,
+                              const gprx_options* options, gprx_batch** out);
+gprx_status gprx_batch_destroy(gprx_batch* h);
+uint64_t gprx_batch_num_params(const gprx_batch* h);
+/* NLML and gradient of every problem at its own θ (row i of params,
+ * n_problems × p, log space) in one launch.  status[i] is GPRX_OK or why
+ * problem i could not be evaluated (its nlml / grad are then unset); the
+ * call itself fails only for invalid arguments or a device error. */
+gprx_status gprx_batch_eval(gprx_batch* h, const double* params, uint64_t p, double* nlml, double* grad,
+                            int32_t* status);
+/* Fits every problem as gprx_exact_fit fits one (L-BFGS over the logit map,
+ * barrier on failed evaluations, restarts from the same seeded draws), with
+ * all optimizers on the device and the evaluation rounds replayed from one
+ * CUDA graph.  Writes the best θ (n_problems × p), one report and one status
+ * per problem. */
+gprx_status gprx_batch_fit(gprx_batch* h, const double* params0, uint64_t p, const gprx_lbfgs_options* opt,
+                           double* params_out, gprx_fit_report* reports, int32_t* status);
+
+/* ------------------------------------------------------------------ */
 /* device microbenchmarks (diagnostics; no gprx counterpart)            */
 /* ------------------------------------------------------------------ */
 /* ms per launch of the FP64 DMMA GEMM C(m×n) = op(A)·op(B), k deep. */

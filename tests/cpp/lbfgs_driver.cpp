@@ -1,4 +1,4 @@
-// Test driver for the host L-BFGS (gprx_b200/csrc/lbfgs.cpp) on analytic
+// Test driver for the L-BFGS (gprx_b200/csrc/lbfgs.h, compiled for the host) on analytic
 // objectives: Rosenbrock, a quadratic with a barrier region (a point that
 // cannot be evaluated costs 1e300 with a zero gradient, as gprx's EvalCache
 // does), and the logit map round trip.  Prints one JSON object per case.
@@ -15,15 +15,16 @@ static void run(const char* name, F f, std::vector<double> x0, double tol) {
   LbfgsConfig cfg;
   cfg.tol_grad = tol;
   cfg.max_iterations = 500;
-  LbfgsRC lb;
+  static HostLbfgs lb;
   lb.start(cfg, x0.data(), (int)x0.size());
   std::vector<double> g(x0.size());
-  while (lb.task() == LbfgsRC::EVALUATE) {
-    double v = f(lb.point(), g);
+  while (lb.task() == HostLbfgs::EVALUATE) {
+    std::vector<double> pt(lb.point(), lb.point() + x0.size());
+    double v = f(pt, g);
     lb.resume(v, g.data());
   }
   std::printf("{\"case\": \"%s\", \"f\": %.17g, \"x\": [", name, lb.best_value());
-  for (size_t i = 0; i < lb.best().size(); ++i) std::printf("%s%.17g", i ? ", " : "", lb.best()[i]);
+  for (size_t i = 0; i < x0.size(); ++i) std::printf("%s%.17g", i ? ", " : "", lb.best()[i]);
   std::printf("], \"iters\": %llu, \"evals\": %llu, \"converged\": %d}\n", (unsigned long long)lb.iterations(),
               (unsigned long long)lb.evaluations(), lb.converged() ? 1 : 0);
 }
@@ -49,10 +50,10 @@ int main() {
       },
       {-20.0, 5.0}, 1e-8);
   LogitMap map;
-  map.init(3, 1e-5, 1e5);
+  map.init(1e-5, 1e5);
   double lt[3] = {std::log(0.3), std::log(2.0), std::log(1e-3)}, z[3], back[3], jac[3];
-  bool ok = map.from_log(lt, z);
-  map.to_log(z, back, jac);
+  bool ok = map.from_log(lt, 3, z);
+  map.to_log(z, 3, back, jac);
   double err = 0.0;
   for (int i = 0; i < 3; ++i) err = std::fmax(err, std::fabs(back[i] - lt[i]));
   // dlogθ/dz against a central difference
@@ -61,8 +62,8 @@ int main() {
     double zp[3] = {z[0], z[1], z[2]}, zm[3] = {z[0], z[1], z[2]}, lp[3], lm[3];
     zp[i] += 1e-6;
     zm[i] -= 1e-6;
-    map.to_log(zp, lp, nullptr);
-    map.to_log(zm, lm, nullptr);
+    map.to_log(zp, 3, lp, nullptr);
+    map.to_log(zm, 3, lm, nullptr);
     fd_err = std::fmax(fd_err, std::fabs((lp[i] - lm[i]) / 2e-6 - jac[i]));
   }
   std::printf("{\"case\": \"logit\", \"ok\": %d, \"roundtrip\": %.3g, \"jac\": %.3g}\n", ok ? 1 : 0, err, fd_err);
