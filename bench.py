@@ -192,6 +192,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-evals", type=int, default=0,
+                    help="only factor once and run this many evaluations (for an ncu launch list), no JSON line")
     args = ap.parse_args()
     n, d = args.n, D
     warm = max(3, args.warmup)
@@ -240,6 +242,11 @@ def main():
     model = gx.Gpr(spec, gx.GaussianLikelihood(NOISE), precision=prec, device=local) \
         .with_optimizer(gx.Fixed()).factor(x, n, d, y)
     stream = torch.cuda.ExternalStream(model.stream_ptr(), device=dev)
+    if args.profile_evals > 0:
+        for i in range(args.profile_evals):
+            model.value_and_gradient(thetas[i % len(thetas)])
+        torch.cuda.synchronize()
+        return
 
     def barrier():
         if dist is not None:
