@@ -34,6 +34,7 @@
 #include <string>
 #include <vector>
 
+#include "cta_gemm.cuh"
 #include "diag_block.cuh"
 #include "kernels.cuh"
 #include "lbfgs.h"
@@ -83,11 +84,7 @@ struct BatchEvalArgs {
 };
 
 constexpr int BT = FD_THREADS;  // 256 threads: 8 warps
-constexpr int GM = 64, GN = 128, GK = 32;
-constexpr int GA_LD = GM + 4;  // ≡ 4 mod 16 doubles: conflict-free fragment loads
-constexpr int GB_LD = GN + 4;
-constexpr int G_STAGE = GK * GA_LD + GK * GB_LD;
-constexpr int KM_FULL = 0, KM_FROM_ROW = 1, KM_FROM_COL = 2;
+static_assert(BT == CG_THREADS, "the diagonal step and the CTA GEMM share the block");
 
 __host__ __device__ inline long long batch_ld(int n) { return ((long long)n + 7) / 8 * 8; }
 
@@ -114,129 +111,14 @@ __device__ inline Work work_of(double* base, int nmax) {
 }
 
 // ---------------------------------------------------------------------------
-// In-CTA GEMM over 64×128 output tiles (8 warps of 32×32, DMMA m16n8k4, two
-// cp.async stages of 32-deep k chunks):
-//   C = alpha · Σ_{k∈[kb,K)} opA(i,k) opB(k,j) + beta · C
-//   opA(i,k) = TA ? A[k + i·lda] : A[i + k·lda]
-//   opB(k,j) = TB ? B[j + k·ldb] : B[k + j·ldb]
-// lower: only entries i ≥ j are written (tiles wholly above the diagonal are
-// skipped).  kmode: KM_FULL kb = 0; KM_FROM_ROW kb = the tile's first row
-// (opA zero for k < i); KM_FROM_COL kb = the tile's first column (opB zero
-// for k < j).  A tile reads all its inputs before it writes C, so C may alias
-// A's rows when one tile spans all of N (the panel step).
-// ---------------------------------------------------------------------------
-template <bool TA, bool TB>
-__device__ void cta_gemm(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
-                         double* C, long long ldc, double alpha, double beta, bool lower, int kmode, double* smem) {
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-  const int wm = warp & 1, wn = warp >> 1;
-  const int tm_n = (M + GM - 1) / GM, tn_n = (N + GN - 1) / GN;
-  for (int tile = 0; tile < tm_n * tn_n; ++tile) {
-    const int m0 = (tile % tm_n) * GM, n0 = (tile / tm_n) * GN;
-    if (lower && m0 + GM - 1 < n0) continue;
-    int kb = kmode == KM_FROM_ROW ? m0 : kmode == KM_FROM_COL ? n0 : 0;
-    const int ke = K;
-    if (kb > ke) kb = ke;
-    // a warp whose 32×32 block lies wholly above the diagonal only loads
-    const bool wskip = lower && (m0 + wm * 32 + 31 < n0 + wn * 32);
-    double acc[2][4][4];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) acc[a][b][r] = 0.0;
-    const int nch = (ke - kb + GK - 1) / GK;
-    auto load = [&](int st, int k0) {
-      double* sA = smem + st * G_STAGE;
-      double* sB = sA + GK * GA_LD;
-#pragma unroll
-      for (int it = 0; it < GM * GK / BT; ++it) {
-        const int e = tid + it * BT;
-        int i, k;
-        if (TA) { k = e % GK; i = e / GK; } else { i = e % GM; k = e / GM; }
-        const int gi = m0 + i, gk = k0 + k;
-        const bool ok = gi < M && gk < ke;
-        const double* src = ok ? (TA ? A + gk + (long long)gi * lda : A + gi + (long long)gk * lda) : A;
-        cp_async8(sA + k * GA_LD + i, src, ok);
-      }
-#pragma unroll
-      for (int it = 0; it < GK * GN / BT; ++it) {
-        const int e = tid + it * BT;
-        int k, j;
-        if (TB) { j = e % GN; k = e / GN; } else { k = e % GK; j = e / GK; }
-        const int gj = n0 + j, gk = k0 + k;
-        const bool ok = gj < N && gk < ke;
-        const double* src = ok ? (TB ? B + gj + (long long)gk * ldb : B + gk + (long long)gj * ldb) : B;
-        cp_async8(sB + k * GB_LD + j, src, ok);
-      }
-      cp_async_commit();
-    };
-    __syncthreads();  // the previous user of the stages is done
-    if (nch > 0) load(0, kb);
-    for (int ch = 0; ch < nch; ++ch) {
-      if (ch + 1 < nch) {
-        load((ch + 1) & 1, kb + (ch + 1) * GK);
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
-      __syncthreads();
-      if (!wskip) {
-        const double* sA = smem + (ch & 1) * G_STAGE;
-        const double* sB = sA + GK * GA_LD;
-#pragma unroll
-        for (int kk = 0; kk < GK; kk += 4) {
-          double a[2][2], b[4];
-#pragma unroll
-          for (int mi = 0; mi < 2; ++mi) {
-            a[mi][0] = sA[(kk + t4) * GA_LD + wm * 32 + mi * 16 + g];
-            a[mi][1] = sA[(kk + t4) * GA_LD + wm * 32 + mi * 16 + g + 8];
-          }
-#pragma unroll
-          for (int nj = 0; nj < 4; ++nj) b[nj] = sB[(kk + t4) * GB_LD + wn * 32 + nj * 8 + g];
-#pragma unroll
-          for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-            for (int nj = 0; nj < 4; ++nj) dmma_16x8x4(acc[mi][nj], a[mi][0], a[mi][1], b[nj]);
-        }
-      }
-      __syncthreads();
-    }
-    // epilogue: the C group is loaded before any of it is stored
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi) {
-      double cv[4][4];
-      bool okv[4][4];
-#pragma unroll
-      for (int nj = 0; nj < 4; ++nj)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int row = m0 + wm * 32 + mi * 16 + g + ((r & 2) ? 8 : 0);
-          const int col = n0 + wn * 32 + nj * 8 + 2 * t4 + (r & 1);
-          okv[nj][r] = row < M && col < N && !(lower && row < col);
-          cv[nj][r] = (okv[nj][r] && beta != 0.0) ? C[row + (long long)col * ldc] : 0.0;
-        }
-#pragma unroll
-      for (int nj = 0; nj < 4; ++nj)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          if (!okv[nj][r]) continue;
-          const int row = m0 + wm * 32 + mi * 16 + g + ((r & 2) ? 8 : 0);
-          const int col = n0 + wn * 32 + nj * 8 + 2 * t4 + (r & 1);
-          double v = alpha * acc[mi][nj][r];
-          if (beta != 0.0) v = fma(beta, cv[nj][r], v);
-          C[row + (long long)col * ldc] = v;
-        }
-    }
-  }
-  __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
 // fill and gradient over 64×64 lower tiles
 // ---------------------------------------------------------------------------
 constexpr int FT_B = 64;
+// pairs one thread evaluates together (ARD trees take fewer: registers)
+template <int ARD_D>
+constexpr int pairs_w() {
+  return ARD_D == 0 ? 4 : ARD_D <= 8 ? 2 : 1;
+}
 
 template <int ARD_D>
 __device__ double pair_dx(const double* xi, const double* xj, int d, double (&dx)[ARD_D > 0 ? ARD_D : 1]) {
@@ -278,15 +160,25 @@ __device__ bool cta_fill_lower(const KTree& t, const double* x, int n, double* A
       stage_points(x, n, d, i0, j0, xi, xj);
       __syncthreads();
       const int r = tid % FT_B, i = i0 + r;
-      for (int c = tid / FT_B; c < FT_B; c += BT / FT_B) {
-        const int j = j0 + c;
-        if (i >= n || j >= n || i < j) continue;
-        double dx[ARD_D > 0 ? ARD_D : 1];
-        const double r2 = pair_dx<ARD_D>(xi + r, xj + c, d, dx);
-        double v = kt_value<ARD_D>(t, dx, r2);
-        if (i == j) v += diag_add;
-        if (!isfinite(v)) bad = true;
-        A[i + (long long)j * ld] = v;
+      constexpr int CS = BT / FT_B;  // column stride of one thread
+      constexpr int PW = pairs_w<ARD_D>();
+#pragma unroll 1
+      for (int k0 = 0; k0 < FT_B / CS; k0 += PW) {
+        const int cb = tid / FT_B + k0 * CS;
+        if (i >= n || j0 + cb > i) continue;  // every pair of the group lies above the diagonal
+        double dx[PW][ARD_D > 0 ? ARD_D : 1], r2[PW], kv[PW];
+#pragma unroll
+        for (int w = 0; w < PW; ++w) r2[w] = pair_dx<ARD_D>(xi + r, xj + cb + w * CS, d, dx[w]);
+        kt_value_w<ARD_D, PW>(t, dx, r2, kv);
+#pragma unroll
+        for (int w = 0; w < PW; ++w) {
+          const int j = j0 + cb + w * CS;
+          if (j >= n || i < j) continue;
+          double v = kv[w];
+          if (i == j) v += diag_add;
+          if (!isfinite(v)) bad = true;
+          A[i + (long long)j * ld] = v;
+        }
       }
     }
   if (bad) *flag_sh = 1;
@@ -328,14 +220,26 @@ __device__ void cta_grad(const KTree& t, const double* x, int n, const double* k
       }
       __syncthreads();
       const int r = tid % FT_B, i = i0 + r;
-      for (int c = tid / FT_B; c < FT_B; c += BT / FT_B) {
-        const int j = j0 + c;
-        if (i >= n || j >= n || i < j) continue;
-        const double w = fma(ai[r], aj[c], -kinv[i + (long long)j * ld]);
-        if (i == j) acc_noise += w;
-        double dx[AD];
-        const double r2 = pair_dx<ARD_D>(xi + r, xj + c, d, dx);
-        kt_accumulate_grad<ARD_D>(t, dx, r2, (i == j) ? w : 2.0 * w, acc_leaf, acc_ard);
+      constexpr int CS = BT / FT_B;
+      constexpr int PW = pairs_w<ARD_D>();
+#pragma unroll 1
+      for (int k0 = 0; k0 < FT_B / CS; k0 += PW) {
+        const int cb = tid / FT_B + k0 * CS;
+        if (i >= n || j0 + cb > i) continue;
+        double dx[PW][AD], r2[PW], wt[PW];
+#pragma unroll
+        for (int w = 0; w < PW; ++w) {
+          const int c = cb + w * CS, j = j0 + c;
+          r2[w] = pair_dx<ARD_D>(xi + r, xj + c, d, dx[w]);
+          double wv = 0.0;  // pairs outside the lower triangle weigh nothing
+          if (j < n && i >= j) {
+            wv = fma(ai[r], aj[c], -kinv[i + (long long)j * ld]);
+            if (i == j) acc_noise += wv;
+            else wv *= 2.0;
+          }
+          wt[w] = wv;
+        }
+        kt_accumulate_grad_w<ARD_D, PW>(t, dx, r2, wt, acc_leaf, acc_ard);
       }
     }
   const int lane = tid & 31, warp = tid >> 5;
@@ -379,10 +283,10 @@ __device__ int cta_potrf(const Work& w, int n, long long ld, double* smem, int* 
     if (rest <= 0) break;
     double* P = w.A + (k0 + nbk) + (long long)k0 * ld;
     // P := P L_kk⁻ᵀ (in place: one tile spans all nbk ≤ 128 columns)
-    cta_gemm<false, true>(rest, nbk, nbk, P, ld, lk, NB_DIAG, P, ld, 1.0, 0.0, false, KM_FULL, smem);
+    cta_gemm<false, true>(rest, nbk, nbk, P, ld, lk, NB_DIAG, P, ld, 1.0, 0.0, false, CG_FULL, smem);
     // A22 −= P Pᵀ (lower)
     double* A22 = w.A + (k0 + nbk) + (long long)(k0 + nbk) * ld;
-    cta_gemm<false, true>(rest, rest, nbk, P, ld, P, ld, A22, ld, -1.0, 1.0, true, KM_FULL, smem);
+    cta_gemm<false, true>(rest, rest, nbk, P, ld, P, ld, A22, ld, -1.0, 1.0, true, CG_FULL, smem);
   }
   return -1;
 }
@@ -399,9 +303,9 @@ __device__ void cta_trtri(const Work& w, int n, long long ld, double* smem) {
     }
     if (r0 == 0) continue;
     // T = L_i,<i X_<i,<i  (X lower: k from the tile's first column)
-    cta_gemm<false, false>(nbi, r0, r0, w.A + r0, ld, w.X, ld, w.T, NB_DIAG, 1.0, 0.0, false, KM_FROM_COL, smem);
+    cta_gemm<false, false>(nbi, r0, r0, w.A + r0, ld, w.X, ld, w.T, NB_DIAG, 1.0, 0.0, false, CG_FROM_COL, smem);
     // X_i,<i = −L_ii⁻¹ T
-    cta_gemm<false, false>(nbi, r0, nbi, li, NB_DIAG, w.T, NB_DIAG, w.X + r0, ld, -1.0, 0.0, false, KM_FULL, smem);
+    cta_gemm<false, false>(nbi, r0, nbi, li, NB_DIAG, w.T, NB_DIAG, w.X + r0, ld, -1.0, 0.0, false, CG_FULL, smem);
   }
   __syncthreads();
 }
@@ -471,7 +375,7 @@ __device__ void cta_eval(const BatchEvalArgs& a, int q, const Work& w, double* s
   for (int i = tid; i < n; i += BT) acc = fma(P.y[i], w.alpha[i], acc);
   const double quad = block_sum(acc, red);
   // K⁻¹ = Xᵀ X (lower) over L in A
-  cta_gemm<true, false>(n, n, n, w.X, ld, w.X, ld, w.A, ld, 1.0, 0.0, true, KM_FROM_ROW, smem);
+  cta_gemm<true, false>(n, n, n, w.X, ld, w.X, ld, w.A, ld, 1.0, 0.0, true, CG_FROM_ROW, smem);
   cta_grad<ARD_D>(tree, P.x, n, w.A, ld, w.alpha, smem, slots);
   if (tid == 0) {
     constexpr int NS = GRAD_SLOTS_LEAF + (ARD_D > 0 ? ARD_D : 1) + 1;
@@ -508,7 +412,7 @@ __global__ void __launch_bounds__(BT, 1) batch_eval_kernel(BatchEvalArgs a) {
 }
 
 inline size_t batch_smem() {
-  size_t gemm = (size_t)2 * G_STAGE * sizeof(double);
+  size_t gemm = cg_smem_bytes();
   size_t tiles = (size_t)(2 * GPRX_MAX_DIM * FT_B + 2 * FT_B + (BT / 32) * 64) * sizeof(double);
   return std::max(std::max(diag_block_smem(), gemm), tiles);
 }

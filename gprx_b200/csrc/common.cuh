@@ -131,116 +131,198 @@ GPRX_HD inline int kt_set_theta(KTree& t, const double* th) {
   return GPRX_OK;
 }
 
-// Leaf values at one pair.  dx[f] = x1_f − x2_f.
-template <int ARD_D>
-__device__ __forceinline__ void kt_leaf_values(const KTree& t, const double* dx, double r2,
-                                               double (&v)[KT_MAX_LEAVES], double& ard_q) {
-  ard_q = 0.0;
-  if (ARD_D > 0) {
+// The pair evaluators take W pairs at once: the W evaluations are
+// independent chains of FP64 math that the scheduler interleaves, which keeps
+// the FP64 pipe busy when few warps are resident (one 256-thread CTA per SM in
+// the batched path).  W = 1 is the single-pair form of the large kernels.
+
+// Leaf values at W pairs.  dx[w][f] = x1_f − x2_f of pair w, r2[w] = |dx|².
+template <int ARD_D, int W>
+__device__ __forceinline__ void kt_leaf_values_w(const KTree& t, const double (&dx)[W][ARD_D > 0 ? ARD_D : 1],
+                                                 const double (&r2)[W], double (&v)[KT_MAX_LEAVES][W]) {
+  double ard_q[W];
 #pragma unroll
-    for (int f = 0; f < ARD_D; ++f) {
-      if (f < t.d) ard_q = fma(dx[f] * dx[f], t.inv_ell2[f], ard_q);
+  for (int w = 0; w < W; ++w) {
+    ard_q[w] = 0.0;
+    if (ARD_D > 0) {
+#pragma unroll
+      for (int f = 0; f < (ARD_D > 0 ? ARD_D : 1); ++f)
+        if (f < t.d) ard_q[w] = fma(dx[w][f] * dx[w][f], t.inv_ell2[f], ard_q[w]);
     }
   }
 #pragma unroll
   for (int l = 0; l < KT_MAX_LEAVES; ++l) {
-    if (l >= t.n_leaves) { v[l] = 0.0; continue; }
+    if (l >= t.n_leaves) {
+#pragma unroll
+      for (int w = 0; w < W; ++w) v[l][w] = 0.0;
+      continue;
+    }
     const KLeaf& lf = t.leaf[l];
-    double val;
     switch (lf.kind) {
-      case GPRX_LEAF_CONSTANT: val = lf.c0; break;
-      case GPRX_LEAF_RBF: val = exp(-r2 * lf.c0); break;
-      case GPRX_LEAF_RBF_ARD: val = exp(-0.5 * ard_q); break;
+      case GPRX_LEAF_CONSTANT:
+#pragma unroll
+        for (int w = 0; w < W; ++w) v[l][w] = lf.c0;
+        break;
+      case GPRX_LEAF_RBF:
+#pragma unroll
+        for (int w = 0; w < W; ++w) v[l][w] = exp(-r2[w] * lf.c0);
+        break;
+      case GPRX_LEAF_RBF_ARD:
+#pragma unroll
+        for (int w = 0; w < W; ++w) v[l][w] = exp(-0.5 * ard_q[w]);
+        break;
       case GPRX_LEAF_PERIODIC: {
-        double s = sin(lf.c0 * sqrt(fmax(r2, 0.0)));
-        val = exp(-2.0 * s * s * lf.c1);
+        double s[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) s[w] = sin(lf.c0 * sqrt(fmax(r2[w], 0.0)));
+#pragma unroll
+        for (int w = 0; w < W; ++w) v[l][w] = exp(-2.0 * s[w] * s[w] * lf.c1);
         break;
       }
-      default: val = 0.0;
+      default:
+#pragma unroll
+        for (int w = 0; w < W; ++w) v[l][w] = 0.0;
     }
-    v[l] = val;
   }
 }
 
-__device__ __forceinline__ double kt_combine(const KTree& t, const double (&v)[KT_MAX_LEAVES]) {
-  double k = 0.0;
+template <int W>
+__device__ __forceinline__ void kt_combine_w(const KTree& t, const double (&v)[KT_MAX_LEAVES][W], double (&k)[W]) {
+#pragma unroll
+  for (int w = 0; w < W; ++w) k[w] = 0.0;
 #pragma unroll
   for (int tt = 0; tt < KT_MAX_TERMS; ++tt) {
     if (tt >= t.n_terms) break;
-    double p = 1.0;
+    const unsigned mask = t.term_mask[tt];
+    double p[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) p[w] = 1.0;
 #pragma unroll
     for (int l = 0; l < KT_MAX_LEAVES; ++l)
-      if ((t.term_mask[tt] >> l) & 1u) p *= v[l];
-    k += p;
+      if ((mask >> l) & 1u) {
+#pragma unroll
+        for (int w = 0; w < W; ++w) p[w] *= v[l][w];
+      }
+#pragma unroll
+    for (int w = 0; w < W; ++w) k[w] += p[w];
   }
-  return k;
 }
 
-// k(x1, x2).  x1/x2 are feature-0 pointers with strides s1/s2.
+// k(x1, x2) at W pairs.
+template <int ARD_D, int W>
+__device__ __forceinline__ void kt_value_w(const KTree& t, const double (&dx)[W][ARD_D > 0 ? ARD_D : 1],
+                                           const double (&r2)[W], double (&k)[W]) {
+  double v[KT_MAX_LEAVES][W];
+  kt_leaf_values_w<ARD_D, W>(t, dx, r2, v);
+  kt_combine_w<W>(t, v, k);
+}
+
+// k(x1, x2) at one pair.
 template <int ARD_D>
 __device__ __forceinline__ double kt_value(const KTree& t, const double* dx, double r2) {
-  double v[KT_MAX_LEAVES];
-  double q;
-  kt_leaf_values<ARD_D>(t, dx, r2, v, q);
-  return kt_combine(t, v);
+  constexpr int AD = ARD_D > 0 ? ARD_D : 1;
+  double d1[1][AD];
+#pragma unroll
+  for (int f = 0; f < AD; ++f) d1[0][f] = dx[f];
+  const double r[1] = {r2};
+  double k[1];
+  kt_value_w<ARD_D, 1>(t, d1, r, k);
+  return k[0];
 }
 
-// Accumulates w · ∂k/∂θ into per-leaf slots (acc_leaf[l][0..1]) and per-dim ARD
-// slots (acc_ard[f]); the host maps slots to θ indices.  A Sum gives each term
-// the same weight; a Product gives a factor the weight times the other factors
-// (src/kernel/compiled/weighted.rs:274-345).
-template <int ARD_D>
-__device__ __forceinline__ void kt_accumulate_grad(const KTree& t, const double* dx, double r2, double w,
-                                                   double (&acc_leaf)[KT_MAX_LEAVES][KT_ACC_PER_LEAF],
-                                                   double (&acc_ard)[ARD_D > 0 ? ARD_D : 1]) {
-  double v[KT_MAX_LEAVES];
-  double q;
-  kt_leaf_values<ARD_D>(t, dx, r2, v, q);
-  double adj[KT_MAX_LEAVES];
+// Accumulates wt[w] · ∂k/∂θ of W pairs into per-leaf slots (acc_leaf[l][0..1])
+// and per-dim ARD slots (acc_ard[f]); the host maps slots to θ indices.  A Sum
+// gives each term the same weight; a Product gives a factor the weight times
+// the other factors (src/kernel/compiled/weighted.rs:274-345).
+template <int ARD_D, int W>
+__device__ __forceinline__ void kt_accumulate_grad_w(const KTree& t, const double (&dx)[W][ARD_D > 0 ? ARD_D : 1],
+                                                     const double (&r2)[W], const double (&wt)[W],
+                                                     double (&acc_leaf)[KT_MAX_LEAVES][KT_ACC_PER_LEAF],
+                                                     double (&acc_ard)[ARD_D > 0 ? ARD_D : 1]) {
+  double v[KT_MAX_LEAVES][W];
+  kt_leaf_values_w<ARD_D, W>(t, dx, r2, v);
+  double adj[KT_MAX_LEAVES][W];
 #pragma unroll
-  for (int l = 0; l < KT_MAX_LEAVES; ++l) adj[l] = 0.0;
+  for (int l = 0; l < KT_MAX_LEAVES; ++l)
+#pragma unroll
+    for (int w = 0; w < W; ++w) adj[l][w] = 0.0;
 #pragma unroll
   for (int tt = 0; tt < KT_MAX_TERMS; ++tt) {
     if (tt >= t.n_terms) break;
-    unsigned mask = t.term_mask[tt];
+    const unsigned mask = t.term_mask[tt];
 #pragma unroll
     for (int l = 0; l < KT_MAX_LEAVES; ++l) {
       if (!((mask >> l) & 1u)) continue;
-      double others = 1.0;
+      double others[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w) others[w] = 1.0;
 #pragma unroll
       for (int o = 0; o < KT_MAX_LEAVES; ++o)
-        if (o != l && ((mask >> o) & 1u)) others *= v[o];
-      adj[l] += others;
+        if (o != l && ((mask >> o) & 1u)) {
+#pragma unroll
+          for (int w = 0; w < W; ++w) others[w] *= v[o][w];
+        }
+#pragma unroll
+      for (int w = 0; w < W; ++w) adj[l][w] += others[w];
     }
   }
 #pragma unroll
   for (int l = 0; l < KT_MAX_LEAVES; ++l) {
     if (l >= t.n_leaves) break;
     const KLeaf& lf = t.leaf[l];
-    double wa = w * adj[l];
     switch (lf.kind) {
-      case GPRX_LEAF_CONSTANT: acc_leaf[l][0] = fma(wa, lf.c0, acc_leaf[l][0]); break;
-      case GPRX_LEAF_RBF: acc_leaf[l][0] = fma(wa * v[l], 2.0 * lf.c0 * r2, acc_leaf[l][0]); break;
+      case GPRX_LEAF_CONSTANT:
+#pragma unroll
+        for (int w = 0; w < W; ++w) acc_leaf[l][0] = fma(wt[w] * adj[l][w], lf.c0, acc_leaf[l][0]);
+        break;
+      case GPRX_LEAF_RBF:
+#pragma unroll
+        for (int w = 0; w < W; ++w)
+          acc_leaf[l][0] = fma(wt[w] * adj[l][w] * v[l][w], 2.0 * lf.c0 * r2[w], acc_leaf[l][0]);
+        break;
       case GPRX_LEAF_RBF_ARD:
         if (ARD_D > 0) {
-          double wv = wa * v[l];
 #pragma unroll
-          for (int f = 0; f < (ARD_D > 0 ? ARD_D : 1); ++f)
-            if (f < t.d) acc_ard[f] = fma(wv, dx[f] * dx[f] * t.inv_ell2[f], acc_ard[f]);
+          for (int w = 0; w < W; ++w) {
+            const double wv = wt[w] * adj[l][w] * v[l][w];
+#pragma unroll
+            for (int f = 0; f < (ARD_D > 0 ? ARD_D : 1); ++f)
+              if (f < t.d) acc_ard[f] = fma(wv, dx[w][f] * dx[w][f] * t.inv_ell2[f], acc_ard[f]);
+          }
         }
         break;
       case GPRX_LEAF_PERIODIC: {
-        double a = lf.c0 * sqrt(fmax(r2, 0.0));
-        double s, c;
-        sincos(a, &s, &c);
-        double wv = wa * v[l] * 4.0 * lf.c1 * s;
-        acc_leaf[l][0] = fma(wv, s, acc_leaf[l][0]);
-        acc_leaf[l][1] = fma(wv, c * a, acc_leaf[l][1]);
+        double a[W], s[W], c[W];
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          a[w] = lf.c0 * sqrt(fmax(r2[w], 0.0));
+          sincos(a[w], &s[w], &c[w]);
+        }
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          const double wv = wt[w] * adj[l][w] * v[l][w] * 4.0 * lf.c1 * s[w];
+          acc_leaf[l][0] = fma(wv, s[w], acc_leaf[l][0]);
+          acc_leaf[l][1] = fma(wv, c[w] * a[w], acc_leaf[l][1]);
+        }
         break;
       }
-      default: break;
+      default:
+        break;
     }
   }
+}
+
+template <int ARD_D>
+__device__ __forceinline__ void kt_accumulate_grad(const KTree& t, const double* dx, double r2, double w,
+                                                   double (&acc_leaf)[KT_MAX_LEAVES][KT_ACC_PER_LEAF],
+                                                   double (&acc_ard)[ARD_D > 0 ? ARD_D : 1]) {
+  constexpr int AD = ARD_D > 0 ? ARD_D : 1;
+  double d1[1][AD];
+#pragma unroll
+  for (int f = 0; f < AD; ++f) d1[0][f] = dx[f];
+  const double r[1] = {r2};
+  const double wt[1] = {w};
+  kt_accumulate_grad_w<ARD_D, 1>(t, d1, r, wt, acc_leaf, acc_ard);
 }
 
 // Number of accumulator slots and the θ index of each (host side).
