@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -92,7 +93,7 @@ __host__ __device__ inline long long batch_ld(int n) { return ((long long)n + 7)
 struct Work {
   double *A, *X, *T, *linv, *z, *alpha;
 };
-__host__ __device__ inline long long work_doubles(int nmax) {
+__host__ __device__ constexpr long long work_doubles(int nmax) {
   long long ld = ((long long)nmax + 7) / 8 * 8;
   long long nblk = (nmax + NB_DIAG - 1) / NB_DIAG;
   return 2 * ld * nmax + (long long)NB_DIAG * ld + nblk * NB_DIAG * NB_DIAG + 2 * ld;
@@ -868,6 +869,159 @@ gprx_status BatchState::fit(const double* theta0, const gprx_lbfgs_options* o, d
   return GPRX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free evaluation of one exact problem (gprx_exact_eval_noalloc).
+//
+// For callers that cannot allocate device memory at the moment they need an
+// evaluation: code running while a CUDA graph is being captured on the
+// stream, inside an allocator-owned memory pool (a framework that owns every
+// byte of the device, a server under a fixed HBM budget), or in a real-time
+// loop where the device-wide synchronisation of cudaMalloc/cudaFree is not
+// acceptable.  The scratch the evaluation needs (the header of the persistent
+// kernel and one CTA workspace) lives in the file-scope array below, sized for
+// problems of up to NOALLOC_MAX_N points; every device that loads the library
+// holds it until the process exits.  The caller passes device inputs and
+// outputs; only the θ vector and the kernel tree come from host memory.
+// ---------------------------------------------------------------------------
+constexpr int NOALLOC_MAX_N = 512;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+struct NoAllocHeader {
+  BatchProblem prob;
+  BatchHeader hdr;
+  int order[1];
+  int status[1];
+  double log_theta[BATCH_MAX_VARS];
+  double nlml[1];
+  double grad[BATCH_MAX_VARS];
+};
+// the header is padded to 256 bytes so that the workspace keeps the alignment
+// the CTA GEMM's 16-byte copies rely on
+constexpr long long NOALLOC_HEADER_DOUBLES = ((long long)sizeof(NoAllocHeader) + 255) / 256 * 32;
+constexpr long long NOALLOC_SCRATCH_DOUBLES = NOALLOC_HEADER_DOUBLES + work_doubles(NOALLOC_MAX_N);
+
+// 5.3 MB per device.  Host code must not pass this name to a kernel: on the
+// host it is a stand-in, not a device address (see noalloc_scratch_ptr).
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
+
+struct NoAllocTheta {
+  double v[BATCH_MAX_VARS];
+};
+
+// Writes the header of this call (everything the evaluation reads that must
+// start fresh: the queue counter, the problem, θ, the status).
+__global__ void noalloc_prep_kernel(double* scratch, BatchProblem prob, NoAllocTheta th, int p) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  NoAllocHeader* h = reinterpret_cast<NoAllocHeader*>(scratch);
+  h->prob = prob;
+  h->hdr.queue = 0;
+  h->hdr.active = 0;
+  h->order[0] = 0;
+  h->status[0] = GPRX_NOT_CONVERGED;  // overwritten by the evaluation
+  h->nlml[0] = 0.0;
+  for (int i = 0; i < BATCH_MAX_VARS; ++i) {
+    h->log_theta[i] = i < p ? th.v[i] : 0.0;
+    h->grad[i] = 0.0;
+  }
+}
+
+__global__ void noalloc_finish_kernel(const double* scratch, int p, double* nlml, double* grad, int32_t* status) {
+  const NoAllocHeader* h = reinterpret_cast<const NoAllocHeader*>(scratch);
+  const int i = threadIdx.x;
+  if (i == 0) {
+    *status = h->status[0];
+    *nlml = h->status[0] == GPRX_OK ? h->nlml[0] : 0.0;
+  }
+  if (grad && i < p) grad[i] = h->status[0] == GPRX_OK ? h->grad[i] : 0.0;
+}
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (with that device current) and kept.
+static gprx_status noalloc_scratch_ptr(int dev, double** out) {
+  static std::mutex mu;
+  static double* ptrs[NOALLOC_MAX_DEVICES] = {};
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return set_error(GPRX_INVALID_CONFIG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptrs[dev]) {
+    double* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    const int smem = (int)batch_smem();
+    cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if ((e = cudaFuncSetAttribute(batch_eval_kernel<0>, a, smem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(batch_eval_kernel<4>, a, smem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(batch_eval_kernel<8>, a, smem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(batch_eval_kernel<16>, a, smem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(batch_eval_kernel<32>, a, smem)) != cudaSuccess)
+      return set_cuda_error(e, "shared-memory attribute of the evaluation kernel");
+    ptrs[dev] = p;
+  }
+  *out = ptrs[dev];
+  return GPRX_OK;
+}
+
+static gprx_status exact_eval_noalloc(const double* x, const double* y, uint64_t n, uint64_t d,
+                                      const gprx_kernel_node* nodes, int32_t n_nodes, const double* params,
+                                      uint64_t p, const gprx_options* opts, double* nlml, double* grad,
+                                      int32_t* status, void* stream) {
+  if (!x || !y || !nodes || !params || !nlml || !status) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (n == 0) return set_error(GPRX_EMPTY_INPUT, "no training points");
+  if (d == 0) return set_error(GPRX_EMPTY_INPUT, "no features (d = 0)");
+  if (n > (uint64_t)NOALLOC_MAX_N)
+    return set_error(GPRX_CAPACITY, "gprx_exact_eval_noalloc takes at most 512 points (its fixed scratch size); "
+                                    "use gprx_exact_eval or gprx_batch_eval for larger problems");
+  if (p < 1 || p > (uint64_t)BATCH_MAX_VARS)
+    return set_error(GPRX_INVALID_CONFIG, "gprx_exact_eval_noalloc takes 1..16 parameters");
+  gprx_options o;
+  if (opts) o = *opts;
+  else gprx_options_default(&o);
+  if (o.jitter_kind != GPRX_JITTER_FIXED && o.jitter_max_retries > BATCH_MAX_JITTERS)
+    return set_error(GPRX_INVALID_CONFIG, "at most 8 jitter retries");
+  HostKernel kern;
+  std::string why;
+  gprx_status st = kern.init(nodes, n_nodes, params, (int)p - 1, (int)d, &why);
+  if (st != GPRX_OK) return set_error(st, why);
+  int dev = 0;
+  GPRX_CUDA_TRY(cudaGetDevice(&dev));
+  double* scratch = nullptr;
+  if ((st = noalloc_scratch_ptr(dev, &scratch)) != GPRX_OK) return st;
+  NoAllocHeader* h = reinterpret_cast<NoAllocHeader*>(scratch);  // a device address
+  BatchProblem prob{x, y, (int)n, 0};
+  NoAllocTheta th{};
+  for (uint64_t i = 0; i < p; ++i) th.v[i] = params[i];
+  BatchEvalArgs a{};
+  a.probs = &h->prob;
+  a.order = h->order;
+  a.nprob = 1;
+  a.p = (int)p;
+  a.log_theta = h->log_theta;
+  a.active = nullptr;
+  a.nlml = h->nlml;
+  a.grad = h->grad;
+  a.status = h->status;
+  a.hdr = &h->hdr;
+  a.work = scratch + NOALLOC_HEADER_DOUBLES;
+  a.work_stride = 0;
+  a.nmax = (int)n;
+  a.jit = jitter_list(o);
+  a.tmpl = kern.tree;
+  for (int i = 0; i < 64; ++i) a.slot_param[i] = i < (int)kern.slot_param.size() ? kern.slot_param[i] : -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t smem = batch_smem();
+  noalloc_prep_kernel<<<1, 32, 0, s>>>(scratch, prob, th, (int)p);
+  switch (kern.ard_d) {
+    case 0: batch_eval_kernel<0><<<1, BT, smem, s>>>(a); break;
+    case 4: batch_eval_kernel<4><<<1, BT, smem, s>>>(a); break;
+    case 8: batch_eval_kernel<8><<<1, BT, smem, s>>>(a); break;
+    case 16: batch_eval_kernel<16><<<1, BT, smem, s>>>(a); break;
+    default: batch_eval_kernel<32><<<1, BT, smem, s>>>(a); break;
+  }
+  noalloc_finish_kernel<<<1, 32, 0, s>>>(scratch, (int)p, nlml, grad, status);
+  count_launch(3);
+  GPRX_CUDA_TRY(cudaGetLastError());
+  return GPRX_OK;
+}
+
 }  // namespace gprx
 
 using namespace gprx;
@@ -910,6 +1064,13 @@ gprx_status gprx_batch_fit(gprx_batch* h, const double* params0, uint64_t p, con
   if (!h) return set_error(GPRX_INVALID_ARGUMENT, "null handle");
   if (p != (uint64_t)h->s.p) return set_error(GPRX_SHAPE_MISMATCH, "params must hold p values per problem");
   return h->s.fit(params0, opt, params_out, reports, status);
+}
+
+gprx_status gprx_exact_eval_noalloc(const double* x, const double* y, uint64_t n, uint64_t d,
+                                    const gprx_kernel_node* nodes, int32_t n_nodes, const double* params, uint64_t p,
+                                    const gprx_options* options, double* nlml, double* grad, int32_t* status,
+                                    void* stream) {
+  return exact_eval_noalloc(x, y, n, d, nodes, n_nodes, params, p, options, nlml, grad, status, stream);
 }
 
 }  // extern "C"

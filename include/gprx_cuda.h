@@ -292,6 +292,31 @@ gprx_status gprx_batch_eval(gprx_batch* h, const double* params, uint64_t p, dou
 gprx_status gprx_batch_fit(gprx_batch* h, const double* params0, uint64_t p, const gprx_lbfgs_options* opt,
                            double* params_out, gprx_fit_report* reports, int32_t* status);
 
+/* Allocation-free NLML + gradient of ONE exact problem (no counterpart in the
+ * reference).  For callers that cannot allocate device memory when they need
+ * an evaluation: work issued while a CUDA graph is being captured, code inside
+ * a framework or server that owns every byte of the device, or a loop that
+ * cannot take the device-wide synchronisation of cudaMalloc/cudaFree.
+ *  - x (n×d column-major), y, nlml, grad (p values, may be NULL) and status
+ *    are DEVICE pointers owned by the caller; params (log θ, p values) and the
+ *    kernel tree are host memory read during the call.
+ *  - n ≤ 512 and p ≤ 16; larger requests return GPRX_CAPACITY / INVALID_CONFIG.
+ *  - The work is enqueued on `stream` (a cudaStream_t; NULL = default stream)
+ *    and the call returns without waiting: *status (a gprx_status) and the
+ *    results are valid once the stream reaches them.  On a failed evaluation
+ *    *status says why and nlml / grad are written as 0.
+ *  - The scratch is one fixed 5.3 MB array in device memory per GPU, shared by
+ *    every call: calls whose work overlaps on the GPU (other streams, other
+ *    threads) race and must be ordered by the caller.  The first call on a
+ *    device looks up that array's address and sets the kernel's shared-memory
+ *    limit; make that first call before any stream capture.
+ *  - Same result as gprx_batch_eval / gprx_exact_eval of the same problem
+ *    (one CTA evaluates it in a fixed order). */
+gprx_status gprx_exact_eval_noalloc(const double* x, const double* y, uint64_t n, uint64_t d,
+                                    const gprx_kernel_node* nodes, int32_t n_nodes, const double* params, uint64_t p,
+                                    const gprx_options* options, double* nlml, double* grad, int32_t* status,
+                                    void* stream);
+
 /* ------------------------------------------------------------------ */
 /* device microbenchmarks (diagnostics; no gprx counterpart)            */
 /* ------------------------------------------------------------------ */
