@@ -183,6 +183,117 @@ def cpu_reference(n, d, x, y, thetas, steps, warmup, budget_s=6.0):
     return 1.0 / dt, dt, cores, sample
 
 
+# ---------------------------------------------------------------------------
+# batched fits (4096 ragged problems, Rbf + Periodic, d = 3)
+# ---------------------------------------------------------------------------
+BATCH_P = 4096
+BATCH_D = 3
+
+
+def batched_synth(torch, dev, count=BATCH_P, seed=3):
+    """Sizes log-uniform in [32, 1024], x ~ U[0,5]³, period ~ U[10, 20]
+    (shorter periods make the Euclidean-distance periodic kernel indefinite
+    in 3-d), θ_true = (ℓ_rbf 1, ℓ_per 1, p, σn² 0.1); y a draw from each
+    problem's GP prior (Cholesky on the device, data generation only)."""
+    import gprx_b200 as gx
+
+    rng = gx.SeededRng(seed)
+    u = rng.unit(count)
+    sizes = np.floor(np.exp(math.log(32) + u * (math.log(1024) - math.log(32)))).astype(np.int64)
+    periods = 10.0 + 10.0 * rng.unit(count)
+    xs, ys = [], []
+    for n, per in zip(sizes, periods):
+        x = 5.0 * rng.unit(int(n) * BATCH_D)
+        z = rng.normal(int(n))
+        xt = torch.from_numpy(x.reshape(BATCH_D, int(n)).T.copy()).to(dev)
+        r2 = torch.cdist(xt, xt).pow(2)
+        k = torch.exp(-0.5 * r2) + torch.exp(-2.0 * torch.sin(math.pi * torch.sqrt(r2) / per) ** 2)
+        k += 0.1 * torch.eye(int(n), dtype=torch.float64, device=dev)
+        y = torch.linalg.cholesky(k) @ torch.from_numpy(z).to(dev)
+        xs.append(x)
+        ys.append(y.cpu().numpy())
+    theta0 = np.stack([np.zeros(count), np.zeros(count), np.log(periods), np.full(count, math.log(0.1))], axis=1)
+    return sizes, xs, ys, theta0
+
+
+def batched_measure(torch, dev, count=BATCH_P, single_sample=32, cpu_sample=48, fp64_peak=None):
+    import gprx_b200 as gx
+    from gprx_b200 import _lib as L
+
+    sizes, xs, ys, theta0 = batched_synth(torch, dev, count)
+    spec = gx.RbfKernel(1.0) + gx.PeriodicKernel(1.0, 15.0)
+    opt = gx.Lbfgs().with_tolerance(1e-6)
+    # end to end through the public API: upload, fit, results back
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b = gx.GprBatch(spec, xs, ys, BATCH_D, device=dev.index or 0)
+    res = b.fit(theta0, opt)
+    e2e_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(b.stream_ptr(), device=dev)
+    # device-timed fit (inputs resident)
+    l0 = L.lib().gprx_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = b.fit(theta0, opt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = int(L.lib().gprx_launch_count() - l0)
+    fit_s = e0.elapsed_time(e1) * 1e-3
+    # one evaluation round at θ0 for the roofline (Σ n³ flop per round)
+    e0.record(stream)
+    nl, g, st = b.value_and_gradient(theta0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    round_ms = e0.elapsed_time(e1)
+    flops = float((sizes.astype(np.float64) ** 3).sum())
+    achieved = flops / (round_ms * 1e-3) / 1e12
+    # one model per launch: the single-model path on every k-th problem
+    idx = list(range(0, count, max(1, count // single_sample)))[:single_sample]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in idx:
+        m = gx.Gpr(gx.RbfKernel(1.0) + gx.PeriodicKernel(1.0, math.exp(theta0[i][2])), gx.GaussianLikelihood(0.1),
+                   optimizer=opt, device=dev.index or 0)
+        m.fit(xs[i], int(sizes[i]), BATCH_D, ys[i])
+    single_s = time.perf_counter() - t0
+    single_fps = len(idx) / single_s
+    # CPU: the oracle's evaluations on a sample, times evaluations per fit
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    nodes = [[1, 2], [10, 0], [13, 0]]
+    cidx = list(range(0, count, max(1, count // cpu_sample)))[:cpu_sample]
+    t0 = time.perf_counter()
+    for i in cidx:
+        O.exact_eval(nodes, theta0[i], xs[i], int(sizes[i]), BATCH_D, ys[i])
+    cpu_eval_s = (time.perf_counter() - t0) / len(cidx)
+    evals_per_fit = float(res.evaluations.mean())
+    cpu_fps = 1.0 / (cpu_eval_s * evals_per_fit)
+    bytes_in = int(sum(x.nbytes + y.nbytes for x, y in zip(xs, ys)) + theta0.nbytes)
+    return {
+        "metric": "batched fits/s (4096 ragged exact GPs, L-BFGS to |g| < 1e-6)",
+        "value": count / fit_s, "unit": "fits/s", "ms_per_fit_batch": fit_s * 1e3,
+        "config": {"workload": "batched_exact_fit_4096_ragged_rbf_periodic_d3", "problems": count,
+                   "n": "log-uniform [32, 1024]", "sum_n3": flops, "d": BATCH_D,
+                   "kernel": "RbfKernel(1.0) + PeriodicKernel(1.0, p), p ~ U[10, 20]", "noise_variance": 0.1,
+                   "tolerance": 1e-6},
+        "status_ok": int((res.status == 0).sum()), "converged": int(res.converged.sum()),
+        "evaluations_mean": evals_per_fit, "evaluations_max": int(res.evaluations.max()),
+        "gpu_launches": launches,
+        "e2e": {"value": count / e2e_s, "unit": "fits/s", "h2d_bytes_per_step": bytes_in,
+                "d2h_bytes_per_step": int(theta0.nbytes + count * (8 * 4 + 4 * 2))},
+        "one_model_per_launch": {"value": single_fps, "unit": "fits/s",
+                                 "sample": "%d problems (every %d-th), Gpr.fit each" % (len(idx), count // single_sample)},
+        "speedup_vs_one_model_per_launch": (count / fit_s) / single_fps,
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak if fp64_peak else None, "kernel": "batch_eval_kernel",
+                     "work": "sum of n_i^3 flop per evaluation round", "round_ms": round_ms},
+        "cpu_baseline": {"value": cpu_fps, "unit": "fits/s", "cores": int(O.lib().orc_num_threads()), "kind": "port",
+                         "sample": "oracle NLML+gradient of %d problems (every %d-th) at θ0, times the batched run's "
+                                   "mean evaluations per fit (%.1f)" % (len(cidx), count // cpu_sample,
+                                                                         evals_per_fit)},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -194,6 +305,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-evals", type=int, default=0,
                     help="only factor once and run this many evaluations (for an ncu launch list), no JSON line")
+    ap.add_argument("--workload", default="all", choices=["all", "exact", "batched"],
+                    help="all: the exact line with the batched measurement as its 'batched' key")
+    ap.add_argument("--batch-problems", type=int, default=BATCH_P)
     args = ap.parse_args()
     n, d = args.n, D
     warm = max(3, args.warmup)
@@ -236,6 +350,21 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+
+    if args.workload == "batched":
+        if args.profile_evals > 0:
+            sizes, xs, ys, theta0 = batched_synth(torch, dev, args.batch_problems)
+            b = gx.GprBatch(gx.RbfKernel(1.0) + gx.PeriodicKernel(1.0, 15.0), xs, ys, BATCH_D, device=local)
+            for _ in range(args.profile_evals):
+                b.value_and_gradient(theta0)
+            torch.cuda.synchronize()
+            return
+        peak = fp64_peak_tflops(torch, dev)
+        out = batched_measure(torch, dev, args.batch_problems, fp64_peak=peak)
+        out.update({"n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f64", "data": "synthetic"})
+        print(json.dumps(out), flush=True)
+        return
 
     spec = gx.ConstantKernel(CONST) * gx.RbfArdKernel(list(np.exp(theta[1:1 + d])))
     prec = gx.Precision.Fp64 if args.precision == "fp64" else gx.Precision.Mixed
@@ -323,9 +452,13 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, cores, sample = cpu_reference(n, d, x, y, thetas, steps=1, warmup=0, budget_s=30.0)
         line["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": cores, "kind": "port", "sample": sample}
+    if args.workload == "all" and world == 1:
+        del model
+        torch.cuda.empty_cache()
+        line["batched"] = batched_measure(torch, dev, args.batch_problems, fp64_peak=fp64_peak)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del model
+    model = None
     if dist is not None:
         dist.destroy_process_group()
 

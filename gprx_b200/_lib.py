@@ -130,6 +130,7 @@ _SIGS = {
     "gprx_batch_eval": (C.c_int32, [C.c_void_p, D, C.c_uint64, D, D, I32]),
     "gprx_batch_fit": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.POINTER(LbfgsOptions), D, C.POINTER(FitReport),
                                    I32]),
+    "gprx_batch_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "gprx_probe_dgemm": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
     "gprx_probe_potrf": (C.c_int32, [C.c_int32, C.c_int32, D]),
     "gprx_rng_seed": (None, [C.POINTER(Rng), C.c_uint64]),

@@ -766,6 +766,12 @@ class GprBatch:
             raise ShapeMismatch("params must be n_problems × %d" % self.p)
         return a
 
+    def stream_ptr(self):
+        """The handle's CUDA stream (for event timing)."""
+        s = C.c_void_p()
+        check(L.lib().gprx_batch_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def value_and_gradient(self, params):
         """NLML, gradient and status of every problem at its own θ (row i)."""
         a = self._params(params)

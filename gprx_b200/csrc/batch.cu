@@ -1066,6 +1066,12 @@ gprx_status gprx_batch_fit(gprx_batch* h, const double* params0, uint64_t p, con
   return h->s.fit(params0, opt, params_out, reports, status);
 }
 
+gprx_status gprx_batch_stream(gprx_batch* h, void** stream) {
+  if (!h || !stream) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  *stream = (void*)h->s.stream;
+  return GPRX_OK;
+}
+
 gprx_status gprx_exact_eval_noalloc(const double* x, const double* y, uint64_t n, uint64_t d,
                                     const gprx_kernel_node* nodes, int32_t n_nodes, const double* params, uint64_t p,
                                     const gprx_options* options, double* nlml, double* grad, int32_t* status,

@@ -291,6 +291,8 @@ gprx_status gprx_batch_eval(gprx_batch* h, const double* params, uint64_t p, dou
  * per problem. */
 gprx_status gprx_batch_fit(gprx_batch* h, const double* params0, uint64_t p, const gprx_lbfgs_options* opt,
                            double* params_out, gprx_fit_report* reports, int32_t* status);
+/* The CUDA stream (a cudaStream_t) of the handle, for event timing. */
+gprx_status gprx_batch_stream(gprx_batch* h, void** stream);
 
 /* Allocation-free NLML + gradient of ONE exact problem (no counterpart in the
  * reference).  For callers that cannot allocate device memory when they need
