@@ -133,6 +133,7 @@ _SIGS = {
     "gprx_batch_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "gprx_probe_dgemm": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
     "gprx_probe_potrf": (C.c_int32, [C.c_int32, C.c_int32, D]),
+    "gprx_probe_emu_gemm": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
     "gprx_rng_seed": (None, [C.POINTER(Rng), C.c_uint64]),
     "gprx_rng_next_u64": (C.c_uint64, [C.POINTER(Rng)]),
     "gprx_rng_unit": (C.c_double, [C.POINTER(Rng)]),

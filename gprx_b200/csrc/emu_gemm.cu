@@ -1,0 +1,379 @@
+// emu_gemm.cu — see emu_gemm.cuh.
+//
+// Slice planes are stored pre-tiled: for plane p, 128-row tile rt and
+// 64-byte K chunk kc, one 8 KB block at ((p·ntr + rt)·nkc + kc)·8 KB holds the
+// chunk in the K-major, no-swizzle UMMA layout (8-row × 16-byte core
+// matrices; the four K-adjacent core matrices of a row group 128 B apart, row
+// groups 512 B apart), so a pipeline stage is filled by 2S bulk copies
+// (cp.async.bulk, completion counted on the stage's "full" mbarrier).
+//
+// Kernel shape: one CTA of 128 threads per 128×64 output tile.  Thread 0
+// issues the bulk copies and the MMAs (tcgen05.mma.cta_group::1.kind::i8,
+// M = 128, K = 32): slice p of A against the stacked B slices q = 0..S-1-p,
+// so term p+q lands in TMEM columns 64(p+q) and one MMA of N = 64(S − p)
+// (split at 256) covers every term of slice p; tcgen05.commit to the stage's
+// "empty" mbarrier frees it for the next copy.
+// The epilogue (all four warps, TMEM lane = output row) loads the S terms,
+// combines them in FP64 and writes beta·C + alpha·2^-(e_i+e_j)·Σ_t 2^-7t C_t.
+// Every wait on an mbarrier is bounded by a clock limit; a wait that runs
+// out sets the error flag and the kernel still frees its TMEM and returns.
+
+#include <cmath>
+
+#include "emu_gemm.cuh"
+#include "gemm_f64.cuh"
+
+namespace gprx {
+
+// ---------------------------------------------------------------------------
+// slicing
+// ---------------------------------------------------------------------------
+// exps[r] = 6 − E with max_k |op(r,k)| = m·2^E, m ∈ [0.5, 1): the scaled row
+// maximum lies in [32, 64).
+__global__ void emu_exp_rows_kernel(const double* M, long long ld, int R, int K, int Rpad, int* exps) {
+  // trans = false: row r is M[r + k·ld]; consecutive threads take consecutive
+  // rows, so every k step is one coalesced access per warp
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= Rpad) return;
+  double mx = 0.0;
+  if (r < R)
+    for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(M[r + (long long)k * ld]));
+  int E = 0;
+  frexp(mx, &E);
+  exps[r] = mx > 0.0 ? 6 - E : 0;
+}
+
+__global__ void emu_exp_rows_t_kernel(const double* M, long long ld, int R, int K, int Rpad, int* exps) {
+  // trans = true: row r is M[k + r·ld], contiguous; one warp per row
+  const int r = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (r >= Rpad) return;
+  double mx = 0.0;
+  if (r < R)
+    for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(M[k + (long long)r * ld]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if (lane == 0) {
+    int E = 0;
+    frexp(mx, &E);
+    exps[r] = mx > 0.0 ? 6 - E : 0;
+  }
+}
+
+// One block per 32 rows × 64 columns of K: the tile is staged in shared
+// memory (coalesced reads in either storage order), then each thread writes
+// 8 digits of one row for every slice plane into the pre-tiled layout.
+template <int S>
+__global__ void __launch_bounds__(256) emu_slice_kernel(const double* M, long long ld, bool trans, int R, int K,
+                                                        int Rpad, int Kpad, const int* exps, int8_t* out) {
+  __shared__ double t[32][65];
+  const int r0 = blockIdx.x * 32, kc = blockIdx.y, k0 = kc * 64, tid = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int r, k;
+    if (!trans) {
+      r = tid & 31;
+      k = (tid >> 5) + 8 * i;
+    } else {
+      k = tid & 63;
+      r = (tid >> 6) + 4 * i;
+    }
+    const int gr = r0 + r, gk = k0 + k;
+    double a = 0.0;
+    if (gr < R && gk < K) a = trans ? M[gk + (long long)gr * ld] : M[gr + (long long)gk * ld];
+    t[r][k] = a;
+  }
+  __syncthreads();
+  const int r = tid >> 3, c8 = tid & 7, gr = r0 + r;
+  if (gr >= Rpad) return;
+  const int e = exps[gr];
+  uint32_t w[S][2];
+#pragma unroll
+  for (int p = 0; p < S; ++p) w[p][0] = w[p][1] = 0u;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    double a = ldexp(t[r][c8 * 8 + u], e);
+#pragma unroll
+    for (int p = 0; p < S; ++p) {
+      const double d = rint(a);
+      w[p][u >> 2] |= ((uint32_t)(uint8_t)(int8_t)(int)d) << (8 * (u & 3));
+      a = (a - d) * 128.0;
+    }
+  }
+  const int ntr = Rpad / EMU_M, nkc = Kpad / EMU_KC, rt = gr / EMU_M, rr = gr % EMU_M;
+  const size_t within = (size_t)(rr >> 3) * 512 + (c8 >> 1) * 128 + (rr & 7) * 16 + (c8 & 1) * 8;
+#pragma unroll
+  for (int p = 0; p < S; ++p) {
+    const size_t blk = ((size_t)p * ntr + rt) * nkc + kc;
+    *reinterpret_cast<uint2*>(out + blk * 8192 + within) = make_uint2(w[p][0], w[p][1]);
+  }
+}
+
+cudaError_t emu_slice(const double* M, long long ld, bool trans, const EmuOperand& op, cudaStream_t s) {
+  if (op.S < 1 || op.S > EMU_MAX_S || op.Rpad % EMU_M || op.Kpad % EMU_KC) return cudaErrorInvalidValue;
+  if (!trans) {
+    GPRX_LAUNCH(emu_exp_rows_kernel, ceil_div(op.Rpad, 128), 128, 0, s, M, ld, op.R, op.K, op.Rpad, op.exps);
+  } else {
+    GPRX_LAUNCH(emu_exp_rows_t_kernel, ceil_div((long long)op.Rpad * 32, 256), 256, 0, s, M, ld, op.R, op.K,
+                op.Rpad, op.exps);
+  }
+  const dim3 grid(op.Rpad / 32, op.Kpad / 64);
+  switch (op.S) {
+    case 4: GPRX_LAUNCH(emu_slice_kernel<4>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.exps, op.slices); break;
+    case 5: GPRX_LAUNCH(emu_slice_kernel<5>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.exps, op.slices); break;
+    case 6: GPRX_LAUNCH(emu_slice_kernel<6>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.exps, op.slices); break;
+    case 7: GPRX_LAUNCH(emu_slice_kernel<7>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.exps, op.slices); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// K-major, no swizzle: LBO = 128 B between K-adjacent core matrices, SBO =
+// 512 B between 8-row groups, version 1 (sm100).
+__device__ __forceinline__ uint64_t emu_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(512u >> 4) << 32) |
+         (1ull << 46);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// Waits for the phase of `parity` with a clock limit (about two seconds).
+__device__ bool emu_wait(uint64_t* bar, uint32_t parity, int* err) {
+  const uint32_t a = smem_u32(bar);
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > 4000000000LL) {
+      if (err) atomicExch(err, 1);
+      return false;
+    }
+  }
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(addr));
+}
+
+// ---------------------------------------------------------------------------
+// GEMM
+// ---------------------------------------------------------------------------
+struct EmuGemmArgs {
+  const int8_t* A;
+  const int8_t* B;
+  const int* expA;
+  const int* expB;
+  int ntrA, ntrB;  // 128-row tiles per plane
+  int M, N, Kpad;
+  double* C;
+  long long ldc;
+  double alpha, beta;
+  int lower;
+  long long row0, col0;
+  int kmode;
+  int* err;
+};
+
+template <int S>
+constexpr int emu_stages() {
+  return S <= 6 ? 3 : 2;
+}
+template <int S>
+constexpr int emu_stage_bytes() {
+  return S * (EMU_M + EMU_N) * EMU_KC;
+}
+
+template <int S>
+__global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g) {
+  constexpr int STAGES = emu_stages<S>();
+  constexpr int A_SL = EMU_M * EMU_KC, B_SL = EMU_N * EMU_KC;
+  constexpr int STAGE = emu_stage_bytes<S>();
+  extern __shared__ __align__(1024) uint8_t emu_smem[];
+  uint8_t* smem = emu_smem;
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+  __shared__ uint32_t tmem_sh;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long i0 = (long long)blockIdx.x * EMU_M, j0 = (long long)blockIdx.y * EMU_N;
+  if (g.lower && i0 + g.row0 + EMU_M - 1 < j0 + g.col0) return;  // wholly above the diagonal
+  const int nkc = g.Kpad / EMU_KC;
+  int kc0 = 0, kc1 = nkc;
+  if (g.kmode == 1) kc0 = (int)(i0 / EMU_KC);
+  else if (g.kmode == 2) kc0 = (int)(j0 / EMU_KC);
+  else if (g.kmode == 3) kc1 = (int)min((long long)nkc, (i0 + EMU_M + EMU_KC - 1) / EMU_KC);
+  const int nch = kc0 < kc1 ? kc1 - kc0 : 0;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                 "r"(512));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int s2 = 0; s2 < STAGES; ++s2) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s2])), "r"(1));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&empty[s2])), "r"(1));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_sh;
+
+  if (tid == 0) {
+    // s32 accumulate, signed A and B, K-major both, M = 128 (N set per MMA)
+    const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(EMU_M >> 4) << 24);
+    const int8_t* Ab = g.A + ((size_t)blockIdx.x * nkc) * 8192;
+    const int8_t* Bb = g.B + ((size_t)(blockIdx.y >> 1) * nkc) * 8192 + (blockIdx.y & 1) * 4096;
+    const size_t planeA = (size_t)g.ntrA * nkc * 8192, planeB = (size_t)g.ntrB * nkc * 8192;
+    bool ok = true;
+    for (int c = 0; c < nch + STAGES - 1 && ok; ++c) {
+      if (c < nch) {
+        const int st = c % STAGES;
+        if (c >= STAGES) ok = emu_wait(&empty[st], (uint32_t)(((c / STAGES) - 1) & 1), g.err);
+        uint8_t* base = smem + st * STAGE;
+        expect_tx(&full[st], (uint32_t)STAGE);
+        const size_t off = (size_t)(kc0 + c) * 8192;
+#pragma unroll
+        for (int p = 0; p < S; ++p) bulk_load(base + p * A_SL, Ab + p * planeA + off, A_SL, &full[st]);
+#pragma unroll
+        for (int q = 0; q < S; ++q) bulk_load(base + S * A_SL + q * B_SL, Bb + q * planeB + off, B_SL, &full[st]);
+      }
+      const int m = c - (STAGES - 1);
+      if (m >= 0 && ok) {
+        const int st = m % STAGES;
+        ok = emu_wait(&full[st], (uint32_t)((m / STAGES) & 1), g.err);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint8_t* base = smem + st * STAGE;
+        const uint32_t a0 = smem_u32(base), b0 = smem_u32(base + S * A_SL);
+#pragma unroll
+        for (int p = 0; p < S; ++p)
+#pragma unroll
+          for (int q0 = 0; q0 < S - p; q0 += 4) {
+            const int nq = (S - p - q0) < 4 ? (S - p - q0) : 4;
+            const uint32_t id = idesc | ((uint32_t)(nq * EMU_N >> 3) << 17);
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk)
+              umma_i8(tmem + (p + q0) * EMU_N, emu_desc(a0 + p * A_SL + kk * 256),
+                      emu_desc(b0 + q0 * B_SL + kk * 256), id, (m > 0 || p > 0 || kk > 0) ? 1u : 0u);
+          }
+        umma_commit(&empty[st]);
+      }
+    }
+    if (nch > 0 && ok) emu_wait(&empty[(nch - 1) % STAGES], (uint32_t)(((nch - 1) / STAGES) & 1), g.err);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  // epilogue: thread = output row
+  const long long i = i0 + warp * 32 + lane;
+  const int ea = i < g.M ? g.expA[i] : 0;
+  const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+  for (int cb = 0; cb < EMU_N; cb += 16) {
+    uint32_t v[S][16];
+#pragma unroll
+    for (int t = 0; t < S; ++t) tmem_ld16(trow + t * EMU_N + cb, v[t]);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const long long j = j0 + cb + u;
+      if (i >= g.M || j >= g.N || (g.lower && i + g.row0 < j + g.col0)) continue;
+      double acc = (double)(int)v[S - 1][u];
+#pragma unroll
+      for (int t = S - 2; t >= 0; --t) acc = fma(acc, 0.0078125, (double)(int)v[t][u]);
+      if (nch == 0) acc = 0.0;
+      const double val = ldexp(acc, -(ea + g.expB[j]));
+      double* cp = g.C + i + j * g.ldc;
+      *cp = g.beta != 0.0 ? fma(g.alpha, val, g.beta * *cp) : g.alpha * val;
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512));
+}
+
+size_t emu_gemm_smem(int S) {
+  return (size_t)(S <= 6 ? 3 : 2) * S * (EMU_M + EMU_N) * EMU_KC;
+}
+
+template <int S>
+static cudaError_t launch_emu(const EmuGemmArgs& g, dim3 grid, cudaStream_t s) {
+  const int smem = (int)emu_gemm_smem(S);
+  cudaError_t e = cudaFuncSetAttribute(emu_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  GPRX_LAUNCH(emu_gemm_kernel<S>, grid, EMU_THREADS, smem, s, g);
+  return cudaGetLastError();
+}
+
+cudaError_t emu_gemm(const EmuOperand& A, const EmuOperand& B, double* C, long long ldc, double alpha, double beta,
+                     bool lower, long long row0, long long col0, int kmode, int* err, cudaStream_t s) {
+  if (A.S != B.S || A.Kpad != B.Kpad || A.S < 4 || A.S > 7) return cudaErrorInvalidValue;
+  if (A.R <= 0 || B.R <= 0) return cudaSuccess;
+  EmuGemmArgs g;
+  g.A = A.slices;
+  g.B = B.slices;
+  g.expA = A.exps;
+  g.expB = B.exps;
+  g.ntrA = A.Rpad / EMU_M;
+  g.ntrB = B.Rpad / EMU_M;
+  g.M = A.R;
+  g.N = B.R;
+  g.Kpad = A.Kpad;
+  g.C = C;
+  g.ldc = ldc;
+  g.alpha = alpha;
+  g.beta = beta;
+  g.lower = lower ? 1 : 0;
+  g.row0 = row0;
+  g.col0 = col0;
+  g.kmode = kmode;
+  g.err = err;
+  // B's padded rows (multiple of 128) cover every 64-row tile the grid touches
+  dim3 grid(A.Rpad / EMU_M, ceil_div(B.R, EMU_N));
+  switch (A.S) {
+    case 4: return launch_emu<4>(g, grid, s);
+    case 5: return launch_emu<5>(g, grid, s);
+    case 6: return launch_emu<6>(g, grid, s);
+    default: return launch_emu<7>(g, grid, s);
+  }
+}
+
+}  // namespace gprx

@@ -4,9 +4,11 @@
 // the blocked factor in isolation.
 
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "dense_f64.cuh"
+#include "emu_gemm.cuh"
 #include "runtime.cuh"
 
 namespace gprx {
@@ -33,6 +35,31 @@ __global__ void fill_spd_kernel(double* a, long long ld, int n) {
     if (i == j) v += 1.0;
     a[i + (long long)j * ld] = v;
   }
+}
+
+__global__ void abs_copy_kernel(const double* a, double* b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = fabs(a[i]);
+}
+
+// rows of a scaled by 2^((r % 9) − 4): the per-row exponents differ
+__global__ void scale_rows_kernel(double* a, long long ld, int rows, int cols) {
+  const long long total = (long long)rows * cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e % rows);
+    a[r + (e / rows) * ld] = ldexp(a[r + (e / rows) * ld], (r % 9) - 4);
+  }
+}
+
+// max over entries of |c − ref| / max(cabs, tiny)
+__global__ void rel_err_kernel(const double* c, const double* ref, const double* cabs, long long n,
+                               unsigned long long* out_bits) {
+  double m = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(c[i] - ref[i]) / fmax(cabs[i], 1e-300));
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out_bits, (unsigned long long)__double_as_longlong(m));
 }
 
 }  // namespace gprx
@@ -109,6 +136,89 @@ gprx_status gprx_probe_potrf(int32_t n, int32_t reps, double* ms_per_factor) {
   if (e != cudaSuccess) return set_cuda_error(e, "probe potrf");
   if (hs.code != GPRX_OK) return set_error(hs.code, "probe potrf status");
   *ms_per_factor = total / reps;
+  return GPRX_OK;
+}
+
+// The int8-sliced FP64 product C = A·Bᵀ (A m×k, B n×k, S slices) against the
+// FP64 DMMA product: out[0] ms per emulated GEMM, out[1] ms to slice both
+// operands, out[2] ms per DMMA GEMM, out[3] max |C − C_ref| / (|A|·|B|ᵀ).
+gprx_status gprx_probe_emu_gemm(int32_t m, int32_t n, int32_t k, int32_t S, int32_t reps, double* out) {
+  if (m <= 0 || n <= 0 || k <= 0 || reps <= 0 || !out || S < 4 || S > 7)
+    return set_error(GPRX_INVALID_ARGUMENT, "sizes");
+  DevBuf<double> A, B, Aa, Ba, C, R, Cabs;
+  DevBuf<int8_t> sa, sb;
+  DevBuf<int> ea, eb, err;
+  DevBuf<unsigned long long> mx;
+  EmuOperand a, b;
+  a.R = m; a.K = k; a.S = S; a.Rpad = emu_pad_rows(m); a.Kpad = emu_pad_k(k);
+  b.R = n; b.K = k; b.S = S; b.Rpad = emu_pad_rows(n); b.Kpad = emu_pad_k(k);
+  const size_t sza = (size_t)m * k, szb = (size_t)n * k, szc = (size_t)m * n;
+  if (A.alloc(sza) || B.alloc(szb) || Aa.alloc(sza) || Ba.alloc(szb) || C.alloc(szc) || R.alloc(szc) ||
+      Cabs.alloc(szc) || sa.alloc(emu_slice_bytes(m, k, S)) || sb.alloc(emu_slice_bytes(n, k, S)) ||
+      ea.alloc(a.Rpad) || eb.alloc(b.Rpad) || err.alloc(1) || mx.alloc(1))
+    return set_error(GPRX_OUT_OF_MEMORY, "probe buffers");
+  a.slices = sa.p; a.exps = ea.p; b.slices = sb.p; b.exps = eb.p;
+  cudaStream_t s;
+  GPRX_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  fill_pattern_kernel<<<1184, 256, 0, s>>>(A.p, (long long)sza, 3u);
+  fill_pattern_kernel<<<1184, 256, 0, s>>>(B.p, (long long)szb, 4u);
+  scale_rows_kernel<<<1184, 256, 0, s>>>(A.p, m, m, k);
+  abs_copy_kernel<<<1184, 256, 0, s>>>(A.p, Aa.p, (long long)sza);
+  abs_copy_kernel<<<1184, 256, 0, s>>>(B.p, Ba.p, (long long)szb);
+  cudaMemsetAsync(err.p, 0, sizeof(int), s);
+  cudaMemsetAsync(mx.p, 0, sizeof(unsigned long long), s);
+  GemmParams pr = gemm_params(m, n, k, A.p, m, B.p, n, R.p, m, 1.0, 0.0, nullptr);
+  GemmParams pa = gemm_params(m, n, k, Aa.p, m, Ba.p, n, Cabs.p, m, 1.0, 0.0, nullptr);
+  cudaError_t e = dgemm(false, true, pr, s);
+  if (e == cudaSuccess) e = dgemm(false, true, pa, s);
+  if (e == cudaSuccess) e = emu_slice(A.p, m, false, a, s);
+  if (e == cudaSuccess) e = emu_slice(B.p, n, false, b, s);
+  if (e == cudaSuccess) e = emu_gemm(a, b, C.p, m, 1.0, 0.0, false, 0, 0, 0, err.p, s);
+  if (e == cudaSuccess) {
+    rel_err_kernel<<<592, 256, 0, s>>>(C.p, R.p, Cabs.p, (long long)szc, mx.p);
+    e = cudaGetLastError();
+  }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float t_emu = 0.f, t_slice = 0.f, t_d = 0.f;
+  if (e == cudaSuccess) {
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = emu_gemm(a, b, C.p, m, 1.0, 0.0, false, 0, 0, 0, err.p, s);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&t_emu, e0, e1);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+      e = emu_slice(A.p, m, false, a, s);
+      if (e == cudaSuccess) e = emu_slice(B.p, n, false, b, s);
+    }
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&t_slice, e0, e1);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = dgemm(false, true, pr, s);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&t_d, e0, e1);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  int herr = 0;
+  unsigned long long hm = 0;
+  cudaMemcpy(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&hm, mx.p, sizeof(hm), cudaMemcpyDeviceToHost);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(s);
+  if (e != cudaSuccess) return set_cuda_error(e, "probe emu gemm");
+  if (e2 != cudaSuccess) return set_cuda_error(e2, "probe emu gemm sync");
+  if (herr) return set_error(GPRX_TIMEOUT, "emulated GEMM: a bounded wait ran out");
+  out[0] = t_emu / reps;
+  out[1] = t_slice / reps;
+  out[2] = t_d / reps;
+  double hd;
+  std::memcpy(&hd, &hm, sizeof(hd));
+  out[3] = hd;
   return GPRX_OK;
 }
 
