@@ -13,6 +13,7 @@
 #include <algorithm>
 
 #include "dense_f64.cuh"
+#include "emu_gemm.cuh"
 #include "diag_block.cuh"
 
 namespace gprx {
@@ -339,6 +340,74 @@ cudaError_t trtri_blocked(const double* L, long long ld, int n, const double* li
     }
   }
   return cudaGetLastError();
+}
+
+cudaError_t trtri_blocked_emu(const double* L, long long ld, int n, const double* linv, double* X, long long ldx,
+                              double* scratch, const EmuWork& w, int emu_min, DevStatus* st, cudaStream_t s) {
+  int nblk = ceil_div(n, NB);
+  GPRX_LAUNCH(copy_diag_blocks_kernel, nblk, 256, 0, s, linv, n, X, ldx);
+  for (long long b = 2LL * NB; b < 2LL * n; b *= 2) {
+    long long h = b / 2;
+    if (h >= n) break;
+    long long full = n / b;
+    long long r = n - full * b;
+    for (int part = 0; part < 2; ++part) {
+      long long s0, cnt, h2;
+      if (part == 0) {
+        if (full == 0) continue;
+        s0 = 0;
+        cnt = full;
+        h2 = h;
+      } else {
+        if (r <= h) continue;
+        s0 = full * b;
+        cnt = 1;
+        h2 = r - h;
+      }
+      if (h < emu_min) {
+        GemmParams p1 = gemm_params((int)h2, (int)h, (int)h, L + (s0 + h) + s0 * ld, ld, X + s0 + s0 * ldx, ldx,
+                                    scratch, h2, 1.0, 0.0, st);
+        p1.mode = GEMM_K_FROM_COL;
+        p1.strideA = b + b * ld;
+        p1.strideB = b + b * ldx;
+        p1.strideC = h2 * h;
+        CK(dgemm(false, false, p1, s, (int)cnt));
+        GemmParams p2 = gemm_params((int)h2, (int)h, (int)h2, X + (s0 + h) + (s0 + h) * ldx, ldx, scratch, h2,
+                                    X + (s0 + h) + s0 * ldx, ldx, -1.0, 0.0, st);
+        p2.mode = GEMM_K_TO_ROW;
+        p2.strideA = b + b * ldx;
+        p2.strideB = h2 * h;
+        p2.strideC = b + b * ldx;
+        CK(dgemm(false, false, p2, s, (int)cnt));
+        continue;
+      }
+      for (long long c = 0; c < cnt; ++c) {
+        const long long o = s0 + c * b;
+        // T = L21 · X11 (rows of L21 against the columns of X11; X11 lower:
+        // k from the tile's first column)
+        EmuOperand a = w.op_a((int)h2, (int)h), bo = w.op_b((int)h, (int)h);
+        CK(emu_slice(L + (o + h) + o * ld, ld, false, a, s));
+        CK(emu_slice(X + o + o * ldx, ldx, true, bo, s));
+        CK(emu_gemm(a, bo, scratch, h2, 1.0, 0.0, false, 0, 0, 2, w.err, s));
+        // X21 = −X22 · T (X22 lower: k up to the tile's last row)
+        EmuOperand a2 = w.op_a((int)h2, (int)h2), b2 = w.op_b((int)h, (int)h2);
+        CK(emu_slice(X + (o + h) + (o + h) * ldx, ldx, false, a2, s));
+        CK(emu_slice(scratch, h2, true, b2, s));
+        CK(emu_gemm(a2, b2, X + (o + h) + o * ldx, ldx, -1.0, 0.0, false, 0, 0, 3, w.err, s));
+      }
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t lauum_lower_emu(const double* X, long long ldx, int n, double* C, long long ldc, const EmuWork& w,
+                            DevStatus* st, cudaStream_t s) {
+  (void)st;
+  // C(i, j) = Σ_k X(k,i) X(k,j): both operands are the rows of Xᵀ; lower,
+  // k from the tile's first row
+  EmuOperand a = w.op_a(n, n);
+  CK(emu_slice(X, ldx, true, a, s));
+  return emu_gemm(a, a, C, ldc, 1.0, 0.0, true, 0, 0, 1, w.err, s);
 }
 
 cudaError_t lauum_lower(const double* X, long long ldx, int n, double* C, long long ldc, DevStatus* st,

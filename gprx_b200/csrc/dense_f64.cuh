@@ -75,6 +75,15 @@ cudaError_t col_sumsq(const double* M, long long ld, int nrows, int ncols, const
 // out = Σ_i a_i b_i (single block, deterministic).
 cudaError_t dot_dev(const double* a, const double* b, int n, double* out, DevStatus* st, cudaStream_t s);
 
+// The same two products with the FP64 GEMMs emulated on the int8 tensor
+// cores (emu_gemm.cuh) wherever the blocks are at least emu_min wide; the
+// narrower levels stay on DMMA.  X's strict upper triangle must be zero.
+struct EmuWork;
+cudaError_t trtri_blocked_emu(const double* L, long long ld, int n, const double* linv, double* X, long long ldx,
+                              double* scratch, const EmuWork& w, int emu_min, DevStatus* st, cudaStream_t s);
+cudaError_t lauum_lower_emu(const double* X, long long ldx, int n, double* C, long long ldc, const EmuWork& w,
+                            DevStatus* st, cudaStream_t s);
+
 // Sets X (n×n, ld) to the identity (full columns, zero off the diagonal).
 cudaError_t set_identity(double* X, long long ld, int n, cudaStream_t s);
 

@@ -28,34 +28,32 @@ namespace gprx {
 // ---------------------------------------------------------------------------
 // slicing
 // ---------------------------------------------------------------------------
-// exps[r] = 6 − E with max_k |op(r,k)| = m·2^E, m ∈ [0.5, 1): the scaled row
-// maximum lies in [32, 64).
-__global__ void emu_exp_rows_kernel(const double* M, long long ld, int R, int K, int Rpad, int* exps) {
-  // trans = false: row r is M[r + k·ld]; consecutive threads take consecutive
-  // rows, so every k step is one coalesced access per warp
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= Rpad) return;
-  double mx = 0.0;
-  if (r < R)
-    for (int k = 0; k < K; ++k) mx = fmax(mx, fabs(M[r + (long long)k * ld]));
-  int E = 0;
-  frexp(mx, &E);
-  exps[r] = mx > 0.0 ? 6 - E : 0;
-}
-
-__global__ void emu_exp_rows_t_kernel(const double* M, long long ld, int R, int K, int Rpad, int* exps) {
-  // trans = true: row r is M[k + r·ld], contiguous; one warp per row
-  const int r = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (r >= Rpad) return;
-  double mx = 0.0;
-  if (r < R)
-    for (int k = lane; k < K; k += 32) mx = fmax(mx, fabs(M[k + (long long)r * ld]));
+// Row maxima of |op(r,k)| over 32 × 64 tiles (atomicMax on the bit pattern:
+// non-negative doubles order like their bits).
+__global__ void __launch_bounds__(256) emu_rowmax_kernel(const double* M, long long ld, bool trans, int R, int K,
+                                                         unsigned long long* rmax) {
+  __shared__ double t[32][65];
+  const int r0 = blockIdx.x * 32, k0 = blockIdx.y * 64, tid = threadIdx.x;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if (lane == 0) {
-    int E = 0;
-    frexp(mx, &E);
-    exps[r] = mx > 0.0 ? 6 - E : 0;
+  for (int i = 0; i < 8; ++i) {
+    int r, k;
+    if (!trans) {
+      r = tid & 31;
+      k = (tid >> 5) + 8 * i;
+    } else {
+      k = tid & 63;
+      r = (tid >> 6) + 4 * i;
+    }
+    const int gr = r0 + r, gk = k0 + k;
+    double a = 0.0;
+    if (gr < R && gk < K) a = fabs(trans ? M[gk + (long long)gr * ld] : M[gr + (long long)gk * ld]);
+    t[r][k] = a;
+  }
+  __syncthreads();
+  if (tid < 32) {
+    double m = 0.0;
+    for (int k = 0; k < 64; ++k) m = fmax(m, t[tid][k]);
+    if (r0 + tid < R && m > 0.0) atomicMax(rmax + r0 + tid, (unsigned long long)__double_as_longlong(m));
   }
 }
 
@@ -64,7 +62,8 @@ __global__ void emu_exp_rows_t_kernel(const double* M, long long ld, int R, int 
 // 8 digits of one row for every slice plane into the pre-tiled layout.
 template <int S>
 __global__ void __launch_bounds__(256) emu_slice_kernel(const double* M, long long ld, bool trans, int R, int K,
-                                                        int Rpad, int Kpad, const int* exps, int8_t* out) {
+                                                        int Rpad, int Kpad, const unsigned long long* rmax,
+                                                        int* exps, int8_t* out) {
   __shared__ double t[32][65];
   const int r0 = blockIdx.x * 32, kc = blockIdx.y, k0 = kc * 64, tid = threadIdx.x;
 #pragma unroll
@@ -85,7 +84,13 @@ __global__ void __launch_bounds__(256) emu_slice_kernel(const double* M, long lo
   __syncthreads();
   const int r = tid >> 3, c8 = tid & 7, gr = r0 + r;
   if (gr >= Rpad) return;
-  const int e = exps[gr];
+  // exponent e = 6 − E with max_k |op(r,k)| = m·2^E, m ∈ [0.5, 1): the scaled
+  // row maximum lies in [32, 64)
+  const double mx = __longlong_as_double((long long)rmax[gr]);
+  int E = 0;
+  frexp(mx, &E);
+  const int e = mx > 0.0 ? 6 - E : 0;
+  if (blockIdx.y == 0 && c8 == 0) exps[gr] = e;
   uint32_t w[S][2];
 #pragma unroll
   for (int p = 0; p < S; ++p) w[p][0] = w[p][1] = 0u;
@@ -109,20 +114,16 @@ __global__ void __launch_bounds__(256) emu_slice_kernel(const double* M, long lo
 }
 
 cudaError_t emu_slice(const double* M, long long ld, bool trans, const EmuOperand& op, cudaStream_t s) {
-  if (op.S < 1 || op.S > EMU_MAX_S || op.Rpad % EMU_M || op.Kpad % EMU_KC) return cudaErrorInvalidValue;
-  if (!trans) {
-    GPRX_LAUNCH(emu_exp_rows_kernel, ceil_div(op.Rpad, 128), 128, 0, s, M, ld, op.R, op.K, op.Rpad, op.exps);
-  } else {
-    GPRX_LAUNCH(emu_exp_rows_t_kernel, ceil_div((long long)op.Rpad * 32, 256), 256, 0, s, M, ld, op.R, op.K,
-                op.Rpad, op.exps);
-  }
+  if (op.S < 4 || op.S > 7 || op.Rpad % EMU_M || op.Kpad % EMU_KC || !op.rmax) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(op.rmax, 0, sizeof(unsigned long long) * op.Rpad, s);
+  if (e != cudaSuccess) return e;
   const dim3 grid(op.Rpad / 32, op.Kpad / 64);
+  GPRX_LAUNCH(emu_rowmax_kernel, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.rmax);
   switch (op.S) {
-    case 4: GPRX_LAUNCH(emu_slice_kernel<4>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.exps, op.slices); break;
-    case 5: GPRX_LAUNCH(emu_slice_kernel<5>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.exps, op.slices); break;
-    case 6: GPRX_LAUNCH(emu_slice_kernel<6>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.exps, op.slices); break;
-    case 7: GPRX_LAUNCH(emu_slice_kernel<7>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.exps, op.slices); break;
-    default: return cudaErrorInvalidValue;
+    case 4: GPRX_LAUNCH(emu_slice_kernel<4>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
+    case 5: GPRX_LAUNCH(emu_slice_kernel<5>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
+    case 6: GPRX_LAUNCH(emu_slice_kernel<6>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
+    default: GPRX_LAUNCH(emu_slice_kernel<7>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
   }
   return cudaGetLastError();
 }

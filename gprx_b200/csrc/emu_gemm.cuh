@@ -29,11 +29,13 @@ constexpr int EMU_MAX_S = 8;  // S terms × 64 columns ≤ 512 TMEM columns
 
 // Row slices of an FP64 operand op(M) with R rows and K columns:
 //   op(M)(r, k) = trans ? M[k + r·ld] : M[r + k·ld].
-// Planes p = 0..S-1 of Rpad × Kpad int8 (row r contiguous in k, zero
-// padding); exps[r] the row's power-of-two exponent.
+// S planes of Rpad × Kpad int8 digits (zero padding), stored pre-tiled in
+// 8 KB blocks of 128 rows × 64 bytes of K in the UMMA core-matrix order (see
+// emu_gemm.cu); exps[r] the row's power-of-two exponent.
 struct EmuOperand {
   int8_t* slices = nullptr;
   int* exps = nullptr;
+  unsigned long long* rmax = nullptr;  // Rpad words of scratch (row maxima)
   int R = 0, K = 0, Rpad = 0, Kpad = 0, S = 0;
 };
 
@@ -54,5 +56,28 @@ cudaError_t emu_gemm(const EmuOperand& A, const EmuOperand& B, double* C, long l
                      bool lower, long long row0, long long col0, int kmode, int* err, cudaStream_t s);
 
 size_t emu_gemm_smem(int S);
+
+// Device scratch for the products of one handle: slice planes and exponents
+// of two operands sized for n×n, and the bounded-wait error flag.
+struct EmuWork {
+  int8_t* sa = nullptr;
+  int8_t* sb = nullptr;
+  int* ea = nullptr;
+  int* eb = nullptr;
+  unsigned long long* ma = nullptr;
+  unsigned long long* mb = nullptr;
+  int* err = nullptr;
+  int S = 6;
+  EmuOperand op_a(int R, int K) const {
+    EmuOperand o;
+    o.slices = sa; o.exps = ea; o.rmax = ma; o.R = R; o.K = K; o.Rpad = emu_pad_rows(R); o.Kpad = emu_pad_k(K); o.S = S;
+    return o;
+  }
+  EmuOperand op_b(int R, int K) const {
+    EmuOperand o;
+    o.slices = sb; o.exps = eb; o.rmax = mb; o.R = R; o.K = K; o.Rpad = emu_pad_rows(R); o.Kpad = emu_pad_k(K); o.S = S;
+    return o;
+  }
+};
 
 }  // namespace gprx

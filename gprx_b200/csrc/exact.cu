@@ -185,6 +185,16 @@ gprx_status ExactState::factor_current() {
   return GPRX_OK;
 }
 
+gprx_status ExactState::ensure_emu() {
+  const size_t bytes = emu_slice_bytes(cap, cap, 7);
+  const size_t rows = (size_t)emu_pad_rows(cap);
+  if (emu_sa.ensure(bytes) || emu_sb.ensure(bytes) || emu_ea.ensure(rows) || emu_eb.ensure(rows) ||
+      emu_ma.ensure(rows) || emu_mb.ensure(rows) || emu_err.ensure(1))
+    return set_error(GPRX_OUT_OF_MEMORY, "device allocation of the emulated-product scratch failed");
+  GPRX_CUDA_TRY(emu_err_h.ensure(1));
+  return GPRX_OK;
+}
+
 gprx_status ExactState::eval(const double* params, double* nlml_out, double* grad) {
   const int p = num_params();
   std::vector<double> prev(p);
@@ -212,11 +222,27 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
     if ((st = enqueue_factor(j)) != GPRX_OK) return st;
     GPRX_CUDA_TRY(logdet_diag(A.p, ld, n, false, res.p + 0, status.p, stream));
     if (grad) {
-      GPRX_CUDA_TRY(trtri_blocked(A.p, ld, n, linv.p, Xinv.p, ld, scratch.p, status.p, stream));
+      const bool emu = use_emu();
+      EmuWork ew;
+      if (emu) {
+        if ((st = ensure_emu()) != GPRX_OK) return st;
+        ew.sa = emu_sa.p; ew.sb = emu_sb.p; ew.ea = emu_ea.p; ew.eb = emu_eb.p; ew.ma = emu_ma.p; ew.mb = emu_mb.p;
+        ew.err = emu_err.p;
+        ew.S = 7;
+        GPRX_CUDA_TRY(cudaMemsetAsync(emu_err.p, 0, sizeof(int), stream));
+        GPRX_CUDA_TRY(trtri_blocked_emu(A.p, ld, n, linv.p, Xinv.p, ld, scratch.p, ew, EMU_MIN_N, status.p, stream));
+      } else {
+        GPRX_CUDA_TRY(trtri_blocked(A.p, ld, n, linv.p, Xinv.p, ld, scratch.p, status.p, stream));
+      }
       GPRX_CUDA_TRY(trmv_lower(Xinv.p, ld, n, y.p, z.p, status.p, stream));
       GPRX_CUDA_TRY(gemv_t(Xinv.p, ld, n, n, true, z.p, alpha.p, status.p, stream));
       GPRX_CUDA_TRY(dot_dev(y.p, alpha.p, n, res.p + 1, status.p, stream));
-      GPRX_CUDA_TRY(lauum_lower(Xinv.p, ld, n, A.p, ld, status.p, stream));
+      if (emu) {
+        GPRX_CUDA_TRY(lauum_lower_emu(Xinv.p, ld, n, A.p, ld, ew, status.p, stream));
+        GPRX_CUDA_TRY(cudaMemcpyAsync(emu_err_h.p, emu_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+      } else {
+        GPRX_CUDA_TRY(lauum_lower(Xinv.p, ld, n, A.p, ld, status.p, stream));
+      }
       GPRX_CUDA_TRY(cudaEventRecord(ev[3], stream));
       int blocks = 0;
       GPRX_CUDA_TRY(grad_contract(kern, x.p, cap, n, A.p, ld, alpha.p, partials.p, &blocks, status.p, stream));
@@ -235,6 +261,11 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
     DevStatus ds;
     if ((st = read_status(&ds)) != GPRX_OK) return st;
     ev_recorded = true;
+    if (ds.code == GPRX_OK && grad && use_emu() && *emu_err_h.p != 0) {
+      write_params(prev.data());
+      factor_current();
+      return set_error(GPRX_TIMEOUT, "an emulated product's bounded wait ran out");
+    }
     if (ds.code == GPRX_OK) {
       jitter = j;
       factor_ok = grad == nullptr;  // the gradient overwrote L with K⁻¹

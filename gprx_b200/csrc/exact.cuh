@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "dense_f64.cuh"
+#include "emu_gemm.cuh"
 #include "kernels.cuh"
 #include "runtime.cuh"
 
@@ -40,6 +41,11 @@ struct ExactState {
   HostPinned<double> res_h;
   HostPinned<DevStatus> status_h;
   DevBuf<double> qbuf, qx;  // predict scratch
+  // mixed precision: the inverse's products emulated on the int8 tensor cores
+  DevBuf<int8_t> emu_sa, emu_sb;
+  DevBuf<int> emu_ea, emu_eb, emu_err;
+  DevBuf<unsigned long long> emu_ma, emu_mb;
+  HostPinned<int> emu_err_h;
 
   bool factor_ok = false;   // A holds L (LLT) of the current θ
   bool alpha_ok = false;
@@ -56,6 +62,10 @@ struct ExactState {
   gprx_status create(const double* x, uint64_t n, uint64_t d, const double* y, const gprx_kernel_node* nodes,
                      int n_nodes, const double* theta, int n_theta, const gprx_options* o);
   int num_params() const { return kern.n_params + 1; }
+  // smallest n whose inverse uses the emulated products
+  static constexpr int EMU_MIN_N = 1024;
+  bool use_emu() const { return opt.precision == GPRX_PRECISION_MIXED && n >= EMU_MIN_N; }
+  gprx_status ensure_emu();
   void get_params(double* out) const;
   gprx_status write_params(const double* params);
   double noise() const { return std::exp(log_noise); }

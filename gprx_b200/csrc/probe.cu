@@ -148,16 +148,17 @@ gprx_status gprx_probe_emu_gemm(int32_t m, int32_t n, int32_t k, int32_t S, int3
   DevBuf<double> A, B, Aa, Ba, C, R, Cabs;
   DevBuf<int8_t> sa, sb;
   DevBuf<int> ea, eb, err;
-  DevBuf<unsigned long long> mx;
+  DevBuf<unsigned long long> mx, rma, rmb;
   EmuOperand a, b;
   a.R = m; a.K = k; a.S = S; a.Rpad = emu_pad_rows(m); a.Kpad = emu_pad_k(k);
   b.R = n; b.K = k; b.S = S; b.Rpad = emu_pad_rows(n); b.Kpad = emu_pad_k(k);
   const size_t sza = (size_t)m * k, szb = (size_t)n * k, szc = (size_t)m * n;
   if (A.alloc(sza) || B.alloc(szb) || Aa.alloc(sza) || Ba.alloc(szb) || C.alloc(szc) || R.alloc(szc) ||
       Cabs.alloc(szc) || sa.alloc(emu_slice_bytes(m, k, S)) || sb.alloc(emu_slice_bytes(n, k, S)) ||
-      ea.alloc(a.Rpad) || eb.alloc(b.Rpad) || err.alloc(1) || mx.alloc(1))
+      ea.alloc(a.Rpad) || eb.alloc(b.Rpad) || err.alloc(1) || mx.alloc(1) || rma.alloc(a.Rpad) ||
+      rmb.alloc(b.Rpad))
     return set_error(GPRX_OUT_OF_MEMORY, "probe buffers");
-  a.slices = sa.p; a.exps = ea.p; b.slices = sb.p; b.exps = eb.p;
+  a.slices = sa.p; a.exps = ea.p; a.rmax = rma.p; b.slices = sb.p; b.exps = eb.p; b.rmax = rmb.p;
   cudaStream_t s;
   GPRX_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   fill_pattern_kernel<<<1184, 256, 0, s>>>(A.p, (long long)sza, 3u);

@@ -1,0 +1,82 @@
+"""The mixed-precision exact evaluation (Precision.Mixed) against the FP64
+oracle and against the plain FP64 GPU path.
+
+In the mixed form the products of the inverse stage (the triangular inverse's
+block products and K⁻¹ = XᵀX) run on the int8 tensor cores as sliced FP64
+emulations (6 int8 digits of 7 bits per row-scaled entry, exact int32 sums);
+the fill, the factor, the log-det and the gradient contraction stay FP64.
+Targets: NLML within 1e-8 and gradient within 1e-6 relative to FP64,
+|a − e| / max(|e|, 1).  Sizes from n = 1024 (the smallest n that uses the
+emulated products) up, ragged ones included.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+import gprx_b200 as gx
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+TOL_NLML = 1e-8
+TOL_GRAD = 1e-6
+
+
+def make_data(n, d, seed):
+    rs = np.random.RandomState(seed)
+    x = rs.standard_normal(n * d)
+    y = np.sin(x[:n]) + 0.5 * np.cos(x[n:2 * n] if d > 1 else x[:n]) + 0.05 * rs.standard_normal(n)
+    return x, y
+
+
+def model(spec, noise, x, n, d, y, precision):
+    return gx.Gpr(spec, gx.GaussianLikelihood(noise), precision=precision).with_optimizer(gx.Fixed()).factor(
+        x, n, d, y)
+
+
+@pytest.mark.parametrize("n", [1024, 1100, 1536, 2100])
+def test_mixed_eval_matches_oracle_ard8(n):
+    d = 8
+    rs = np.random.RandomState(n)
+    ls = np.exp(rs.uniform(math.log(0.3), math.log(3.0), size=d))
+    spec = gx.ConstantKernel(2.0) * gx.RbfArdKernel(list(ls))
+    nodes = [[2, 2], [12, 0], [11, d]]
+    x, y = make_data(n, d, seed=n + 1)
+    m = model(spec, 0.0025, x, n, d, y, gx.Precision.Mixed)
+    f = model(spec, 0.0025, x, n, d, y, gx.Precision.Fp64)
+    theta = np.array([math.log(2.0)] + list(np.log(ls)) + [math.log(0.0025)])
+    for k in range(2):
+        params = theta + 0.1 * rs.standard_normal(theta.size)
+        nl_o, g_o, _, _ = O.exact_eval(nodes, params, x, n, d, y)
+        nl, g = m.value_and_gradient(params)
+        nl_f, g_f = f.value_and_gradient(params)
+        assert O.rel_err(nl, nl_o) <= TOL_NLML, (nl, nl_o)
+        assert np.all(O.rel_err(g, g_o) <= TOL_GRAD), (g, g_o)
+        assert O.rel_err(nl, nl_f) <= TOL_NLML
+        assert np.all(O.rel_err(g, g_f) <= TOL_GRAD)
+
+
+def test_mixed_eval_matches_oracle_rbf_plus_periodic():
+    n, d = 1300, 1
+    spec = gx.RbfKernel(0.8) + gx.PeriodicKernel(1.1, 2.0)
+    nodes = [[1, 2], [10, 0], [13, 0]]
+    x, y = make_data(n, d, seed=3)
+    m = model(spec, 0.01, x, n, d, y, gx.Precision.Mixed)
+    params = np.array([math.log(0.8), math.log(1.1), math.log(2.0), math.log(0.01)])
+    nl_o, g_o, _, _ = O.exact_eval(nodes, params, x, n, d, y)
+    nl, g = m.value_and_gradient(params)
+    assert O.rel_err(nl, nl_o) <= TOL_NLML
+    assert np.all(O.rel_err(g, g_o) <= TOL_GRAD)
+
+
+def test_mixed_small_n_is_the_fp64_path():
+    # below n = 1024 the mixed form runs the FP64 products: same bits
+    n, d = 700, 3
+    spec = gx.ConstantKernel(1.5) * gx.RbfArdKernel([0.7, 1.2, 2.0])
+    x, y = make_data(n, d, seed=9)
+    params = np.array([math.log(1.5), math.log(0.7), math.log(1.2), math.log(2.0), math.log(0.05)])
+    a = model(spec, 0.05, x, n, d, y, gx.Precision.Mixed).value_and_gradient(params)
+    b = model(spec, 0.05, x, n, d, y, gx.Precision.Fp64).value_and_gradient(params)
+    assert a[0] == b[0] and np.array_equal(a[1], b[1])
