@@ -400,6 +400,47 @@ cudaError_t trtri_blocked_emu(const double* L, long long ld, int n, const double
   return cudaGetLastError();
 }
 
+cudaError_t potrf_trtri_rec(double* A, long long ld, int n, double* X, long long ldx, double* linv,
+                            double* scratch, const EmuWork& w, int leaf, int emu_min, DevStatus* st,
+                            cudaStream_t s, FactorCtx* ctx) {
+  if (n <= leaf) {
+    CK(potrf_blocked(A, ld, n, linv, st, s, ctx));
+    return trtri_blocked_emu(A, ld, n, linv, X, ldx, scratch, w, emu_min, st, s);
+  }
+  const int n1 = (n / 2 + NB - 1) / NB * NB, n2 = n - n1;
+  CK(potrf_trtri_rec(A, ld, n1, X, ldx, linv, scratch, w, leaf, emu_min, st, s, ctx));
+  double* A21 = A + n1;
+  double* A22 = A + n1 + (long long)n1 * ld;
+  // L21 = A21 X11ᵀ (rows of A21 against the rows of X11, k ≤ j), written over A21
+  {
+    EmuOperand a = w.op_a(n2, n1), b = w.op_b(n1, n1);
+    CK(emu_slice(A21, ld, false, a, s));
+    CK(emu_slice(X, ldx, false, b, s));
+    CK(emu_gemm(a, b, A21, ld, 1.0, 0.0, false, 0, 0, 4, w.err, s));
+  }
+  // A22 −= L21 L21ᵀ (lower)
+  {
+    EmuOperand l = w.op_a(n2, n1);
+    CK(emu_slice(A21, ld, false, l, s));
+    CK(emu_gemm(l, l, A22, ld, -1.0, 1.0, true, 0, 0, 0, w.err, s));
+  }
+  CK(potrf_trtri_rec(A22, ld, n2, X + n1 + (long long)n1 * ldx, ldx, linv + (long long)(n1 / NB) * NB * NB, scratch,
+                     w, leaf, emu_min, st, s, ctx));
+  // T = L21 X11 (X11 lower: k from the tile's first column), X21 = −X22 T
+  // (X22 lower: k up to the tile's last row)
+  {
+    EmuOperand a = w.op_a(n2, n1), b = w.op_b(n1, n1);
+    CK(emu_slice(A21, ld, false, a, s));
+    CK(emu_slice(X, ldx, true, b, s));
+    CK(emu_gemm(a, b, scratch, n2, 1.0, 0.0, false, 0, 0, 2, w.err, s));
+    EmuOperand a2 = w.op_a(n2, n2), b2 = w.op_b(n1, n2);
+    CK(emu_slice(X + n1 + (long long)n1 * ldx, ldx, false, a2, s));
+    CK(emu_slice(scratch, n2, true, b2, s));
+    CK(emu_gemm(a2, b2, X + n1, ldx, -1.0, 0.0, false, 0, 0, 3, w.err, s));
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t lauum_lower_emu(const double* X, long long ldx, int n, double* C, long long ldc, const EmuWork& w,
                             DevStatus* st, cudaStream_t s) {
   (void)st;

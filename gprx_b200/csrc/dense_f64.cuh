@@ -84,6 +84,16 @@ cudaError_t trtri_blocked_emu(const double* L, long long ld, int n, const double
 cudaError_t lauum_lower_emu(const double* X, long long ldx, int n, double* C, long long ldc, const EmuWork& w,
                             DevStatus* st, cudaStream_t s);
 
+// Lower LLT of A (n×n) and X = L⁻¹ together by recursive halving: A11 → (L11,
+// X11) recursively, L21 = A21 X11ᵀ, A22 −= L21 L21ᵀ, A22 → (L22, X22),
+// X21 = −X22 (L21 X11), the coupling products as emulated FP64 GEMMs; blocks
+// of at most `leaf` rows use potrf_blocked and trtri_blocked_emu.  linv gets
+// the diagonal-block inverses (block index = row / NB); scratch holds
+// ceil(n/2)² doubles.  X's strict upper triangle must be zero.
+cudaError_t potrf_trtri_rec(double* A, long long ld, int n, double* X, long long ldx, double* linv,
+                            double* scratch, const EmuWork& w, int leaf, int emu_min, DevStatus* st,
+                            cudaStream_t s, FactorCtx* ctx);
+
 // Sets X (n×n, ld) to the identity (full columns, zero off the diagonal).
 cudaError_t set_identity(double* X, long long ld, int n, cudaStream_t s);
 

@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
   if (g.kmode == 1) kc0 = (int)(i0 / EMU_KC);
   else if (g.kmode == 2) kc0 = (int)(j0 / EMU_KC);
   else if (g.kmode == 3) kc1 = (int)min((long long)nkc, (i0 + EMU_M + EMU_KC - 1) / EMU_KC);
+  else if (g.kmode == 4) kc1 = (int)min((long long)nkc, (j0 + EMU_N + EMU_KC - 1) / EMU_KC);
   const int nch = kc0 < kc1 ? kc1 - kc0 : 0;
 
   if (warp == 0) {

@@ -49,8 +49,9 @@ inline size_t emu_slice_bytes(int R, int K, int S) {
 cudaError_t emu_slice(const double* M, long long ld, bool trans, const EmuOperand& op, cudaStream_t s);
 
 // C(i, j) = beta·C + alpha · Σ_{k ∈ [kb, K)} A(i,k) B(j,k) for i < A.R, j < B.R.
-// lower: only i + row0 ≥ j + col0 is written.  kmode as in cta_gemm
-// (0 full; 1 k from the tile's first row; 2 k from the tile's first column).
+// lower: only i + row0 ≥ j + col0 is written.  kmode (triangular operands):
+// 0 full K; 1 k from the tile's first row; 2 k from the tile's first column;
+// 3 k up to the tile's last row; 4 k up to the tile's last column.
 // err: device int set to 1 when a bounded wait gave up (never expected).
 cudaError_t emu_gemm(const EmuOperand& A, const EmuOperand& B, double* C, long long ldc, double alpha, double beta,
                      bool lower, long long row0, long long col0, int kmode, int* err, cudaStream_t s);

@@ -219,21 +219,29 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
   for (double j : js) {
     last = j;
     if ((st = reset_status()) != GPRX_OK) return st;
-    if ((st = enqueue_factor(j)) != GPRX_OK) return st;
+    const bool emu = grad && use_emu();
+    EmuWork ew;
+    if (emu) {
+      // fill, then L and X = L⁻¹ together by recursive halving with the
+      // coupling products emulated
+      if ((st = ensure_emu()) != GPRX_OK) return st;
+      ew.sa = emu_sa.p; ew.sb = emu_sb.p; ew.ea = emu_ea.p; ew.eb = emu_eb.p; ew.ma = emu_ma.p; ew.mb = emu_mb.p;
+      ew.err = emu_err.p;
+      ew.S = 7;
+      GPRX_CUDA_TRY(cudaMemsetAsync(emu_err.p, 0, sizeof(int), stream));
+      GPRX_CUDA_TRY(cudaEventRecord(ev[0], stream));
+      GPRX_CUDA_TRY(fill_lower(kern, x.p, cap, n, A.p, ld, noise() + j, status.p, stream));
+      GPRX_CUDA_TRY(cudaEventRecord(ev[1], stream));
+      GPRX_CUDA_TRY(potrf_trtri_rec(A.p, ld, n, Xinv.p, ld, linv.p, scratch.p, ew, EMU_LEAF_N, EMU_MIN_N, status.p,
+                                    stream, &fctx));
+      GPRX_CUDA_TRY(cudaEventRecord(ev[2], stream));
+    } else {
+      if ((st = enqueue_factor(j)) != GPRX_OK) return st;
+    }
     GPRX_CUDA_TRY(logdet_diag(A.p, ld, n, false, res.p + 0, status.p, stream));
     if (grad) {
-      const bool emu = use_emu();
-      EmuWork ew;
-      if (emu) {
-        if ((st = ensure_emu()) != GPRX_OK) return st;
-        ew.sa = emu_sa.p; ew.sb = emu_sb.p; ew.ea = emu_ea.p; ew.eb = emu_eb.p; ew.ma = emu_ma.p; ew.mb = emu_mb.p;
-        ew.err = emu_err.p;
-        ew.S = 7;
-        GPRX_CUDA_TRY(cudaMemsetAsync(emu_err.p, 0, sizeof(int), stream));
-        GPRX_CUDA_TRY(trtri_blocked_emu(A.p, ld, n, linv.p, Xinv.p, ld, scratch.p, ew, EMU_MIN_N, status.p, stream));
-      } else {
+      if (!emu)  // the mixed factor produced X = L⁻¹ already
         GPRX_CUDA_TRY(trtri_blocked(A.p, ld, n, linv.p, Xinv.p, ld, scratch.p, status.p, stream));
-      }
       GPRX_CUDA_TRY(trmv_lower(Xinv.p, ld, n, y.p, z.p, status.p, stream));
       GPRX_CUDA_TRY(gemv_t(Xinv.p, ld, n, n, true, z.p, alpha.p, status.p, stream));
       GPRX_CUDA_TRY(dot_dev(y.p, alpha.p, n, res.p + 1, status.p, stream));

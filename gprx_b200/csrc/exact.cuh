@@ -64,6 +64,8 @@ struct ExactState {
   int num_params() const { return kern.n_params + 1; }
   // smallest n whose inverse uses the emulated products
   static constexpr int EMU_MIN_N = 1024;
+  // blocks the recursive mixed factor hands to the blocked DMMA factor
+  static constexpr int EMU_LEAF_N = 2048;
   bool use_emu() const { return opt.precision == GPRX_PRECISION_MIXED && n >= EMU_MIN_N; }
   gprx_status ensure_emu();
   void get_params(double* out) const;
