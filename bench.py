@@ -8,7 +8,13 @@ NLML + gradient evaluation at a hyperparameter vector perturbed by N(0, 0.1²)
 in log space (100 perturbations, cycled).  All data are synthetic, from the
 restated SeededRng; no dataset is read.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
+                    [--workload all|exact|batched] [--impl ours|reference]
+
+The default line's value is the mixed form (FP64 products emulated on the
+int8 tensor cores); the plain FP64 form is timed beside it ("fp64") with the
+largest error of the mixed results against it, and the batched-fits
+measurement (4096 ragged problems) rides in the same line ("batched").
 
 N > 1 runs N independent replicas (one exact problem does not shard; launched
 by torchrun, one rank per GPU); `value` is the aggregate evals/s over ranks,
@@ -300,7 +306,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: the mixed form is the headline value, the FP64 form is timed beside it")
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-evals", type=int, default=0,
@@ -321,7 +328,8 @@ def main():
               "noise_variance": NOISE, "perturbations": "100 θ + N(0, 0.1²) in log space, cycled",
               "l2": "inputs larger than L2 (two n×n FP64 buffers of %d MiB each)" % (n * n * 8 // 2 ** 20),
               "parallelism": "replicas" if args.gpus > 1 else "single"}
-    metric = "NLML+grad evals/s n=%d (%s)" % (n, "FP64" if args.precision == "fp64" else "mixed")
+    metric = "NLML+grad evals/s n=%d (%s)" % (n, {"both": "mixed; FP64 beside", "mixed": "mixed",
+                                                   "fp64": "FP64"}[args.precision])
 
     x, y, theta = synth(n, d)
     thetas = perturbations(theta)
@@ -367,98 +375,122 @@ def main():
         return
 
     spec = gx.ConstantKernel(CONST) * gx.RbfArdKernel(list(np.exp(theta[1:1 + d])))
-    prec = gx.Precision.Fp64 if args.precision == "fp64" else gx.Precision.Mixed
-    model = gx.Gpr(spec, gx.GaussianLikelihood(NOISE), precision=prec, device=local) \
-        .with_optimizer(gx.Fixed()).factor(x, n, d, y)
-    stream = torch.cuda.ExternalStream(model.stream_ptr(), device=dev)
-    if args.profile_evals > 0:
-        for i in range(args.profile_evals):
-            model.value_and_gradient(thetas[i % len(thetas)])
-        torch.cuda.synchronize()
-        return
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    # ---- device-resident timing (value) ----
-    for i in range(warm):
-        model.value_and_gradient(thetas[i % len(thetas)])
-    barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    l0 = L.lib().gprx_launch_count()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    stage = np.zeros(5)
-    for i in range(args.steps):
-        model.value_and_gradient(thetas[i % len(thetas)])
-        st = model.stage_times_ms()
-        stage += np.array([st["fill"], st["factor"], st["inverse"], st["gradient"], st["total"]])
-    e1.record(stream)
-    torch.cuda.synchronize()
-    launches = int(L.lib().gprx_launch_count() - l0)
-    ms = e0.elapsed_time(e1)
-    clk = clocks.stop()
-    barrier()
-    ms_max = ms
-    if dist is not None:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
-    value = args.steps * world / (ms_max * 1e-3)
-    stage /= args.steps
+        return float(t.item())
 
-    # ---- end to end through the public API with host buffers ----
-    xh = torch.from_numpy(x).pin_memory().numpy()
-    yh = torch.from_numpy(y).pin_memory().numpy()
-    p = theta.size
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for i in range(args.steps):
-        model.set_data(xh, yh)
-        model.value_and_gradient(thetas[i % len(thetas)])
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": args.steps * world / e2e_s, "unit": "evals/s",
-           "h2d_bytes_per_step": int((n * d + n + p) * 8), "d2h_bytes_per_step": int((1 + p) * 8)}
+    def measure(precision):
+        """Device-timed and end-to-end evaluations of one precision form."""
+        prec = gx.Precision.Fp64 if precision == "fp64" else gx.Precision.Mixed
+        model = gx.Gpr(spec, gx.GaussianLikelihood(NOISE), precision=prec, device=local) \
+            .with_optimizer(gx.Fixed()).factor(x, n, d, y)
+        stream = torch.cuda.ExternalStream(model.stream_ptr(), device=dev)
+        for i in range(warm):
+            model.value_and_gradient(thetas[i % len(thetas)])
+        barrier()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        l0 = L.lib().gprx_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        stage = np.zeros(5)
+        outs = []
+        for i in range(args.steps):
+            outs.append(model.value_and_gradient(thetas[i % len(thetas)]))
+            st = model.stage_times_ms()
+            stage += np.array([st["fill"], st["factor"], st["inverse"], st["gradient"], st["total"]])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = int(L.lib().gprx_launch_count() - l0)
+        clk = clocks.stop()
+        barrier()
+        ms_max = max_over_ranks(e0.elapsed_time(e1))
+        # end to end through the public API with host buffers
+        xh = torch.from_numpy(x).pin_memory().numpy()
+        yh = torch.from_numpy(y).pin_memory().numpy()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            model.set_data(xh, yh)
+            model.value_and_gradient(thetas[i % len(thetas)])
+        torch.cuda.synchronize()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        del model
+        torch.cuda.empty_cache()
+        return {"value": args.steps * world / (ms_max * 1e-3), "ms_per_step": ms_max / args.steps,
+                "stage": stage / args.steps, "launches": launches, "clocks": clk, "outs": outs,
+                "e2e": {"value": args.steps * world / e2e_s, "unit": "evals/s",
+                        "h2d_bytes_per_step": int((n * d + n + theta.size) * 8),
+                        "d2h_bytes_per_step": int((1 + theta.size) * 8)}}
 
-    # ---- roofline: the DMMA-driven stages (factor + inverse), n³ flops ----
+    if args.profile_evals > 0:
+        prec = gx.Precision.Fp64 if args.precision == "fp64" else gx.Precision.Mixed
+        model = gx.Gpr(spec, gx.GaussianLikelihood(NOISE), precision=prec, device=local) \
+            .with_optimizer(gx.Fixed()).factor(x, n, d, y)
+        for i in range(args.profile_evals):
+            model.value_and_gradient(thetas[i % len(thetas)])
+        torch.cuda.synchronize()
+        return
+
+    forms = ["fp64"] if args.precision == "fp64" else ["mixed"] if args.precision == "mixed" else ["fp64", "mixed"]
+    res = {f: measure(f) for f in forms}
+    head = res["mixed"] if "mixed" in res else res["fp64"]
+    stage = head["stage"]
     peaks = measured_peaks()
     fp64_peak = fp64_peak_tflops(torch, dev) if rank == 0 else None
     dmma_ms = stage[1] + stage[2]
     achieved = (n ** 3) / (dmma_ms * 1e-3) / 1e12
     traffic = load_traffic()
+    mixed = "mixed" in res
     roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak if fp64_peak else None,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)",
-                "kernel": "dgemm_kernel (DMMA m16n8k4 f64) inside potrf/trtri/lauum",
-                "work": "n^3 flops per evaluation (potrf n^3/3 + trtri n^3/3 + lauum n^3/3)",
+                "kernel": ("emu_gemm_kernel<7> (int8 tcgen05, FP64-emulated) + dgemm_kernel (DMMA f64)" if mixed
+                           else "dgemm_kernel (DMMA m16n8k4 f64) inside potrf/trtri/lauum"),
+                "work": "n^3 FP64(-equivalent) flops per evaluation (potrf n^3/3 + trtri n^3/3 + lauum n^3/3)",
                 "traffic": traffic.get("bytes_per_eval") if traffic else None,
                 "stage_ms": {"fill": stage[0], "factor": stage[1], "inverse": stage[2], "gradient": stage[3],
                              "total": stage[4]}}
-
-    line = {"metric": metric, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
-            "warmup": warm, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config, "e2e": e2e,
-            "gpu_launches": launches, "roofline": roofline, "clocks": clk,
-            "bf16_peak_reference": peaks.get("bf16_tflops")}
+    if mixed:
+        config["precision"] = ("mixed: factor and inverse by recursive halving, coupling products and K^-1 = X^T X "
+                               "as FP64 products emulated on int8 tensor cores (7 slices); FP64 fill, 2048-row "
+                               "leaves, log-det and gradient")
+    line = {"metric": metric, "value": head["value"], "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": warm, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if not mixed else "f64 (int8-emulated products)",
+            "data": "synthetic", "config": config, "e2e": head["e2e"], "gpu_launches": head["launches"],
+            "roofline": roofline, "clocks": head["clocks"], "bf16_peak_reference": peaks.get("bf16_tflops")}
+    if mixed and "fp64" in res:
+        f, m = res["fp64"], res["mixed"]
+        nl_err = max(abs(a[0] - b[0]) / max(abs(b[0]), 1.0) for a, b in zip(m["outs"], f["outs"]))
+        g_err = max(float(np.max(np.abs(a[1] - b[1]) / np.maximum(np.abs(b[1]), 1.0)))
+                    for a, b in zip(m["outs"], f["outs"]))
+        line["fp64"] = {"value": f["value"], "unit": "evals/s", "ms_per_step": f["ms_per_step"], "e2e": f["e2e"],
+                        "stage_ms": {"fill": f["stage"][0], "factor": f["stage"][1], "inverse": f["stage"][2],
+                                     "gradient": f["stage"][3], "total": f["stage"][4]},
+                        "roofline_frac": (n ** 3) / ((f["stage"][1] + f["stage"][2]) * 1e-3) / 1e12 / fp64_peak
+                        if fp64_peak else None}
+        line["mixed_vs_fp64"] = m["value"] / f["value"]
+        line["mixed_error_vs_fp64"] = {"nlml_rel_max": nl_err, "grad_rel_max": g_err,
+                                       "measure": "max over the timed evaluations of |a − e| / max(|e|, 1)"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, cores, sample = cpu_reference(n, d, x, y, thetas, steps=1, warmup=0, budget_s=30.0)
         line["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": cores, "kind": "port", "sample": sample}
     if args.workload == "all" and world == 1:
-        del model
         torch.cuda.empty_cache()
         line["batched"] = batched_measure(torch, dev, args.batch_problems, fp64_peak=fp64_peak)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    model = None
     if dist is not None:
         dist.destroy_process_group()
 
