@@ -300,6 +300,101 @@ def batched_measure(torch, dev, count=BATCH_P, single_sample=32, cpu_sample=48, 
     }
 
 
+# ---------------------------------------------------------------------------
+# serving: Poisson stream of fit / predict / online requests
+# ---------------------------------------------------------------------------
+SERVE_D = 4
+
+
+def serving_synth(torch, dev, count=12, seed=4):
+    """Datasets for the fit requests: n log-uniform in [64, 4096], x ~ N(0, I₄),
+    y a draw from the GP prior (RbfArd, ℓ = 1) plus N(0, 0.05²)."""
+    import gprx_b200 as gx
+
+    rng = gx.SeededRng(seed)
+    out = []
+    for _ in range(count):
+        n = int(math.exp(math.log(64) + rng.unit(1)[0] * (math.log(4096) - math.log(64))))
+        x = rng.normal(n * SERVE_D)
+        xt = torch.from_numpy(x.reshape(SERVE_D, n).T.copy()).to(dev)
+        k = torch.exp(-0.5 * torch.cdist(xt, xt).pow(2)) + 0.05 ** 2 * torch.eye(n, dtype=torch.float64, device=dev)
+        y = (torch.linalg.cholesky(k) @ torch.from_numpy(rng.normal(n)).to(dev)).cpu().numpy()
+        out.append((n, x, y))
+    return out
+
+
+def serving_measure(torch, dev, rate, duration, precision, datasets, seed=5, workers=8):
+    """Requests arrive as a Poisson process of `rate` per second for
+    `duration` seconds: 20% fits (a new model on one of the datasets), 60%
+    predictions (1..10⁴ points, log-uniform) against a model, 20% online
+    steps (add or remove 1..16 points).  Latency = submission to completion."""
+    import concurrent.futures as cf
+
+    import gprx_b200 as gx
+
+    rs = np.random.RandomState(seed)
+    prec = gx.Precision.Fp64 if precision == "fp64" else gx.Precision.Mixed
+    srv = gx.Server(device=dev.index or 0, workers=workers)
+    kern = gx.RbfArdKernel([1.0] * SERVE_D)
+    lik = gx.GaussianLikelihood(0.05 ** 2)
+    models = []  # (model id, n, removable original ids)
+    for n, x, y in datasets[:3]:  # a few resident models before the stream starts
+        mid = srv.submit_fit(kern, lik, x, n, SERVE_D, y, precision=prec)
+        srv.wait(mid)
+        models.append([mid, n, list(range(n))])
+    pool = cf.ThreadPoolExecutor(max_workers=64)
+    futs = []
+    kinds = []
+    t0 = time.perf_counter()
+    t = 0.0
+    while True:
+        t += rs.exponential(1.0 / rate)
+        if t > duration:
+            break
+        now = time.perf_counter() - t0
+        if t > now:
+            time.sleep(t - now)
+        u = rs.rand()
+        if u < 0.2:
+            n, x, y = datasets[rs.randint(len(datasets))]
+            rid = srv.submit_fit(kern, lik, x, n, SERVE_D, y, precision=prec)
+            models.append([rid, n, list(range(n))])
+            kinds.append("fit")
+        elif u < 0.8:
+            m = models[rs.randint(len(models))]
+            q = int(math.exp(rs.uniform(0.0, math.log(1e4))))
+            rid, _, _ = srv.submit_predict(m[0], rs.standard_normal(q * SERVE_D), q)
+            kinds.append("predict")
+        else:
+            m = models[rs.randint(len(models))]
+            k = int(rs.randint(1, 17))
+            if rs.rand() < 0.5 or len(m[2]) <= k + 8:
+                rid, _ = srv.submit_add(m[0], rs.standard_normal(k * SERVE_D), rs.standard_normal(k), k)
+            else:
+                take = [m[2].pop(rs.randint(len(m[2]))) for _ in range(k)]
+                rid = srv.submit_remove(m[0], take)
+            kinds.append("online")
+        futs.append(pool.submit(srv.wait, rid))
+    res = [f.result() for f in futs]
+    wall = time.perf_counter() - t0
+    pool.shutdown()
+    stats = srv.stats()
+    srv.close()
+    lat = np.array([r[1]["latency_ms"] for r in res])
+    ok = np.array([r[0] == 0 for r in res])
+    per = {}
+    for kind in ("fit", "predict", "online"):
+        sel = np.array([k == kind for k in kinds]) & ok
+        if sel.any():
+            per[kind] = {"count": int(sel.sum()), "p50_ms": float(np.percentile(lat[sel], 50)),
+                         "p99_ms": float(np.percentile(lat[sel], 99))}
+    return {"arrival_rate_per_s": rate, "duration_s": duration, "precision": precision,
+            "requests": len(res), "completed_ok": int(ok.sum()), "requests_per_s": float(ok.sum() / wall),
+            "p50_ms": float(np.percentile(lat[ok], 50)) if ok.any() else None,
+            "p99_ms": float(np.percentile(lat[ok], 99)) if ok.any() else None,
+            "per_kind": per, "merged_predict_launches": stats["merged_launches"], "workers": workers}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -312,9 +407,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-evals", type=int, default=0,
                     help="only factor once and run this many evaluations (for an ncu launch list), no JSON line")
-    ap.add_argument("--workload", default="all", choices=["all", "exact", "batched"],
+    ap.add_argument("--workload", default="all", choices=["all", "exact", "batched", "serving"],
                     help="all: the exact line with the batched measurement as its 'batched' key")
     ap.add_argument("--batch-problems", type=int, default=BATCH_P)
+    ap.add_argument("--serve-rates", default="2,4,8", help="arrival rates (requests/s) of the serving sweep")
+    ap.add_argument("--serve-seconds", type=float, default=15.0)
     args = ap.parse_args()
     n, d = args.n, D
     warm = max(3, args.warmup)
@@ -358,6 +455,23 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+
+    if args.workload == "serving":
+        datasets = serving_synth(torch, dev)
+        sweep = []
+        for prec in ("fp64", "mixed"):
+            for rate in [float(r) for r in args.serve_rates.split(",")]:
+                sweep.append(serving_measure(torch, dev, rate, args.serve_seconds, prec, datasets))
+        head = max((r for r in sweep if r["precision"] == "mixed"), key=lambda r: r["requests_per_s"])
+        out = {"metric": "serving p99 latency (ms) at the highest sustained rate", "value": head["p99_ms"],
+               "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": len(sweep), "warmup": 3,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": "serving_exact_rbfard_d4_poisson", "mix": "20% fit, 60% predict, 20% online",
+                          "fit_n": "log-uniform [64, 4096]", "predict_q": "log-uniform [1, 1e4]",
+                          "online_points": "1..16"},
+               "sweep": sweep}
+        print(json.dumps(out), flush=True)
+        return
 
     if args.workload == "batched":
         if args.profile_evals > 0:
@@ -489,6 +603,8 @@ def main():
     if args.workload == "all" and world == 1:
         torch.cuda.empty_cache()
         line["batched"] = batched_measure(torch, dev, args.batch_problems, fp64_peak=fp64_peak)
+        datasets = serving_synth(torch, dev)
+        line["serving"] = [serving_measure(torch, dev, 4.0, 12.0, prec, datasets) for prec in ("fp64", "mixed")]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

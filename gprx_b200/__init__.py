@@ -41,6 +41,7 @@ from .api import (  # noqa: F401
     RbfArdKernel,
     RbfKernel,
     SeededRng,
+    Server,
     Sgpr,
     ShapeMismatch,
     VarianceKind,

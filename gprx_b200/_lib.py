@@ -69,6 +69,20 @@ class ErrorInfo(C.Structure):
                 ("cuda_error", C.c_int32), ("iterations", C.c_uint64), ("message", C.c_char * 256)]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("device", C.c_int32), ("workers", C.c_int32), ("hbm_budget_bytes", C.c_uint64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("model", C.c_uint64), ("kind", C.c_int32), ("submit_ns", C.c_int64),
+                ("start_ns", C.c_int64), ("end_ns", C.c_int64), ("merged", C.c_int32), ("message", C.c_char * 256)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("merged_launches", C.c_uint64), ("used_bytes", C.c_uint64),
+                ("resident_models", C.c_uint64)]
+
+
 class Rng(C.Structure):
     _fields_ = [("s", C.c_uint64 * 4)]
 
@@ -131,6 +145,16 @@ _SIGS = {
     "gprx_batch_fit": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.POINTER(LbfgsOptions), D, C.POINTER(FitReport),
                                    I32]),
     "gprx_batch_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "gprx_server_options_default": (None, [C.POINTER(ServerOptions)]),
+    "gprx_server_create": (C.c_int32, [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    "gprx_server_destroy": (C.c_int32, [C.c_void_p]),
+    "gprx_server_fit": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_uint64, D, C.POINTER(KernelNode), C.c_int32, D,
+                                    C.c_int32, C.POINTER(Options), C.POINTER(LbfgsOptions), C.c_int32, U64]),
+    "gprx_server_predict": (C.c_int32, [C.c_void_p, C.c_uint64, D, C.c_uint64, C.c_uint64, C.c_int32, D, D, U64]),
+    "gprx_server_add": (C.c_int32, [C.c_void_p, C.c_uint64, D, D, C.c_uint64, C.c_uint64, U64, U64]),
+    "gprx_server_remove": (C.c_int32, [C.c_void_p, C.c_uint64, U64, C.c_uint64, U64]),
+    "gprx_server_wait": (C.c_int32, [C.c_void_p, C.c_uint64, C.POINTER(RequestInfo)]),
+    "gprx_server_stats": (C.c_int32, [C.c_void_p, C.POINTER(ServerStats)]),
     "gprx_probe_dgemm": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),
     "gprx_probe_potrf": (C.c_int32, [C.c_int32, C.c_int32, D]),
     "gprx_probe_emu_gemm": (C.c_int32, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, D]),

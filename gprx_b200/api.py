@@ -797,6 +797,99 @@ class GprBatch:
 
 
 # ---------------------------------------------------------------------------
+# serving: a request loop over resident exact models
+# ---------------------------------------------------------------------------
+class Server:
+    """Continuous request loop on one GPU (gprx_server_*): fit, predict and
+    online add/remove requests against resident models, admitted by free
+    workers and the HBM budget, overlapping on the device; consecutive
+    predicts of one model share a launch.  submit_* return a request id;
+    wait(id) blocks until it completes and returns its info (the outputs of
+    a predict / add are in the arrays submit_* returned)."""
+
+    def __init__(self, device=0, workers=8, hbm_budget_bytes=150 << 30):
+        o = L.ServerOptions()
+        L.lib().gprx_server_options_default(C.byref(o))
+        o.device, o.workers, o.hbm_budget_bytes = int(device), int(workers), int(hbm_budget_bytes)
+        h = C.c_void_p()
+        check(L.lib().gprx_server_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self._keep = {}  # request id → buffers the library writes on completion
+        self.d = {}      # model id → d
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            L.lib().gprx_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit_fit(self, kernel, likelihood, x, n, d, y, optimizer=None, precision=Precision.Fp64):
+        x = _check_points(x, n, d)
+        y = L.f64(y)
+        nodes, nn = kernel.node_array()
+        theta = L.f64(kernel.get_params() + [likelihood.log_noise_variance])
+        o = L.Options()
+        L.lib().gprx_options_default(C.byref(o))
+        o.precision = int(precision)
+        opt = optimizer if optimizer is not None else Lbfgs()
+        lo = opt._c() if not isinstance(opt, Fixed) else Lbfgs()._c()
+        rid = C.c_uint64()
+        check(L.lib().gprx_server_fit(self._h, L.ptr(x), n, d, L.ptr(y), nodes, nn, L.ptr(theta), theta.size,
+                                      C.byref(o), C.byref(lo), 0 if isinstance(opt, Fixed) else 1, C.byref(rid)))
+        self.d[rid.value] = d
+        return rid.value
+
+    def submit_predict(self, model, xs, q, kind=VarianceKind.Observation):
+        d = self.d[model]
+        xs = _check_points(xs, q, d)
+        mean = np.zeros(q)
+        var = np.zeros(q)
+        rid = C.c_uint64()
+        check(L.lib().gprx_server_predict(self._h, model, L.ptr(xs), q, d, int(kind), L.ptr(mean), L.ptr(var),
+                                          C.byref(rid)))
+        self._keep[rid.value] = (mean, var)
+        return rid.value, mean, var
+
+    def submit_add(self, model, x, y, k):
+        d = self.d[model]
+        x = _check_points(x, k, d)
+        y = L.f64(y)
+        ids = np.zeros(k, dtype=np.uint64)
+        rid = C.c_uint64()
+        check(L.lib().gprx_server_add(self._h, model, L.ptr(x), L.ptr(y), k, d, ids.ctypes.data_as(L.U64),
+                                      C.byref(rid)))
+        self._keep[rid.value] = (ids,)
+        return rid.value, ids
+
+    def submit_remove(self, model, ids):
+        ids = np.ascontiguousarray(np.asarray(ids, dtype=np.uint64))
+        rid = C.c_uint64()
+        check(L.lib().gprx_server_remove(self._h, model, ids.ctypes.data_as(L.U64), ids.size, C.byref(rid)))
+        return rid.value
+
+    def wait(self, rid):
+        """Blocks until request rid completes; returns (status, info dict)."""
+        info = L.RequestInfo()
+        st = L.lib().gprx_server_wait(self._h, rid, C.byref(info))
+        self._keep.pop(rid, None)
+        return st, {"status": info.status, "model": info.model, "kind": info.kind,
+                    "latency_ms": (info.end_ns - info.submit_ns) * 1e-6,
+                    "queue_ms": (info.start_ns - info.submit_ns) * 1e-6, "merged": info.merged,
+                    "message": info.message.decode(errors="replace")}
+
+    def stats(self):
+        s = L.ServerStats()
+        check(L.lib().gprx_server_stats(self._h, C.byref(s)))
+        return {"completed": s.completed, "merged_launches": s.merged_launches, "used_bytes": s.used_bytes,
+                "resident_models": s.resident_models}
+
+
+# ---------------------------------------------------------------------------
 # seeded RNG (src/rng.rs)
 # ---------------------------------------------------------------------------
 class SeededRng:

@@ -294,6 +294,63 @@ gprx_status gprx_batch_fit(gprx_batch* h, const double* params0, uint64_t p, con
 /* The CUDA stream (a cudaStream_t) of the handle, for event timing. */
 gprx_status gprx_batch_stream(gprx_batch* h, void** stream);
 
+/* ------------------------------------------------------------------ */
+/* serving: a request loop over resident exact models on one GPU (no    */
+/* counterpart in the reference; each request is the work of Gpr::fit, */
+/* FittedGpr::predict_with, OnlineGpr::insert / delete)                 */
+/* ------------------------------------------------------------------ */
+typedef struct gprx_server gprx_server;
+
+typedef struct {
+  int32_t device;
+  int32_t workers;            /* host worker threads = requests in flight */
+  uint64_t hbm_budget_bytes;  /* device memory the resident models may take */
+} gprx_server_options;
+
+typedef struct {
+  gprx_status status;
+  uint64_t model;
+  int32_t kind;               /* 0 fit, 1 predict, 2 add, 3 remove */
+  int64_t submit_ns, start_ns, end_ns;  /* steady-clock times */
+  int32_t merged;             /* requests that shared this request's launch */
+  char message[256];
+} gprx_request_info;
+
+typedef struct {
+  uint64_t completed;
+  uint64_t merged_launches;
+  uint64_t used_bytes;
+  uint64_t resident_models;
+} gprx_server_stats_t;
+
+void gprx_server_options_default(gprx_server_options* opt);
+/* Starts the worker threads. */
+gprx_status gprx_server_create(const gprx_server_options* opt, gprx_server** out);
+/* Stops the workers (requests still queued are dropped) and frees every model. */
+gprx_status gprx_server_destroy(gprx_server* s);
+/* Queues a fit (optimize = 1: L-BFGS; 0: factor at θ) of a new model; the
+ * request id is also the model id.  Inputs are copied at submission. */
+gprx_status gprx_server_fit(gprx_server* s, const double* x, uint64_t n, uint64_t d, const double* y,
+                            const gprx_kernel_node* nodes, int32_t n_nodes, const double* theta, int32_t n_theta,
+                            const gprx_options* options, const gprx_lbfgs_options* lbfgs, int32_t optimize,
+                            uint64_t* request_id);
+/* Queues a prediction at q points (column-major q×d, copied); mean and var
+ * (q values each) are written when the request completes and must stay
+ * valid until gprx_server_wait returns for it. */
+gprx_status gprx_server_predict(gprx_server* s, uint64_t model, const double* xs, uint64_t q, uint64_t d,
+                                int32_t variance_kind, double* mean, double* var, uint64_t* request_id);
+/* Queues an online insert of k points (x column-major k×d, copied); ids_out
+ * (k values, may be NULL) receives their PointIds on completion. */
+gprx_status gprx_server_add(gprx_server* s, uint64_t model, const double* x, const double* y, uint64_t k, uint64_t d,
+                            uint64_t* ids_out, uint64_t* request_id);
+/* Queues an online delete of k PointIds (copied). */
+gprx_status gprx_server_remove(gprx_server* s, uint64_t model, const uint64_t* ids, uint64_t k,
+                               uint64_t* request_id);
+/* Blocks until the request completes; returns its status.  A completed
+ * predict / add / remove request is forgotten after this call. */
+gprx_status gprx_server_wait(gprx_server* s, uint64_t request_id, gprx_request_info* info);
+gprx_status gprx_server_stats(gprx_server* s, gprx_server_stats_t* out);
+
 /* Allocation-free NLML + gradient of ONE exact problem (no counterpart in the
  * reference).  For callers that cannot allocate device memory when they need
  * an evaluation: work issued while a CUDA graph is being captured, code inside
