@@ -13,8 +13,10 @@ restated SeededRng; no dataset is read.
 
 The default line's value is the mixed form (FP64 products emulated on the
 int8 tensor cores); the plain FP64 form is timed beside it ("fp64") with the
-largest error of the mixed results against it, and the batched-fits
-measurement (4096 ragged problems) rides in the same line ("batched").
+largest error of the mixed results against it.  The other workloads ride in
+the same line: "batched" (4096 ragged exact fits), "serving" (a Poisson
+request stream, p50/p99) and "sgpr" (VFE at n = 10⁶, m = 1024); each is also
+available alone through --workload.
 
 N > 1 runs N independent replicas (one exact problem does not shard; launched
 by torchrun, one rank per GPU); `value` is the aggregate evals/s over ranks,
@@ -301,6 +303,71 @@ def batched_measure(torch, dev, count=BATCH_P, single_sample=32, cpu_sample=48, 
 
 
 # ---------------------------------------------------------------------------
+# sparse VFE at n = 10⁶, m = 1024 (Sgpr, RbfArd d = 4)
+# ---------------------------------------------------------------------------
+def sgpr_synth(n=1_000_000, m=1024, d=4, seed=2):
+    """x ~ U[0,1]⁴, y = Σ_k sin(2π f_k x_k) + N(0, 0.1²) with f_k ~ U[0.5, 2];
+    lengthscales log-uniform in [0.5, 2]; Z a seeded subset of m rows of x
+    (up_to without replacement)."""
+    import gprx_b200 as gx
+
+    rng = gx.SeededRng(seed)
+    x = rng.unit(n * d)
+    f = 0.5 + 1.5 * rng.unit(d)
+    ls = np.exp(math.log(0.5) + rng.unit(d) * (math.log(2.0) - math.log(0.5)))
+    xm = x.reshape(d, n)
+    y = np.sin(2 * math.pi * f[:, None] * xm).sum(0) + 0.1 * rng.normal(n)
+    idx = rng.subset(n, m)
+    z = xm[:, idx].reshape(-1).copy()
+    return x, y, z, ls
+
+
+def sgpr_measure(torch, dev, steps, warm, n=1_000_000, m=1024, d=4, cpu_n=5_000):
+    import gprx_b200 as gx
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    x, y, z, ls = sgpr_synth(n, m, d)
+    spec = gx.RbfArdKernel(list(ls))
+    theta = np.array(list(np.log(ls)) + [math.log(0.1)])
+    rng = gx.SeededRng(6)
+    thetas = [theta + 0.1 * rng.normal(theta.size) for _ in range(16)]
+    mdl = gx.Sgpr(spec, gx.GaussianLikelihood(0.1)).with_optimizer(gx.Fixed()).factor(x, n, d, y, z, m)
+    stream = torch.cuda.ExternalStream(mdl.stream_ptr(), device=dev)
+    for i in range(warm):
+        mdl.value_and_gradient(thetas[i % len(thetas)])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        mdl.value_and_gradient(thetas[i % len(thetas)])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    st = mdl.stage_times_ms()
+    del mdl
+    torch.cuda.empty_cache()
+    # CPU oracle on the first cpu_n points (the evaluation is O(n m²)), scaled by n / cpu_n
+    xs = x.reshape(d, n)[:, :cpu_n].reshape(-1).copy()
+    t0 = time.perf_counter()
+    orc = O.Sgpr([[11, d]], thetas[0], xs, cpu_n, d, y[:cpu_n].copy(), z, m)
+    orc.nlml()
+    orc.grad()
+    cpu_s = (time.perf_counter() - t0) * n / cpu_n
+    flops = 7.0 * m * m * n + 2.0 * m ** 3 / 3.0
+    return {"metric": "Sgpr VFE NLML+grad evals/s (n=1e6, m=1024, FP64)", "value": 1000.0 / ms, "unit": "evals/s",
+            "ms_per_step": ms, "steps": steps, "stage_ms": st,
+            "config": {"workload": "sgpr_vfe_n1e6_m1024_rbfard_d4", "n": n, "m": m, "d": d,
+                       "inducing": "seeded subset of x (up_to without replacement)", "noise_variance": 0.1},
+            "roofline": {"bound": "tensor", "work": "7 m^2 n + 2 m^3 / 3 flop per evaluation",
+                         "achieved": flops / (ms * 1e-3) / 1e12, "unit": "TFLOP/s"},
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "evals/s", "cores": int(O.lib().orc_num_threads()),
+                             "kind": "port", "sample": "oracle assembly + NLML + gradient on the first %d points, "
+                                                       "time scaled by n / %d (O(n m²))" % (cpu_n, cpu_n)}}
+
+
+# ---------------------------------------------------------------------------
 # serving: Poisson stream of fit / predict / online requests
 # ---------------------------------------------------------------------------
 SERVE_D = 4
@@ -407,7 +474,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-evals", type=int, default=0,
                     help="only factor once and run this many evaluations (for an ncu launch list), no JSON line")
-    ap.add_argument("--workload", default="all", choices=["all", "exact", "batched", "serving"],
+    ap.add_argument("--workload", default="all", choices=["all", "exact", "batched", "serving", "sgpr"],
                     help="all: the exact line with the batched measurement as its 'batched' key")
     ap.add_argument("--batch-problems", type=int, default=BATCH_P)
     ap.add_argument("--serve-rates", default="2,4,8", help="arrival rates (requests/s) of the serving sweep")
@@ -455,6 +522,13 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+
+    if args.workload == "sgpr":
+        out = sgpr_measure(torch, dev, args.steps, warm)
+        out.update({"n_gpus": 1, "warmup": warm, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "f64", "data": "synthetic"})
+        print(json.dumps(out), flush=True)
+        return
 
     if args.workload == "serving":
         datasets = serving_synth(torch, dev)
@@ -605,6 +679,8 @@ def main():
         line["batched"] = batched_measure(torch, dev, args.batch_problems, fp64_peak=fp64_peak)
         datasets = serving_synth(torch, dev)
         line["serving"] = [serving_measure(torch, dev, 4.0, 12.0, prec, datasets) for prec in ("fp64", "mixed")]
+        torch.cuda.empty_cache()
+        line["sgpr"] = sgpr_measure(torch, dev, 3, 2)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
