@@ -494,6 +494,34 @@ cudaError_t trsm_lower_t(const double* L, long long ld, int n, const double* lin
   return cudaGetLastError();
 }
 
+// split point of a recursive solve: half of n rounded up to whole NB blocks
+// (the diagonal-block inverses are indexed by row / NB)
+static int rec_split(int n) { return ceil_div(ceil_div(n, 2), NB) * NB; }
+
+cudaError_t trsm_lower_rec(const double* L, long long ld, int n, const double* linv, double* B, long long ldb, int q,
+                           int leaf, DevStatus* st, cudaStream_t s) {
+  const int n1 = rec_split(n);
+  if (n <= leaf || n1 >= n) return trsm_lower(L, ld, n, linv, B, ldb, q, st, s);
+  const int n2 = n - n1;
+  CK(trsm_lower_rec(L, ld, n1, linv, B, ldb, q, leaf, st, s));
+  GemmParams p = gemm_params(n2, q, n1, L + n1, ld, B, ldb, B + n1, ldb, -1.0, 1.0, st);
+  CK(dgemm(false, false, p, s));
+  return trsm_lower_rec(L + n1 + (long long)n1 * ld, ld, n2, linv + (long long)(n1 / NB) * NB * NB, B + n1, ldb, q,
+                        leaf, st, s);
+}
+
+cudaError_t trsm_lower_t_rec(const double* L, long long ld, int n, const double* linv, double* B, long long ldb,
+                             int q, int leaf, DevStatus* st, cudaStream_t s) {
+  const int n1 = rec_split(n);
+  if (n <= leaf || n1 >= n) return trsm_lower_t(L, ld, n, linv, B, ldb, q, st, s);
+  const int n2 = n - n1;
+  CK(trsm_lower_t_rec(L + n1 + (long long)n1 * ld, ld, n2, linv + (long long)(n1 / NB) * NB * NB, B + n1, ldb, q,
+                      leaf, st, s));
+  GemmParams p = gemm_params(n1, q, n2, L + n1, ld, B + n1, ldb, B, ldb, -1.0, 1.0, st);
+  CK(dgemm(true, false, p, s));
+  return trsm_lower_t_rec(L, ld, n1, linv, B, ldb, q, leaf, st, s);
+}
+
 // ---------------------------------------------------------------------------
 // reductions and matrix-vector products (HBM-bound)
 // ---------------------------------------------------------------------------

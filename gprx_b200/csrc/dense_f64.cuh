@@ -52,11 +52,23 @@ cudaError_t trtri_blocked(const double* L, long long ld, int n, const double* li
 cudaError_t lauum_lower(const double* X, long long ldx, int n, double* C, long long ldc, DevStatus* st,
                         cudaStream_t s);
 
+struct EmuWork;
+
 // B (n×q, ldb) := L⁻¹ B   /   := L⁻ᵀ B, with L's diagonal block inverses.
 cudaError_t trsm_lower(const double* L, long long ld, int n, const double* linv, double* B, long long ldb, int q,
                        DevStatus* st, cudaStream_t s);
 cudaError_t trsm_lower_t(const double* L, long long ld, int n, const double* linv, double* B, long long ldb, int q,
                          DevStatus* st, cudaStream_t s);
+
+// The same two solves for wide B (q ≫ n) by recursive halving: X1 from the
+// top half, one rank-n1 update B2 −= L21 X1 (L21ᵀ X2 for the transpose), then
+// the bottom half; blocks of at most `leaf` rows use trsm_lower /
+// trsm_lower_t.  The updates have K = n/2, n/4, … instead of NB, so the
+// DGEMMs run near their large-K rate.
+cudaError_t trsm_lower_rec(const double* L, long long ld, int n, const double* linv, double* B, long long ldb, int q,
+                           int leaf, DevStatus* st, cudaStream_t s);
+cudaError_t trsm_lower_t_rec(const double* L, long long ld, int n, const double* linv, double* B, long long ldb,
+                             int q, int leaf, DevStatus* st, cudaStream_t s);
 
 // out = log|det L|² contribution: 2 Σ ln L_ii (lower LLT) or Σ ln D_i (ldlt=true).
 cudaError_t logdet_diag(const double* L, long long ld, int n, bool ldlt, double* out, DevStatus* st,
@@ -78,7 +90,6 @@ cudaError_t dot_dev(const double* a, const double* b, int n, double* out, DevSta
 // The same two products with the FP64 GEMMs emulated on the int8 tensor
 // cores (emu_gemm.cuh) wherever the blocks are at least emu_min wide; the
 // narrower levels stay on DMMA.  X's strict upper triangle must be zero.
-struct EmuWork;
 cudaError_t trtri_blocked_emu(const double* L, long long ld, int n, const double* linv, double* X, long long ldx,
                               double* scratch, const EmuWork& w, int emu_min, DevStatus* st, cudaStream_t s);
 cudaError_t lauum_lower_emu(const double* X, long long ldx, int n, double* C, long long ldc, const EmuWork& w,

@@ -215,11 +215,11 @@ static __device__ int diag_block_factor_inv(double* A, long long lda, long long 
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  for (int e = tid; e < npad * npad; e += nt) {
-    int i = e % npad, j = e / npad;
-    if (i < j) s[i + j * FLS] = 0.0;
-    else if (i >= nb || j >= nb) s[i + j * FLS] = (i == j) ? 1.0 : 0.0;
-  }
+  for (int j = warp; j < npad; j += nw)
+    for (int i = lane; i < npad; i += 32) {
+      if (i < j) s[i + j * FLS] = 0.0;
+      else if (i >= nb || j >= nb) s[i + j * FLS] = (i == j) ? 1.0 : 0.0;
+    }
   __syncthreads();
   const int np = npad / SB;
   // one call site of the warp factor (a second inlined copy ran several times
@@ -307,7 +307,11 @@ static __device__ int diag_block_factor_inv(double* A, long long lda, long long 
     __syncthreads();
   }
   for (int j = warp; j < NB_DIAG; j += nw)
-    for (int i = lane; i < NB_DIAG; i += 32) linv[i + j * NB_DIAG] = (i < nb && j < nb && i >= j) ? s[i + j * FLS] : 0.0;
+    for (int i = 2 * lane; i < NB_DIAG; i += 64) {
+      const double a = (i < nb && j < nb && i >= j) ? s[i + j * FLS] : 0.0;
+      const double b = (i + 1 < nb && j < nb && i + 1 >= j) ? s[i + 1 + j * FLS] : 0.0;
+      *reinterpret_cast<double2*>(linv + i + j * NB_DIAG) = make_double2(a, b);
+    }
   __syncthreads();
   return -1;
 }

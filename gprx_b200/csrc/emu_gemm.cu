@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) emu_slice_kernel(const double* M, long lo
 }
 
 cudaError_t emu_slice(const double* M, long long ld, bool trans, const EmuOperand& op, cudaStream_t s) {
-  if (op.S < 4 || op.S > 7 || op.Rpad % EMU_M || op.Kpad % EMU_KC || !op.rmax) return cudaErrorInvalidValue;
+  if (op.S < 4 || op.S > EMU_MAX_S || op.Rpad % EMU_M || op.Kpad % EMU_KC || !op.rmax) return cudaErrorInvalidValue;
   cudaError_t e = cudaMemsetAsync(op.rmax, 0, sizeof(unsigned long long) * op.Rpad, s);
   if (e != cudaSuccess) return e;
   const dim3 grid(op.Rpad / 32, op.Kpad / 64);
@@ -123,7 +123,8 @@ cudaError_t emu_slice(const double* M, long long ld, bool trans, const EmuOperan
     case 4: GPRX_LAUNCH(emu_slice_kernel<4>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
     case 5: GPRX_LAUNCH(emu_slice_kernel<5>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
     case 6: GPRX_LAUNCH(emu_slice_kernel<6>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
-    default: GPRX_LAUNCH(emu_slice_kernel<7>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
+    case 7: GPRX_LAUNCH(emu_slice_kernel<7>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
+    default: GPRX_LAUNCH(emu_slice_kernel<8>, grid, 256, 0, s, M, ld, trans, op.R, op.K, op.Rpad, op.Kpad, op.rmax, op.exps, op.slices); break;
   }
   return cudaGetLastError();
 }
@@ -210,6 +211,8 @@ struct EmuGemmArgs {
   long long row0, col0;
   int kmode;
   int* err;
+  int kz;              // > 0: blockIdx.z takes K chunks [z·kz, (z+1)·kz) into C + z·zstride
+  long long zstride;
 };
 
 template <int S>
@@ -239,7 +242,12 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
   else if (g.kmode == 2) kc0 = (int)(j0 / EMU_KC);
   else if (g.kmode == 3) kc1 = (int)min((long long)nkc, (i0 + EMU_M + EMU_KC - 1) / EMU_KC);
   else if (g.kmode == 4) kc1 = (int)min((long long)nkc, (j0 + EMU_N + EMU_KC - 1) / EMU_KC);
+  if (g.kz > 0) {
+    kc0 = (int)blockIdx.z * g.kz;
+    kc1 = min(nkc, kc0 + g.kz);
+  }
   const int nch = kc0 < kc1 ? kc1 - kc0 : 0;
+  double* const Cz = g.C + (long long)blockIdx.z * g.zstride;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
       for (int t = S - 2; t >= 0; --t) acc = fma(acc, 0.0078125, (double)(int)v[t][u]);
       if (nch == 0) acc = 0.0;
       const double val = ldexp(acc, -(ea + g.expB[j]));
-      double* cp = g.C + i + j * g.ldc;
+      double* cp = Cz + i + j * g.ldc;
       *cp = g.beta != 0.0 ? fma(g.alpha, val, g.beta * *cp) : g.alpha * val;
     }
   }
@@ -345,10 +353,18 @@ static cudaError_t launch_emu(const EmuGemmArgs& g, dim3 grid, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t emu_gemm(const EmuOperand& A, const EmuOperand& B, double* C, long long ldc, double alpha, double beta,
-                     bool lower, long long row0, long long col0, int kmode, int* err, cudaStream_t s) {
-  if (A.S != B.S || A.Kpad != B.Kpad || A.S < 4 || A.S > 7) return cudaErrorInvalidValue;
-  if (A.R <= 0 || B.R <= 0) return cudaSuccess;
+static cudaError_t launch_emu_any(const EmuGemmArgs& g, int S, dim3 grid, cudaStream_t s) {
+  switch (S) {
+    case 4: return launch_emu<4>(g, grid, s);
+    case 5: return launch_emu<5>(g, grid, s);
+    case 6: return launch_emu<6>(g, grid, s);
+    case 7: return launch_emu<7>(g, grid, s);
+    default: return launch_emu<8>(g, grid, s);
+  }
+}
+
+static EmuGemmArgs emu_args(const EmuOperand& A, const EmuOperand& B, double* C, long long ldc, double alpha,
+                            double beta, bool lower, long long row0, long long col0, int kmode, int* err) {
   EmuGemmArgs g;
   g.A = A.slices;
   g.B = B.slices;
@@ -368,14 +384,28 @@ cudaError_t emu_gemm(const EmuOperand& A, const EmuOperand& B, double* C, long l
   g.col0 = col0;
   g.kmode = kmode;
   g.err = err;
+  g.kz = 0;
+  g.zstride = 0;
+  return g;
+}
+
+cudaError_t emu_gemm(const EmuOperand& A, const EmuOperand& B, double* C, long long ldc, double alpha, double beta,
+                     bool lower, long long row0, long long col0, int kmode, int* err, cudaStream_t s) {
+  if (A.S != B.S || A.Kpad != B.Kpad || A.S < 4 || A.S > EMU_MAX_S) return cudaErrorInvalidValue;
+  if (A.R <= 0 || B.R <= 0) return cudaSuccess;
+  const EmuGemmArgs g = emu_args(A, B, C, ldc, alpha, beta, lower, row0, col0, kmode, err);
   // B's padded rows (multiple of 128) cover every 64-row tile the grid touches
-  dim3 grid(A.Rpad / EMU_M, ceil_div(B.R, EMU_N));
-  switch (A.S) {
-    case 4: return launch_emu<4>(g, grid, s);
-    case 5: return launch_emu<5>(g, grid, s);
-    case 6: return launch_emu<6>(g, grid, s);
-    default: return launch_emu<7>(g, grid, s);
-  }
+  return launch_emu_any(g, A.S, dim3(A.Rpad / EMU_M, ceil_div(B.R, EMU_N)), s);
+}
+
+cudaError_t emu_gemm_splitk(const EmuOperand& A, const EmuOperand& B, double* C, long long ldc, long long zstride,
+                            int kz, bool lower, int* err, cudaStream_t s) {
+  if (A.S != B.S || A.Kpad != B.Kpad || A.S < 4 || A.S > EMU_MAX_S || kz <= 0) return cudaErrorInvalidValue;
+  if (A.R <= 0 || B.R <= 0) return cudaSuccess;
+  EmuGemmArgs g = emu_args(A, B, C, ldc, 1.0, 0.0, lower, 0, 0, 0, err);
+  g.kz = kz;
+  g.zstride = zstride;
+  return launch_emu_any(g, A.S, dim3(A.Rpad / EMU_M, ceil_div(B.R, EMU_N), emu_splitk_parts(A.Kpad, kz)), s);
 }
 
 }  // namespace gprx

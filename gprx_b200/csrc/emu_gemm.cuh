@@ -56,6 +56,13 @@ cudaError_t emu_slice(const double* M, long long ld, bool trans, const EmuOperan
 cudaError_t emu_gemm(const EmuOperand& A, const EmuOperand& B, double* C, long long ldc, double alpha, double beta,
                      bool lower, long long row0, long long col0, int kmode, int* err, cudaStream_t s);
 
+// Split K: part z (z < emu_splitk_parts(Kpad, kz)) of the full product,
+// Σ over K chunks [z·kz, (z+1)·kz) of 64 bytes, is written (alpha 1, beta 0)
+// to C + z·zstride; kz·64·S·2^12 < 2^31 keeps each part's int32 sums exact.
+inline int emu_splitk_parts(int Kpad, int kz) { return (Kpad / EMU_KC + kz - 1) / kz; }
+cudaError_t emu_gemm_splitk(const EmuOperand& A, const EmuOperand& B, double* C, long long ldc, long long zstride,
+                            int kz, bool lower, int* err, cudaStream_t s);
+
 size_t emu_gemm_smem(int S);
 
 // Device scratch for the products of one handle: slice planes and exponents

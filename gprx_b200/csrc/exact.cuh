@@ -66,7 +66,10 @@ struct ExactState {
   static constexpr int EMU_MIN_N = 1024;
   // blocks the recursive mixed factor hands to the blocked DMMA factor
   static constexpr int EMU_LEAF_N = 2048;
-  bool use_emu() const { return opt.precision == GPRX_PRECISION_MIXED && n >= EMU_MIN_N; }
+  // largest n (the longest K of a product) whose 7-digit int32 sums stay
+  // exact: K·7·2^12 < 2^31; larger n runs the FP64 products
+  static constexpr int EMU_MAX_N = 65536;
+  bool use_emu() const { return opt.precision == GPRX_PRECISION_MIXED && n >= EMU_MIN_N && n <= EMU_MAX_N; }
   gprx_status ensure_emu();
   void get_params(double* out) const;
   gprx_status write_params(const double* params);

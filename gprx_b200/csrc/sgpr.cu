@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "dense_f64.cuh"
+#include "emu_gemm.cuh"
 #include "kernels.cuh"
 #include "lbfgs.h"
 #include "runtime.cuh"
@@ -264,6 +265,20 @@ struct SgprState {
       qbuf, qbuf2, qx, Btrial;
   DevBuf<int> slot_param;
   DevBuf<DevStatus> status;
+  // mixed precision: the two m×m Gram products over n (B = A Aᵀ and H = G Aᵀ)
+  // emulated on the int8 tensor cores, split over K across CTAs
+  DevBuf<int8_t> emu_sa, emu_sb;
+  DevBuf<double> emu_part;
+  DevBuf<int> emu_ea, emu_eb, emu_err;
+  DevBuf<unsigned long long> emu_ma, emu_mb;
+  HostPinned<int> emu_err_h;
+  static constexpr long long EMU_MIN_N = 16384;  // smallest n that uses the emulated products
+  static constexpr int EMU_S = 7;                // int8 digits per entry
+  static constexpr int EMU_PART_K = 32768;       // K of one split-K part: K·S·2^12 < 2^31 keeps its int32 sums exact
+  static constexpr int EMU_GROUP = 8 * EMU_PART_K;  // columns of n sliced at a time (8 parts in flight)
+  static constexpr int TRSM_LEAF = 256;          // rows of the blocked solves under the recursive m×n solves
+  bool use_emu() const { return opt.precision == GPRX_PRECISION_MIXED && n >= EMU_MIN_N; }
+  gprx_status ensure_emu(EmuWork& w);
   HostPinned<double> res_h;
   HostPinned<DevStatus> status_h;
   FactorCtx fctx;
@@ -474,6 +489,68 @@ static cudaError_t syrk_splitk(const double* A, long long lda, int m, long long 
   return cudaGetLastError();
 }
 
+gprx_status SgprState::ensure_emu(EmuWork& w) {
+  const int kmax = (int)std::min<long long>(EMU_GROUP, n);
+  const size_t bytes = emu_slice_bytes(m, kmax, EMU_S);
+  const size_t rows = (size_t)emu_pad_rows(m);
+  const int parts = emu_splitk_parts(emu_pad_k(kmax), EMU_PART_K / EMU_KC);
+  if (emu_sa.ensure(bytes) || emu_sb.ensure(bytes) || emu_ea.ensure(rows) || emu_eb.ensure(rows) ||
+      emu_ma.ensure(rows) || emu_mb.ensure(rows) || emu_err.ensure(1) || emu_part.ensure((size_t)parts * ldm * m))
+    return set_error(GPRX_OUT_OF_MEMORY, "device allocation of the emulated-product scratch failed");
+  GPRX_CUDA_TRY(emu_err_h.ensure(1));
+  w.sa = emu_sa.p; w.sb = emu_sb.p; w.ea = emu_ea.p; w.eb = emu_eb.p; w.ma = emu_ma.p; w.mb = emu_mb.p;
+  w.err = emu_err.p;
+  w.S = EMU_S;
+  return GPRX_OK;
+}
+
+// C (m×m, lower part only when lower) = (accumulate ? C : 0) + Σ_z part_z,
+// the parts summed in order z = 0, 1, … (deterministic)
+__global__ void gram_parts_kernel(const double* part, long long ldp, long long pstride, int nz, int m, bool lower,
+                                  bool accumulate, double* C, long long ldc) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)m * m;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e % m), j = (int)(e / m);
+    if (lower && i < j) continue;
+    double acc = accumulate ? C[i + (long long)j * ldc] : 0.0;
+    for (int z = 0; z < nz; ++z) acc += part[z * pstride + i + (long long)j * ldp];
+    C[i + (long long)j * ldc] = acc;
+  }
+}
+
+// C (m×m) = X Yᵀ for X, Y m×nn (rows of length nn), lower or full: n sliced in
+// groups of EMU_GROUP columns, each group's product split over K into parts
+// of EMU_PART_K computed side by side and summed in FP64.
+static cudaError_t emu_gram(const double* X, const double* Y, long long ld, int m, long long nn, bool lower, double* C,
+                            long long ldc, const EmuWork& w, double* part, long long ldp, int group, int part_k,
+                            cudaStream_t s) {
+  cudaError_t e = cudaSuccess;
+  const long long pstride = ldp * m;
+  for (long long k0 = 0; k0 < nn && e == cudaSuccess; k0 += group) {
+    const int kc = (int)std::min<long long>(group, nn - k0);
+    EmuOperand a = w.op_a(m, kc);
+    e = emu_slice(X + k0 * ld, ld, false, a, s);
+    EmuOperand b = a;
+    if (e == cudaSuccess && Y != X) {
+      b = w.op_b(m, kc);
+      e = emu_slice(Y + k0 * ld, ld, false, b, s);
+    }
+    const int kz = part_k / EMU_KC;
+    if (e == cudaSuccess) e = emu_gemm_splitk(a, b, part, ldp, pstride, kz, lower, w.err, s);
+    if (e == cudaSuccess) {
+      GPRX_LAUNCH(gram_parts_kernel, grid_for((long long)m * m, 256), 256, 0, s, part, ldp, pstride,
+                  emu_splitk_parts(a.Kpad, kz), m, lower, k0 > 0, C, ldc);
+      e = cudaGetLastError();
+    }
+  }
+  return e;
+}
+
+__global__ void add_diag_kernel(double* C, long long ld, int m, double v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) C[i + (long long)i * ld] += v;
+}
+
 gprx_status SgprState::assemble() {
   if (n > INT32_MAX) return set_error(GPRX_CAPACITY, "n too large for one assembly");
   const int nn = (int)n;
@@ -501,10 +578,23 @@ gprx_status SgprState::assemble() {
   count_launch();
   // A = L⁻¹ K(Z, X)
   GPRX_CUDA_TRY(fill_cross(kern, z.p, m, m, x.p, cap, nn, Amat.p, ldm, status.p, stream));
-  GPRX_CUDA_TRY(trsm_lower(Lmm.p, ldm, m, linv_mm.p, Amat.p, ldm, nn, status.p, stream));
+  EmuWork ew;
+  const bool emu = use_emu();
+  if (emu) {
+    if ((st = ensure_emu(ew)) != GPRX_OK) return st;
+    GPRX_CUDA_TRY(cudaMemsetAsync(emu_err.p, 0, sizeof(int), stream));
+  }
+  GPRX_CUDA_TRY(trsm_lower_rec(Lmm.p, ldm, m, linv_mm.p, Amat.p, ldm, nn, TRSM_LEAF, status.p, stream));
   GPRX_CUDA_TRY(cudaEventRecord(ev[1], stream));
   // B = A Aᵀ + σ² I, L_B
-  GPRX_CUDA_TRY(syrk_splitk(Amat.p, ldm, m, nn, Amat.p, ldm, true, noise(), splitbuf, Bl.p, ldm, status.p, stream));
+  if (emu) {
+    GPRX_CUDA_TRY(emu_gram(Amat.p, Amat.p, ldm, m, nn, true, Bl.p, ldm, ew, emu_part.p, ldm, EMU_GROUP, EMU_PART_K,
+                           stream));
+    add_diag_kernel<<<ceil_div(m, 256), 256, 0, stream>>>(Bl.p, ldm, m, noise());
+    count_launch();
+  } else {
+    GPRX_CUDA_TRY(syrk_splitk(Amat.p, ldm, m, nn, Amat.p, ldm, true, noise(), splitbuf, Bl.p, ldm, status.p, stream));
+  }
   GPRX_CUDA_TRY(potrf_blocked(Bl.p, ldm, m, linv_B.p, status.p, stream, &fctx));
   // ‖A‖²_F and A y
   int blocks = grid_for((long long)m * nn, 1024);
@@ -523,7 +613,9 @@ gprx_status SgprState::assemble() {
     count_launch();
   }
   GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p + 10, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+  if (emu) GPRX_CUDA_TRY(cudaMemcpyAsync(emu_err_h.p, emu_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
   if ((st = sync_check(GPRX_STAGE_FIT)) != GPRX_OK) return st;
+  if (emu && *emu_err_h.p) return set_error(GPRX_TIMEOUT, "an emulated product's bounded wait ran out");
   pivot_ratio = res_h.p[0];
   afro = res_h.p[1];
   kdiag_sum = (double)n * kern.diag_value();
@@ -565,17 +657,28 @@ gprx_status SgprState::gradient(double* grad) {
       Xt.ensure((size_t)ldm * m) != cudaSuccess)
     return set_error(GPRX_OUT_OF_MEMORY, "gradient buffers");
   if ((st = reset_status()) != GPRX_OK) return st;
-  // G = B⁻¹ A − (w rᵀ + A)/σ²
+  // G = B⁻¹ A − (w rᵀ + A)/σ²: B⁻¹ A by the two triangular solves (an
+  // explicit B⁻¹ would carry cond(B)·ε into the small residual G)
+  const bool emu = use_emu();
+  EmuWork ew;
+  if (emu) {
+    if ((st = ensure_emu(ew)) != GPRX_OK) return st;
+    GPRX_CUDA_TRY(cudaMemsetAsync(emu_err.p, 0, sizeof(int), stream));
+  }
   GPRX_CUDA_TRY(cudaMemcpyAsync(G.p, Amat.p, sizeof(double) * ldm * nn, cudaMemcpyDeviceToDevice, stream));
-  GPRX_CUDA_TRY(trsm_lower(Bl.p, ldm, m, linv_B.p, G.p, ldm, nn, status.p, stream));
-  GPRX_CUDA_TRY(trsm_lower_t(Bl.p, ldm, m, linv_B.p, G.p, ldm, nn, status.p, stream));
+  GPRX_CUDA_TRY(trsm_lower_rec(Bl.p, ldm, m, linv_B.p, G.p, ldm, nn, TRSM_LEAF, status.p, stream));
+  GPRX_CUDA_TRY(trsm_lower_t_rec(Bl.p, ldm, m, linv_B.p, G.p, ldm, nn, TRSM_LEAF, status.p, stream));
   adjoint_update_kernel<<<grid_for((long long)nn * 32, 256), 256, 0, stream>>>(Amat.p, G.p, ldm, m, nn, w.p, y.p,
                                                                                 1.0 / noise_v, status.p);
   count_launch();
-  // H = G Aᵀ
-  GPRX_CUDA_TRY(syrk_splitk(G.p, ldm, m, nn, Amat.p, ldm, false, 0.0, splitbuf, H.p, ldm, status.p, stream));
-  // w_mn = L⁻ᵀ G
-  GPRX_CUDA_TRY(trsm_lower_t(Lmm.p, ldm, m, linv_mm.p, G.p, ldm, nn, status.p, stream));
+  // H = G Aᵀ; w_mn = L⁻ᵀ G
+  if (emu) {
+    GPRX_CUDA_TRY(emu_gram(G.p, Amat.p, ldm, m, nn, false, H.p, ldm, ew, emu_part.p, ldm, EMU_GROUP, EMU_PART_K,
+                           stream));
+  } else {
+    GPRX_CUDA_TRY(syrk_splitk(G.p, ldm, m, nn, Amat.p, ldm, false, 0.0, splitbuf, H.p, ldm, status.p, stream));
+  }
+  GPRX_CUDA_TRY(trsm_lower_t_rec(Lmm.p, ldm, m, linv_mm.p, G.p, ldm, nn, TRSM_LEAF, status.p, stream));
   // w_mm = −sym(L⁻ᵀ tril½(H) L⁻¹)
   tril_half_kernel<<<grid_for((long long)m * m, 256), 256, 0, stream>>>(H.p, ldm, m, Xb.p);
   count_launch();
@@ -606,7 +709,9 @@ gprx_status SgprState::gradient(double* grad) {
   GPRX_CUDA_TRY(dot_dev(w.p, w.p, m, res.p + 3, status.p, stream));
   GPRX_CUDA_TRY(dot_dev(ay.p, w.p, m, res.p + 4, status.p, stream));
   GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p, sizeof(double) * 60, cudaMemcpyDeviceToHost, stream));
+  if (emu) GPRX_CUDA_TRY(cudaMemcpyAsync(emu_err_h.p, emu_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
   if ((st = sync_check(GPRX_STAGE_FIT)) != GPRX_OK) return st;
+  if (emu && *emu_err_h.p) return set_error(GPRX_TIMEOUT, "an emulated product's bounded wait ran out");
   const int nk = kern.n_params;
   std::vector<double> dg;
   diag_grad(kern, dg);

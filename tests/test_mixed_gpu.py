@@ -82,3 +82,51 @@ def test_mixed_small_n_is_the_fp64_path():
     a = model(spec, 0.05, x, n, d, y, gx.Precision.Mixed).value_and_gradient(params)
     b = model(spec, 0.05, x, n, d, y, gx.Precision.Fp64).value_and_gradient(params)
     assert a[0] == b[0] and np.array_equal(a[1], b[1])
+
+
+def test_mixed_sgpr_matches_oracle():
+    # n ≥ 16384 takes the emulated Gram products B = AAᵀ and H = GAᵀ (K
+    # split into parts of 32768); the m×n solves stay FP64
+    n, m, d = 70000, 256, 3
+    rs = np.random.RandomState(12)
+    x = rs.uniform(0, 1, size=n * d)
+    y = np.sin(6 * x[:n]) + np.cos(4 * x[n:2 * n]) + 0.1 * rs.standard_normal(n)
+    idx = rs.choice(n, m, replace=False)
+    z = x.reshape(d, n)[:, idx].reshape(-1).copy()
+    ls = [0.3, 0.5, 0.4]
+    params = np.array([math.log(v) for v in ls] + [math.log(0.05)])
+    orc = O.Sgpr([[11, d]], params, x, n, d, y, z, m)
+    spec = gx.RbfArdKernel(ls)
+    out = {}
+    for prec in (gx.Precision.Mixed, gx.Precision.Fp64):
+        f = gx.Sgpr(spec, gx.GaussianLikelihood(0.05), precision=prec).with_optimizer(gx.Fixed()).factor(
+            x, n, d, y, z, m)
+        out[prec] = f.value_and_gradient(params)
+    nl, g = out[gx.Precision.Mixed]
+    nl_f, g_f = out[gx.Precision.Fp64]
+    assert O.rel_err(nl, orc.nlml()) <= TOL_NLML, (nl, orc.nlml())
+    assert np.all(O.rel_err(g, orc.grad()) <= TOL_GRAD), (g, orc.grad())
+    assert O.rel_err(nl, nl_f) <= TOL_NLML
+    assert np.all(O.rel_err(g, g_f) <= TOL_GRAD)
+
+
+def test_mixed_sgpr_matches_fp64_m1024():
+    # m = 1024 inducing points: the Gram parts cover a 1024² output (more
+    # elements than one grid-stride pass of the reduction), n over one
+    # split-K part of 32768
+    n, m, d = 40000, 1024, 4
+    rs = np.random.RandomState(5)
+    x = rs.uniform(0, 1, size=n * d)
+    y = np.sin(5 * x[:n]) + np.cos(3 * x[n:2 * n]) + 0.1 * rs.standard_normal(n)
+    z = x.reshape(d, n)[:, rs.choice(n, m, replace=False)].reshape(-1).copy()
+    ls = [0.6, 0.9, 1.3, 0.8]
+    params = np.array([math.log(v) for v in ls] + [math.log(0.1)])
+    out = {}
+    for prec in (gx.Precision.Mixed, gx.Precision.Fp64):
+        f = gx.Sgpr(gx.RbfArdKernel(ls), gx.GaussianLikelihood(0.1), precision=prec).with_optimizer(
+            gx.Fixed()).factor(x, n, d, y, z, m)
+        out[prec] = f.value_and_gradient(params)
+    nl, g = out[gx.Precision.Mixed]
+    nl_f, g_f = out[gx.Precision.Fp64]
+    assert O.rel_err(nl, nl_f) <= TOL_NLML, (nl, nl_f)
+    assert np.all(O.rel_err(g, g_f) <= TOL_GRAD), (g, g_f)
