@@ -253,6 +253,15 @@ def batched_measure(torch, dev, count=BATCH_P, single_sample=32, cpu_sample=48, 
     e1.record(stream)
     torch.cuda.synchronize()
     round_ms = e0.elapsed_time(e1)
+    # the autotuned schedule against the one fixed 64×128 tile shape
+    tiles, tune_ms, _ = b.schedule()
+    b.set_schedule([0] * gx.GprBatch.SIZE_CLASSES)
+    e0.record(stream)
+    b.value_and_gradient(theta0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    round_ms_fixed = e0.elapsed_time(e1)
+    b.set_schedule(tiles)
     flops = float((sizes.astype(np.float64) ** 3).sum())
     achieved = flops / (round_ms * 1e-3) / 1e12
     # one model per launch: the single-model path on every k-th problem
@@ -292,6 +301,10 @@ def batched_measure(torch, dev, count=BATCH_P, single_sample=32, cpu_sample=48, 
         "one_model_per_launch": {"value": single_fps, "unit": "fits/s",
                                  "sample": "%d problems (every %d-th), Gpr.fit each" % (len(idx), count // single_sample)},
         "speedup_vs_one_model_per_launch": (count / fit_s) / single_fps,
+        "schedule": {"size_classes": "n <= 64, 128, 256, ..., 4096, larger",
+                     "tile_shapes": [list(t) for t in gx.GprBatch.TILE_SHAPES],
+                     "tile_of_class": [int(v) for v in tiles],
+                     "round_ms_autotuned": round_ms, "round_ms_fixed_64x128": round_ms_fixed},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak if fp64_peak else None, "kernel": "batch_eval_kernel",
                      "work": "sum of n_i^3 flop per evaluation round", "round_ms": round_ms},

@@ -145,6 +145,9 @@ _SIGS = {
     "gprx_batch_fit": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.POINTER(LbfgsOptions), D, C.POINTER(FitReport),
                                    I32]),
     "gprx_batch_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "gprx_batch_autotune": (C.c_int32, [C.c_void_p, D, C.c_uint64]),
+    "gprx_batch_set_schedule": (C.c_int32, [C.c_void_p, I32]),
+    "gprx_batch_schedule": (C.c_int32, [C.c_void_p, I32, C.POINTER(C.c_float), I32]),
     "gprx_server_options_default": (None, [C.POINTER(ServerOptions)]),
     "gprx_server_create": (C.c_int32, [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
     "gprx_server_destroy": (C.c_int32, [C.c_void_p]),

@@ -772,6 +772,36 @@ class GprBatch:
         check(L.lib().gprx_batch_stream(self._h, C.byref(s)))
         return s.value or 0
 
+    # size classes of the schedule (n ≤ 64, ≤ 128, …, ≤ 4096, larger) and the
+    # in-CTA GEMM tile shapes (M, N, K) the autotuner chooses from
+    SIZE_CLASSES = 8
+    TILE_SHAPES = ((64, 128, 32), (64, 64, 32), (32, 64, 32), (32, 32, 16))
+
+    def autotune(self, params):
+        """Times every tile shape on every size class present at θ = params
+        and keeps the fastest (the first evaluation or fit does this by
+        itself); returns schedule()."""
+        a = self._params(params)
+        check(L.lib().gprx_batch_autotune(self._h, L.ptr(a), self.p))
+        return self.schedule()
+
+    def set_schedule(self, tile_of_class):
+        """Fixes the tile shape index of each size class (turns tuning off)."""
+        t = np.ascontiguousarray(np.asarray(tile_of_class, dtype=np.int32))
+        if t.shape != (self.SIZE_CLASSES,):
+            raise ShapeMismatch("one tile shape index per size class (%d)" % self.SIZE_CLASSES)
+        check(L.lib().gprx_batch_set_schedule(self._h, t.ctypes.data_as(L.I32)))
+
+    def schedule(self):
+        """(tile shape per size class, tuning ms per launch [class, shape],
+        whether tuning ran)."""
+        t = np.zeros(self.SIZE_CLASSES, dtype=np.int32)
+        ms = np.zeros((self.SIZE_CLASSES, len(self.TILE_SHAPES)), dtype=np.float32)
+        tuned = np.zeros(1, dtype=np.int32)
+        check(L.lib().gprx_batch_schedule(self._h, t.ctypes.data_as(L.I32), ms.ctypes.data_as(C.POINTER(C.c_float)),
+                                          tuned.ctypes.data_as(L.I32)))
+        return t, ms, bool(tuned[0])
+
     def value_and_gradient(self, params):
         """NLML, gradient and status of every problem at its own θ (row i)."""
         a = self._params(params)

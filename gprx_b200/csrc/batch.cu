@@ -29,6 +29,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -59,6 +60,14 @@ struct JitterList {
   double j[BATCH_MAX_JITTERS];
 };
 
+// size classes of the autotuned schedule: n ≤ 64, ≤ 128, …, ≤ 4096, > 4096
+constexpr int BATCH_SIZE_CLASSES = 8;
+__host__ __device__ inline int batch_size_class(int n) {
+  int c = 0;
+  for (int lim = 64; c < BATCH_SIZE_CLASSES - 1 && n > lim; lim *= 2) ++c;
+  return c;
+}
+
 struct BatchHeader {
   int queue;   // next position in the work order
   int active;  // problems the optimizer round left pending
@@ -78,6 +87,7 @@ struct BatchEvalArgs {
   BatchHeader* hdr;
   double* work;  // per-CTA workspaces
   long long work_stride;
+  int8_t tile_of_class[BATCH_SIZE_CLASSES];  // in-CTA GEMM tile shape per size class (autotuned)
   int nmax;
   JitterList jit;
   KTree tmpl;  // tree structure (θ-dependent constants are set per problem)
@@ -274,7 +284,7 @@ __device__ inline bool in_default_interval(double log_v) {
 
 // LLT of the lower n×n matrix in w.A with the diagonal-block inverses in
 // w.linv.  Returns the failing column or −1.
-__device__ int cta_potrf(const Work& w, int n, long long ld, double* smem, int* fail_sh) {
+__device__ int cta_potrf(const Work& w, int n, long long ld, double* smem, int* fail_sh, int cfg) {
   for (int k0 = 0; k0 < n; k0 += NB_DIAG) {
     const int nbk = min(NB_DIAG, n - k0);
     double* lk = w.linv + (long long)(k0 / NB_DIAG) * NB_DIAG * NB_DIAG;
@@ -283,18 +293,19 @@ __device__ int cta_potrf(const Work& w, int n, long long ld, double* smem, int* 
     const int rest = n - k0 - nbk;
     if (rest <= 0) break;
     double* P = w.A + (k0 + nbk) + (long long)k0 * ld;
-    // P := P L_kk⁻ᵀ (in place: one tile spans all nbk ≤ 128 columns)
-    cta_gemm<false, true>(rest, nbk, nbk, P, ld, lk, NB_DIAG, P, ld, 1.0, 0.0, false, CG_FULL, smem);
+    // P := P L_kk⁻ᵀ (in place: one tile must span all nbk columns)
+    cta_gemm<false, true>(nbk <= cg_tile_n(cfg) ? cfg : 0, rest, nbk, nbk, P, ld, lk, NB_DIAG, P, ld, 1.0, 0.0, false,
+                          CG_FULL, smem);
     // A22 −= P Pᵀ (lower)
     double* A22 = w.A + (k0 + nbk) + (long long)(k0 + nbk) * ld;
-    cta_gemm<false, true>(rest, rest, nbk, P, ld, P, ld, A22, ld, -1.0, 1.0, true, CG_FULL, smem);
+    cta_gemm<false, true>(cfg, rest, rest, nbk, P, ld, P, ld, A22, ld, -1.0, 1.0, true, CG_FULL, smem);
   }
   return -1;
 }
 
 // X = L⁻¹ (lower, the upper part of every diagonal block zero), block rows
 // top to bottom: X_ii = L_ii⁻¹, X_i,<i = −L_ii⁻¹ (L_i,<i X_<i,<i).
-__device__ void cta_trtri(const Work& w, int n, long long ld, double* smem) {
+__device__ void cta_trtri(const Work& w, int n, long long ld, double* smem, int cfg) {
   for (int r0 = 0; r0 < n; r0 += NB_DIAG) {
     const int nbi = min(NB_DIAG, n - r0);
     const double* li = w.linv + (long long)(r0 / NB_DIAG) * NB_DIAG * NB_DIAG;
@@ -304,9 +315,10 @@ __device__ void cta_trtri(const Work& w, int n, long long ld, double* smem) {
     }
     if (r0 == 0) continue;
     // T = L_i,<i X_<i,<i  (X lower: k from the tile's first column)
-    cta_gemm<false, false>(nbi, r0, r0, w.A + r0, ld, w.X, ld, w.T, NB_DIAG, 1.0, 0.0, false, CG_FROM_COL, smem);
+    cta_gemm<false, false>(cfg, nbi, r0, r0, w.A + r0, ld, w.X, ld, w.T, NB_DIAG, 1.0, 0.0, false, CG_FROM_COL, smem);
     // X_i,<i = −L_ii⁻¹ T
-    cta_gemm<false, false>(nbi, r0, nbi, li, NB_DIAG, w.T, NB_DIAG, w.X + r0, ld, -1.0, 0.0, false, CG_FULL, smem);
+    cta_gemm<false, false>(cfg, nbi, r0, nbi, li, NB_DIAG, w.T, NB_DIAG, w.X + r0, ld, -1.0, 0.0, false, CG_FULL,
+                           smem);
   }
   __syncthreads();
 }
@@ -321,6 +333,7 @@ __device__ void cta_eval(const BatchEvalArgs& a, int q, const Work& w, double* s
   const BatchProblem P = a.probs[q];
   const int n = P.n, tid = threadIdx.x, p = a.p;
   const long long ld = batch_ld(n);
+  const int cfg = a.tile_of_class[batch_size_class(n)];
   const double* th = a.log_theta + (long long)q * p;
   if (tid == 0) {
     tree = a.tmpl;
@@ -344,7 +357,7 @@ __device__ void cta_eval(const BatchEvalArgs& a, int q, const Work& w, double* s
       if (tid == 0) a.status[q] = GPRX_NONFINITE_KERNEL;
       return;
     }
-    fail = cta_potrf(w, n, ld, smem, &flag_sh);
+    fail = cta_potrf(w, n, ld, smem, &flag_sh, cfg);
     if (fail < 0) break;
   }
   if (fail >= 0) {
@@ -354,7 +367,7 @@ __device__ void cta_eval(const BatchEvalArgs& a, int q, const Work& w, double* s
   double acc = 0.0;
   for (int i = tid; i < n; i += BT) acc += log(w.A[i + (long long)i * ld]);
   const double logdet = 2.0 * block_sum(acc, red);
-  cta_trtri(w, n, ld, smem);
+  cta_trtri(w, n, ld, smem, cfg);
   // z = X y (rows), α = Xᵀ z (columns)
   for (int i = tid; i < n; i += BT) {
     double s = 0.0;
@@ -376,7 +389,7 @@ __device__ void cta_eval(const BatchEvalArgs& a, int q, const Work& w, double* s
   for (int i = tid; i < n; i += BT) acc = fma(P.y[i], w.alpha[i], acc);
   const double quad = block_sum(acc, red);
   // K⁻¹ = Xᵀ X (lower) over L in A
-  cta_gemm<true, false>(n, n, n, w.X, ld, w.X, ld, w.A, ld, 1.0, 0.0, true, CG_FROM_ROW, smem);
+  cta_gemm<true, false>(cfg, n, n, n, w.X, ld, w.X, ld, w.A, ld, 1.0, 0.0, true, CG_FROM_ROW, smem);
   cta_grad<ARD_D>(tree, P.x, n, w.A, ld, w.alpha, smem, slots);
   if (tid == 0) {
     constexpr int NS = GRAD_SLOTS_LEAF + (ARD_D > 0 ? ARD_D : 1) + 1;
@@ -580,6 +593,14 @@ struct BatchState {
   int graph_rounds = 0;
   FitArgs graph_args{};
   bool graph_valid = false;
+  // schedule: in-CTA GEMM tile shape per size class, autotuned at the first
+  // evaluation unless set by the caller
+  std::vector<int> ord_host;  // the work order (largest n first)
+  std::string tree_sig;       // kernel tree, for the process-wide tuning cache
+  int8_t tiles[BATCH_SIZE_CLASSES] = {};
+  float tune_ms[BATCH_SIZE_CLASSES][CG_CONFIGS] = {};
+  bool tuned = false, tiles_fixed = false;
+  DevBuf<int> tune_order;
 
   ~BatchState() {
     if (stream) cudaStreamSynchronize(stream);
@@ -595,6 +616,7 @@ struct BatchState {
   gprx_status eval(const double* log_theta, double* nl, double* g, int32_t* st);
   gprx_status fit(const double* theta0, const gprx_lbfgs_options* o, double* theta_out, gprx_fit_report* reports,
                   int32_t* st_out);
+  gprx_status autotune(const double* log_theta_dev, bool force);
 };
 
 static JitterList jitter_list(const gprx_options& o) {
@@ -677,6 +699,9 @@ gprx_status BatchState::create(const double* xh, const double* yh, const uint64_
   std::vector<int> ord(nprob);
   std::iota(ord.begin(), ord.end(), 0);
   std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return n_host[a] > n_host[b]; });
+  ord_host = ord;
+  tree_sig = std::to_string(d) + ":";
+  for (int i = 0; i < n_nodes; ++i) tree_sig += std::to_string(nodes[i].kind) + "," + std::to_string(nodes[i].arg) + ";";
   GPRX_CUDA_TRY(cudaMemcpyAsync(probs.p, ph.data(), sizeof(BatchProblem) * nprob, cudaMemcpyHostToDevice, stream));
   GPRX_CUDA_TRY(cudaMemcpyAsync(order.p, ord.data(), sizeof(int) * nprob, cudaMemcpyHostToDevice, stream));
   GPRX_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -701,7 +726,75 @@ BatchEvalArgs BatchState::eval_args(const int* active_dev, const double* log_the
   a.jit = jitter_list(opt);
   a.tmpl = kern.tree;
   for (int i = 0; i < 64; ++i) a.slot_param[i] = i < (int)kern.slot_param.size() ? kern.slot_param[i] : -1;
+  for (int c = 0; c < BATCH_SIZE_CLASSES; ++c) a.tile_of_class[c] = tiles[c];
   return a;
+}
+
+// ---------------------------------------------------------------------------
+// autotuner: for every size class present, time one evaluation launch of a
+// sample of that class's problems (up to two per CTA, at the given θ) with
+// each tile shape, and keep the fastest.  Results are cached per device,
+// kernel tree and class for the life of the process.  Every shape gives the
+// same results bit for bit (cta_gemm.cuh), so tuning changes only the time.
+// ---------------------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tune_cache;
+
+gprx_status BatchState::autotune(const double* log_theta_dev, bool force) {
+  if (tiles_fixed || (tuned && !force)) return GPRX_OK;
+  cudaDeviceProp prop;
+  GPRX_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  const std::string key0 = std::string(prop.name) + "|" + std::to_string(device) + "|" + tree_sig + "|";
+  std::vector<std::vector<int>> by_class(BATCH_SIZE_CLASSES);
+  for (int q : ord_host) by_class[batch_size_class(n_host[q])].push_back(q);
+  if (tune_order.ensure((size_t)std::max(nprob, 1)) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "tuning buffers");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  GPRX_CUDA_TRY(cudaEventCreate(&e0));
+  GPRX_CUDA_TRY(cudaEventCreate(&e1));
+  struct Ev {
+    cudaEvent_t a, b;
+    ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); }
+  } guard{e0, e1};
+  for (int c = 0; c < BATCH_SIZE_CLASSES; ++c) {
+    if (by_class[c].empty()) continue;
+    const std::string key = key0 + std::to_string(c);
+    if (!force) {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      auto it = g_tune_cache.find(key);
+      if (it != g_tune_cache.end()) {
+        tiles[c] = (int8_t)it->second;
+        continue;
+      }
+    }
+    const int ns = (int)std::min<size_t>(by_class[c].size(), (size_t)2 * ctas);
+    GPRX_CUDA_TRY(cudaMemcpyAsync(tune_order.p, by_class[c].data(), sizeof(int) * ns, cudaMemcpyHostToDevice, stream));
+    BatchEvalArgs a = eval_args(nullptr, log_theta_dev);
+    a.order = tune_order.p;
+    a.nprob = ns;
+    int best = 0;
+    for (int cfg = 0; cfg < CG_CONFIGS; ++cfg) {
+      a.tile_of_class[c] = (int8_t)cfg;
+      GPRX_CUDA_TRY(cudaMemsetAsync(hdr.p, 0, sizeof(BatchHeader), stream));
+      GPRX_CUDA_TRY(launch_eval(a));  // warm-up
+      float ms = 0.0f;
+      GPRX_CUDA_TRY(cudaEventRecord(e0, stream));
+      for (int r = 0; r < 2; ++r) {
+        GPRX_CUDA_TRY(cudaMemsetAsync(hdr.p, 0, sizeof(BatchHeader), stream));
+        GPRX_CUDA_TRY(launch_eval(a));
+      }
+      GPRX_CUDA_TRY(cudaEventRecord(e1, stream));
+      GPRX_CUDA_TRY(cudaEventSynchronize(e1));
+      GPRX_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      tune_ms[c][cfg] = ms / 2.0f;
+      if (tune_ms[c][cfg] < tune_ms[c][best]) best = cfg;
+    }
+    tiles[c] = (int8_t)best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = best;
+  }
+  tuned = true;
+  return GPRX_OK;
 }
 
 template <int ARD_D>
@@ -737,6 +830,8 @@ gprx_status BatchState::eval(const double* log_theta, double* nl, double* g, int
   GPRX_CUDA_TRY(cudaSetDevice(device));
   GPRX_CUDA_TRY(
       cudaMemcpyAsync(theta.p, log_theta, sizeof(double) * nprob * p, cudaMemcpyHostToDevice, stream));
+  gprx_status ts = autotune(theta.p, false);
+  if (ts != GPRX_OK) return ts;
   GPRX_CUDA_TRY(cudaMemsetAsync(hdr.p, 0, sizeof(BatchHeader), stream));
   GPRX_CUDA_TRY(cudaMemsetAsync(nlml.p, 0, sizeof(double) * nprob, stream));
   GPRX_CUDA_TRY(launch_eval(eval_args(nullptr, theta.p)));
@@ -815,8 +910,11 @@ gprx_status BatchState::fit(const double* theta0, const gprx_lbfgs_options* o, d
   GPRX_CUDA_TRY(cudaMemsetAsync(hdr.p, 0, sizeof(BatchHeader), stream));
   GPRX_LAUNCH(fit_init_kernel, fg, fb, 0, stream, fa);
   GPRX_CUDA_TRY(cudaGetLastError());
-  // one graph: ROUNDS_PER_GRAPH × {reset header, evaluate, advance}, then the
-  // header back to the host
+  // the schedule at the starting points, then one graph: ROUNDS_PER_GRAPH ×
+  // {reset header, evaluate, advance}, then the header back to the host
+  gprx_status ts = autotune(theta.p, false);
+  if (ts != GPRX_OK) return ts;
+  GPRX_CUDA_TRY(cudaMemsetAsync(hdr.p, 0, sizeof(BatchHeader), stream));
   const BatchEvalArgs ea = eval_args(active.p, theta.p);
   if (graph) {
     cudaGraphExecDestroy(graph);
@@ -1064,6 +1162,36 @@ gprx_status gprx_batch_fit(gprx_batch* h, const double* params0, uint64_t p, con
   if (!h) return set_error(GPRX_INVALID_ARGUMENT, "null handle");
   if (p != (uint64_t)h->s.p) return set_error(GPRX_SHAPE_MISMATCH, "params must hold p values per problem");
   return h->s.fit(params0, opt, params_out, reports, status);
+}
+
+gprx_status gprx_batch_autotune(gprx_batch* h, const double* params, uint64_t p) {
+  if (!h || !params) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (p != (uint64_t)h->s.p) return set_error(GPRX_SHAPE_MISMATCH, "params must hold p values per problem");
+  BatchState& s = h->s;
+  GPRX_CUDA_TRY(cudaSetDevice(s.device));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(s.theta.p, params, sizeof(double) * s.nprob * s.p, cudaMemcpyHostToDevice, s.stream));
+  s.tiles_fixed = false;
+  return s.autotune(s.theta.p, true);
+}
+
+gprx_status gprx_batch_set_schedule(gprx_batch* h, const int32_t* tile_of_class) {
+  if (!h || !tile_of_class) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  for (int c = 0; c < BATCH_SIZE_CLASSES; ++c)
+    if (tile_of_class[c] < 0 || tile_of_class[c] >= CG_CONFIGS)
+      return set_error(GPRX_INVALID_CONFIG, "tile shape index out of range");
+  for (int c = 0; c < BATCH_SIZE_CLASSES; ++c) h->s.tiles[c] = (int8_t)tile_of_class[c];
+  h->s.tiles_fixed = true;
+  return GPRX_OK;
+}
+
+gprx_status gprx_batch_schedule(const gprx_batch* h, int32_t* tile_of_class, float* tune_ms, int32_t* tuned) {
+  if (!h) return set_error(GPRX_INVALID_ARGUMENT, "null handle");
+  for (int c = 0; c < BATCH_SIZE_CLASSES; ++c) {
+    if (tile_of_class) tile_of_class[c] = h->s.tiles[c];
+    for (int k = 0; k < CG_CONFIGS && tune_ms; ++k) tune_ms[c * CG_CONFIGS + k] = h->s.tune_ms[c][k];
+  }
+  if (tuned) *tuned = h->s.tuned ? 1 : 0;
+  return GPRX_OK;
 }
 
 gprx_status gprx_batch_stream(gprx_batch* h, void** stream) {

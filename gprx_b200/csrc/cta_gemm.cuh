@@ -6,16 +6,21 @@
 //   opA(i,k) = TA ? A[k + i·lda] : A[i + k·lda]
 //   opB(k,j) = TB ? B[j + k·ldb] : B[k + j·ldb]
 //
-// Output tiles are 64×128 (8 warps of 32×32, DMMA m16n8k4).  The k chunks
-// (32 deep) of ALL tiles form one stream through a 3-stage cp.async ring, so
-// the next tile's first chunks load while the current tile computes, and the
-// C values a tile needs (beta ≠ 0) are fetched into registers when the tile
-// starts.  Shared-memory layouts follow each operand's contiguous direction
-// (16-byte copies) with leading dimensions ≡ 4 mod 16 doubles, which keeps
-// every fragment load free of bank conflicts.
+// Output tiles are TM×TN (8 warps in a 2×4 grid of (TM/2)×(TN/4) DMMA
+// m16n8k4 blocks); the shapes the autotuner picks from are listed in
+// CgTile below.  The k chunks (TK deep) of ALL tiles form one stream through
+// a 3-stage cp.async ring, so the next tile's first chunks load while the
+// current tile computes, and the C values a tile needs (beta ≠ 0) are fetched
+// into registers when the tile starts.  Shared-memory layouts follow each
+// operand's contiguous direction (16-byte copies) with leading dimensions
+// ≡ 4 mod 16 doubles, which keeps every fragment load free of bank conflicts.
+//
+// Every tile shape sums each output's k terms in the same order (k ascending
+// from a multiple of 4, four per DMMA), so the results do not depend on the
+// shape.
 //
 // lower: only entries i ≥ j are written; tiles wholly above the diagonal are
-// skipped and warps whose 32×32 block is wholly above it only help load.
+// skipped and warps whose block is wholly above it only help load.
 // kmode: CG_FULL kb = 0; CG_FROM_ROW kb = the tile's first row (opA(i,k) = 0
 // for k < i); CG_FROM_COL kb = the tile's first column (opB(k,j) = 0 for
 // k < j).  A tile reads all its inputs before it writes C, so C may alias A's
@@ -27,33 +32,47 @@
 namespace gprx {
 
 constexpr int CG_THREADS = 256;
-constexpr int CG_M = 64, CG_N = 128, CG_K = 32;
 constexpr int CG_STAGES = 3;
 constexpr int CG_FULL = 0, CG_FROM_ROW = 1, CG_FROM_COL = 2;
 
-template <bool TA>
-struct CgA {  // A chunk: 64 (i) × 32 (k)
-  static constexpr int LD = TA ? CG_K + 4 : CG_M + 4;
-  static constexpr int ELEMS = TA ? CG_M * LD : CG_K * LD;
+// tile shapes (TM × TN, k chunk TK) by configuration index
+constexpr int CG_CONFIGS = 4;
+template <int CFG>
+struct CgTile;
+template <> struct CgTile<0> { static constexpr int M = 64, N = 128, K = 32; };
+template <> struct CgTile<1> { static constexpr int M = 64, N = 64, K = 32; };
+template <> struct CgTile<2> { static constexpr int M = 32, N = 64, K = 32; };
+template <> struct CgTile<3> { static constexpr int M = 32, N = 32, K = 16; };
+__host__ __device__ constexpr int cg_tile_n(int cfg) { return cfg == 0 ? 128 : cfg == 3 ? 32 : 64; }
+__host__ __device__ constexpr int cg_tile_m(int cfg) { return cfg <= 1 ? 64 : 32; }
+
+template <bool TA, int TM, int TK>
+struct CgA {  // A chunk: TM (i) × TK (k)
+  static constexpr int LD = TA ? TK + 4 : TM + 4;
+  static constexpr int ELEMS = TA ? TM * LD : TK * LD;
   __device__ static int at(int i, int k) { return TA ? i * LD + k : k * LD + i; }
 };
-template <bool TB>
-struct CgB {  // B chunk: 32 (k) × 128 (j)
-  static constexpr int LD = TB ? CG_N + 4 : CG_K + 4;
-  static constexpr int ELEMS = TB ? CG_K * LD : CG_N * LD;
+template <bool TB, int TN, int TK>
+struct CgB {  // B chunk: TK (k) × TN (j)
+  static constexpr int LD = TB ? TN + 4 : TK + 4;
+  static constexpr int ELEMS = TB ? TK * LD : TN * LD;
   __device__ static int at(int k, int j) { return TB ? k * LD + j : j * LD + k; }
 };
 
-template <bool TA, bool TB>
-constexpr int cg_stage_elems() {
-  return CgA<TA>::ELEMS + CgB<TB>::ELEMS;
+template <int CFG>
+constexpr size_t cg_smem_bytes_cfg() {
+  using T = CgTile<CFG>;
+  constexpr int a = CgA<true, T::M, T::K>::ELEMS > CgA<false, T::M, T::K>::ELEMS ? CgA<true, T::M, T::K>::ELEMS
+                                                                                 : CgA<false, T::M, T::K>::ELEMS;
+  constexpr int b = CgB<true, T::N, T::K>::ELEMS > CgB<false, T::N, T::K>::ELEMS ? CgB<true, T::N, T::K>::ELEMS
+                                                                                 : CgB<false, T::N, T::K>::ELEMS;
+  return (size_t)CG_STAGES * (a + b) * sizeof(double);
 }
+constexpr size_t cg_max2(size_t a, size_t b) { return a > b ? a : b; }
+// the largest stage ring over the shapes and the four orientations
 constexpr size_t cg_smem_bytes() {
-  // the largest stage over the four orientations
-  return (size_t)CG_STAGES * (CgA<true>::ELEMS > CgA<false>::ELEMS ? CgA<true>::ELEMS : CgA<false>::ELEMS) *
-             sizeof(double) +
-         (size_t)CG_STAGES * (CgB<true>::ELEMS > CgB<false>::ELEMS ? CgB<true>::ELEMS : CgB<false>::ELEMS) *
-             sizeof(double);
+  return cg_max2(cg_max2(cg_smem_bytes_cfg<0>(), cg_smem_bytes_cfg<1>()),
+                 cg_max2(cg_smem_bytes_cfg<2>(), cg_smem_bytes_cfg<3>()));
 }
 
 // 16-byte copy of src_bytes ∈ {0, 8, 16} (the rest zero-filled)
@@ -62,12 +81,14 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
 }
 
-template <bool TA, bool TB>
-__device__ void cta_gemm(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
+template <bool TA, bool TB, int CFG>
+__device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
                          double* C, long long ldc, double alpha, double beta, bool lower, int kmode, double* smem) {
-  using SA = CgA<TA>;
-  using SB = CgB<TB>;
-  constexpr int STAGE = cg_stage_elems<TA, TB>();
+  constexpr int CG_M = CgTile<CFG>::M, CG_N = CgTile<CFG>::N, CG_K = CgTile<CFG>::K;
+  constexpr int WM = CG_M / 2, WN = CG_N / 4, MI = WM / 16, NJ = WN / 8;
+  using SA = CgA<TA, CG_M, CG_K>;
+  using SB = CgB<TB, CG_N, CG_K>;
+  constexpr int STAGE = SA::ELEMS + SB::ELEMS;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
   const int wm = warp & 1, wn = warp >> 1;
   const int tm_n = (M + CG_M - 1) / CG_M, tn_n = (N + CG_N - 1) / CG_N;
@@ -185,25 +206,25 @@ __device__ void cta_gemm(int M, int N, int K, const double* A, long long lda, co
   for (int ct = next_used(0); ct < ntiles; ct = next_used(ct + 1)) {
     const int m0 = (ct % tm_n) * CG_M, n0 = (ct / tm_n) * CG_N;
     const int nch = tile_nch(ct);
-    const bool wskip = lower && (m0 + wm * 32 + 31 < n0 + wn * 32);
+    const bool wskip = lower && (m0 + wm * WM + WM - 1 < n0 + wn * WN);
     // C of this tile into registers now; consumed after the k loop
-    double cv[2][4][4];
+    double cv[MI][NJ][4];
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+    for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-      for (int nj = 0; nj < 4; ++nj)
+      for (int nj = 0; nj < NJ; ++nj)
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-          const int row = m0 + wm * 32 + mi * 16 + g + ((r & 2) ? 8 : 0);
-          const int col = n0 + wn * 32 + nj * 8 + 2 * t4 + (r & 1);
+          const int row = m0 + wm * WM + mi * 16 + g + ((r & 2) ? 8 : 0);
+          const int col = n0 + wn * WN + nj * 8 + 2 * t4 + (r & 1);
           const bool ok = beta != 0.0 && row < M && col < N && !(lower && row < col);
           cv[mi][nj][r] = ok ? C[row + (long long)col * ldc] : 0.0;
         }
-    double acc[2][4][4];
+    double acc[MI][NJ][4];
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+    for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-      for (int nj = 0; nj < 4; ++nj)
+      for (int nj = 0; nj < NJ; ++nj)
 #pragma unroll
         for (int r = 0; r < 4; ++r) acc[mi][nj][r] = 0.0;
     for (int c = 0; c < nch; ++c, ++gch) {
@@ -215,29 +236,29 @@ __device__ void cta_gemm(int M, int N, int K, const double* A, long long lda, co
         const double* sB = sA + SA::ELEMS;
 #pragma unroll
         for (int kk = 0; kk < CG_K; kk += 4) {
-          double a[2][2], b[4];
+          double a[MI][2], b[NJ];
 #pragma unroll
-          for (int mi = 0; mi < 2; ++mi) {
-            a[mi][0] = sA[SA::at(wm * 32 + mi * 16 + g, kk + t4)];
-            a[mi][1] = sA[SA::at(wm * 32 + mi * 16 + g + 8, kk + t4)];
+          for (int mi = 0; mi < MI; ++mi) {
+            a[mi][0] = sA[SA::at(wm * WM + mi * 16 + g, kk + t4)];
+            a[mi][1] = sA[SA::at(wm * WM + mi * 16 + g + 8, kk + t4)];
           }
 #pragma unroll
-          for (int nj = 0; nj < 4; ++nj) b[nj] = sB[SB::at(kk + t4, wn * 32 + nj * 8 + g)];
+          for (int nj = 0; nj < NJ; ++nj) b[nj] = sB[SB::at(kk + t4, wn * WN + nj * 8 + g)];
 #pragma unroll
-          for (int mi = 0; mi < 2; ++mi)
+          for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-            for (int nj = 0; nj < 4; ++nj) dmma_16x8x4(acc[mi][nj], a[mi][0], a[mi][1], b[nj]);
+            for (int nj = 0; nj < NJ; ++nj) dmma_16x8x4(acc[mi][nj], a[mi][0], a[mi][1], b[nj]);
         }
       }
     }
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+    for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-      for (int nj = 0; nj < 4; ++nj)
+      for (int nj = 0; nj < NJ; ++nj)
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-          const int row = m0 + wm * 32 + mi * 16 + g + ((r & 2) ? 8 : 0);
-          const int col = n0 + wn * 32 + nj * 8 + 2 * t4 + (r & 1);
+          const int row = m0 + wm * WM + mi * 16 + g + ((r & 2) ? 8 : 0);
+          const int col = n0 + wn * WN + nj * 8 + 2 * t4 + (r & 1);
           if (row < M && col < N && !(lower && row < col)) {
             double v = alpha * acc[mi][nj][r];
             if (beta != 0.0) v = fma(beta, cv[mi][nj][r], v);
@@ -247,6 +268,19 @@ __device__ void cta_gemm(int M, int N, int K, const double* A, long long lda, co
   }
   cp_async_wait<0>();
   __syncthreads();
+}
+
+// cta_gemm_tile with the tile shape chosen at run time (cfg < CG_CONFIGS)
+template <bool TA, bool TB>
+__device__ __forceinline__ void cta_gemm(int cfg, int M, int N, int K, const double* A, long long lda, const double* B,
+                                         long long ldb, double* C, long long ldc, double alpha, double beta, bool lower,
+                                         int kmode, double* smem) {
+  switch (cfg) {
+    case 1: cta_gemm_tile<TA, TB, 1>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, lower, kmode, smem); break;
+    case 2: cta_gemm_tile<TA, TB, 2>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, lower, kmode, smem); break;
+    case 3: cta_gemm_tile<TA, TB, 3>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, lower, kmode, smem); break;
+    default: cta_gemm_tile<TA, TB, 0>(M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, lower, kmode, smem); break;
+  }
 }
 
 }  // namespace gprx

@@ -294,6 +294,24 @@ gprx_status gprx_batch_fit(gprx_batch* h, const double* params0, uint64_t p, con
 /* The CUDA stream (a cudaStream_t) of the handle, for event timing. */
 gprx_status gprx_batch_stream(gprx_batch* h, void** stream);
 
+/* Schedule of the batched evaluation (no counterpart in the reference).
+ * Problems fall into GPRX_BATCH_SIZE_CLASSES size classes (n ≤ 64, ≤ 128,
+ * …, ≤ 4096, larger); each class runs its in-CTA FP64 GEMMs with one of
+ * GPRX_BATCH_TILE_SHAPES tile shapes (0: 64×128×32, 1: 64×64×32,
+ * 2: 32×64×32, 3: 32×32×16).  The first gprx_batch_eval / gprx_batch_fit
+ * autotunes it: every class present is timed with every shape on a sample of
+ * its problems and the fastest is kept (cached per device and kernel tree
+ * for the life of the process).  Every shape gives the same results bit for
+ * bit.  gprx_batch_autotune re-tunes at the given θ (n_problems × p);
+ * gprx_batch_set_schedule fixes the shapes and turns tuning off;
+ * gprx_batch_schedule reads the shapes, the tuning times (ms per launch,
+ * classes × shapes, nullable) and whether tuning ran. */
+#define GPRX_BATCH_SIZE_CLASSES 8
+#define GPRX_BATCH_TILE_SHAPES 4
+gprx_status gprx_batch_autotune(gprx_batch* h, const double* params, uint64_t p);
+gprx_status gprx_batch_set_schedule(gprx_batch* h, const int32_t* tile_of_class);
+gprx_status gprx_batch_schedule(const gprx_batch* h, int32_t* tile_of_class, float* tune_ms, int32_t* tuned);
+
 /* ------------------------------------------------------------------ */
 /* serving: a request loop over resident exact models on one GPU (no    */
 /* counterpart in the reference; each request is the work of Gpr::fit, */

@@ -206,3 +206,57 @@ def test_batch_fit_matches_single_model_fit():
         nl = m.neg_log_marginal_likelihood()
         assert O.rel_err(res.nlml[i], nl) <= 1e-8, (i, res.nlml[i], nl)
         assert np.all(np.abs(res.params[i] - np.array(m.get_params())) <= 1e-4), (res.params[i], m.get_params())
+
+
+@pytest.mark.parametrize("kind", [RBF_PER, CONST_ARD], ids=["rbf+periodic", "const*ard"])
+def test_batch_every_tile_shape_gives_the_same_bits(kind):
+    # the in-CTA GEMMs sum every output's k terms in the same order whatever
+    # the tile shape, so the schedule changes only the time
+    d, nodes, spec = kind
+    rs = np.random.RandomState(21)
+    sizes = list(SIZES)
+    rs.shuffle(sizes)
+    xs, ys = problems(sizes, d, 13)
+    params = random_params(len(sizes), kind, rs)
+    b = gx.GprBatch(spec(params[0][:-1]), xs, ys, d)
+    out = []
+    for k in range(len(gx.GprBatch.TILE_SHAPES)):
+        b.set_schedule([k] * gx.GprBatch.SIZE_CLASSES)
+        out.append(b.value_and_gradient(params))
+    for nl, g, st in out[1:]:
+        assert np.array_equal(st, out[0][2])
+        assert np.array_equal(nl, out[0][0]) and np.array_equal(g, out[0][1])
+    nl, g, st = out[-1]
+    for i in (0, 5, 11):
+        nl_o, g_o, _, _ = O.exact_eval(nodes, params[i], xs[i], sizes[i], d, ys[i])
+        assert O.rel_err(nl[i], nl_o) <= TOL and np.all(O.rel_err(g[i], g_o) <= TOL)
+
+
+def test_batch_autotune_picks_the_fastest_shape_per_class():
+    d, nodes, spec = RBF_PER
+    rs = np.random.RandomState(22)
+    sizes = [int(v) for v in np.exp(rs.uniform(math.log(20), math.log(1000), size=300))]
+    xs, ys = problems(sizes, d, 14)
+    params = random_params(len(sizes), RBF_PER, rs)
+    b = gx.GprBatch(spec(params[0][:-1]), xs, ys, d)
+    _, _, tuned = b.schedule()
+    assert not tuned
+    t, ms, tuned = b.autotune(params)
+    assert tuned
+    present = {min(max(0, int(math.ceil(math.log2(max(n, 1) / 64.0)))), 7) for n in sizes}
+    for c in range(gx.GprBatch.SIZE_CLASSES):
+        if c in present:
+            assert np.all(ms[c] > 0) and t[c] == int(np.argmin(ms[c])), (c, t[c], ms[c])
+        else:
+            assert np.all(ms[c] == 0)
+    nl, g, st = b.value_and_gradient(params)
+    assert np.all(st == 0)
+    b.set_schedule([0] * gx.GprBatch.SIZE_CLASSES)
+    nl0, g0, _ = b.value_and_gradient(params)
+    assert np.array_equal(nl, nl0) and np.array_equal(g, g0)
+    # a fit under the tuned schedule ends where the fixed one does
+    b2 = gx.GprBatch(spec(params[0][:-1]), xs[:40], ys[:40], d)
+    f1 = b2.fit(params[:40], gx.Lbfgs(max_iterations=15))
+    b2.set_schedule([3] * gx.GprBatch.SIZE_CLASSES)
+    f2 = b2.fit(params[:40], gx.Lbfgs(max_iterations=15))
+    assert np.array_equal(f1.params, f2.params)
