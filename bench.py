@@ -681,7 +681,7 @@ def main():
                              "total": stage[4]}}
     if mixed:
         config["precision"] = ("mixed: factor and inverse by recursive halving, coupling products and K^-1 = X^T X "
-                               "as FP64 products emulated on int8 tensor cores (7 slices); FP64 fill, 2048-row "
+                               "as FP64 products emulated on int8 tensor cores (7 slices); FP64 fill, 4096-row "
                                "leaves, log-det and gradient")
     line = {"metric": metric, "value": head["value"], "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": warm, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",

@@ -5,7 +5,7 @@ In the mixed form the factor and the inverse are computed together by
 recursive halving: the coupling products (L21 = A21 X11ᵀ, A22 −= L21 L21ᵀ,
 X21 = −X22 L21 X11) and K⁻¹ = XᵀX run on the int8 tensor cores as sliced FP64
 emulations (7 int8 digits of 7 bits per row-scaled entry, exact int32 sums);
-blocks of up to 2048 rows use the FP64 blocked factor; the fill, the log-det
+blocks of up to 4096 rows use the FP64 blocked factor; the fill, the log-det
 and the gradient contraction stay FP64.
 Targets: NLML within 1e-8 and gradient within 1e-6 relative to FP64,
 |a − e| / max(|e|, 1).  Sizes from n = 1024 (the smallest n that uses the
@@ -38,7 +38,7 @@ def model(spec, noise, x, n, d, y, precision):
         x, n, d, y)
 
 
-@pytest.mark.parametrize("n", [1024, 1100, 1536, 2100, 4500])
+@pytest.mark.parametrize("n", [1024, 1100, 1536, 2100, 4500, 8300])
 def test_mixed_eval_matches_oracle_ard8(n):
     d = 8
     rs = np.random.RandomState(n)
