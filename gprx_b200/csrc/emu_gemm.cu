@@ -7,8 +7,8 @@
 // groups 512 B apart), so a pipeline stage is filled by 2S bulk copies
 // (cp.async.bulk, completion counted on the stage's "full" mbarrier).
 //
-// Kernel shape: one CTA of 128 threads per 128×64 output tile.  Thread 0
-// issues the bulk copies and the MMAs (tcgen05.mma.cta_group::1.kind::i8,
+// Kernel shape: one CTA of 128 threads per 128×64 output tile.  One thread
+// issues the bulk copies and another the MMAs (tcgen05.mma.cta_group::1.kind::i8,
 // M = 128, K = 32): slice p of A against the stacked B slices q = 0..S-1-p,
 // so term p+q lands in TMEM columns 64(p+q) and one MMA of N = 64(S − p)
 // (split at 256) covers every term of slice p; tcgen05.commit to the stage's
@@ -266,46 +266,55 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_sh;
 
-  if (tid == 0) {
-    // s32 accumulate, signed A and B, K-major both, M = 128 (N set per MMA)
-    const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(EMU_M >> 4) << 24);
+  // warp-specialised issue: lane 0 of warp 1 fills the stages, lane 0 of
+  // warp 0 issues the MMAs as soon as a stage is full, so the tensor pipe
+  // holds the next chunk's MMAs while the current chunk's run
+  if (warp == 1 && lane == 0) {
     const int8_t* Ab = g.A + ((size_t)blockIdx.x * nkc) * 8192;
     const int8_t* Bb = g.B + ((size_t)(blockIdx.y >> 1) * nkc) * 8192 + (blockIdx.y & 1) * 4096;
     const size_t planeA = (size_t)g.ntrA * nkc * 8192, planeB = (size_t)g.ntrB * nkc * 8192;
-    bool ok = true;
-    for (int c = 0; c < nch + STAGES - 1 && ok; ++c) {
-      if (c < nch) {
-        const int st = c % STAGES;
-        if (c >= STAGES) ok = emu_wait(&empty[st], (uint32_t)(((c / STAGES) - 1) & 1), g.err);
-        uint8_t* base = smem + st * STAGE;
-        expect_tx(&full[st], (uint32_t)STAGE);
-        const size_t off = (size_t)(kc0 + c) * 8192;
+    int issued = 0;
+    for (int c = 0; c < nch; ++c) {
+      const int st = c % STAGES;
+      if (c >= STAGES && !emu_wait(&empty[st], (uint32_t)(((c / STAGES) - 1) & 1), g.err)) break;
+      uint8_t* base = smem + st * STAGE;
+      expect_tx(&full[st], (uint32_t)STAGE);
+      const size_t off = (size_t)(kc0 + c) * 8192;
 #pragma unroll
-        for (int p = 0; p < S; ++p) bulk_load(base + p * A_SL, Ab + p * planeA + off, A_SL, &full[st]);
+      for (int p = 0; p < S; ++p) bulk_load(base + p * A_SL, Ab + p * planeA + off, A_SL, &full[st]);
 #pragma unroll
-        for (int q = 0; q < S; ++q) bulk_load(base + S * A_SL + q * B_SL, Bb + q * planeB + off, B_SL, &full[st]);
-      }
-      const int m = c - (STAGES - 1);
-      if (m >= 0 && ok) {
-        const int st = m % STAGES;
-        ok = emu_wait(&full[st], (uint32_t)((m / STAGES) & 1), g.err);
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint8_t* base = smem + st * STAGE;
-        const uint32_t a0 = smem_u32(base), b0 = smem_u32(base + S * A_SL);
-#pragma unroll
-        for (int p = 0; p < S; ++p)
-#pragma unroll
-          for (int q0 = 0; q0 < S - p; q0 += 4) {
-            const int nq = (S - p - q0) < 4 ? (S - p - q0) : 4;
-            const uint32_t id = idesc | ((uint32_t)(nq * EMU_N >> 3) << 17);
-#pragma unroll
-            for (int kk = 0; kk < 2; ++kk)
-              umma_i8(tmem + (p + q0) * EMU_N, emu_desc(a0 + p * A_SL + kk * 256),
-                      emu_desc(b0 + q0 * B_SL + kk * 256), id, (m > 0 || p > 0 || kk > 0) ? 1u : 0u);
-          }
-        umma_commit(&empty[st]);
-      }
+      for (int q = 0; q < S; ++q) bulk_load(base + S * A_SL + q * B_SL, Bb + q * planeB + off, B_SL, &full[st]);
+      issued = c + 1;
     }
+    // no copy still in flight when the CTA leaves (the last phase of each
+    // stage; already complete unless a wait above gave up)
+    for (int j = issued > STAGES ? issued - STAGES : 0; j < issued; ++j)
+      emu_wait(&full[j % STAGES], (uint32_t)((j / STAGES) & 1), g.err);
+  } else if (warp == 0 && lane == 0) {
+    // s32 accumulate, signed A and B, K-major both, M = 128 (N set per MMA)
+    const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(EMU_M >> 4) << 24);
+    bool ok = true;
+    for (int m = 0; m < nch && ok; ++m) {
+      const int st = m % STAGES;
+      ok = emu_wait(&full[st], (uint32_t)((m / STAGES) & 1), g.err);
+      if (!ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint8_t* base = smem + st * STAGE;
+      const uint32_t a0 = smem_u32(base), b0 = smem_u32(base + S * A_SL);
+#pragma unroll
+      for (int p = 0; p < S; ++p)
+#pragma unroll
+        for (int q0 = 0; q0 < S - p; q0 += 4) {
+          const int nq = (S - p - q0) < 4 ? (S - p - q0) : 4;
+          const uint32_t id = idesc | ((uint32_t)(nq * EMU_N >> 3) << 17);
+#pragma unroll
+          for (int kk = 0; kk < 2; ++kk)
+            umma_i8(tmem + (p + q0) * EMU_N, emu_desc(a0 + p * A_SL + kk * 256),
+                    emu_desc(b0 + q0 * B_SL + kk * 256), id, (m > 0 || p > 0 || kk > 0) ? 1u : 0u);
+        }
+      umma_commit(&empty[st]);
+    }
+    // every MMA done before the epilogue reads TMEM
     if (nch > 0 && ok) emu_wait(&empty[(nch - 1) % STAGES], (uint32_t)(((nch - 1) / STAGES) & 1), g.err);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
