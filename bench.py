@@ -160,6 +160,36 @@ def load_traffic():
     return None
 
 
+def emu_kernel_roofline(n, peaks, traffic):
+    """The dominant kernel of the mixed form, emu_gemm_kernel<7>, timed with
+    CUDA events on its own stream (gprx_probe_emu_gemm) at the shape of the
+    evaluation's largest product: the top-level coupling L21 = A21 X11ᵀ,
+    (n/2)³.  Work per launch: 28 int8 slice products of 2·(n/2)³ ops (the
+    FP64-equivalent rate is that ÷ 28).  Peak: twice the measured dense bf16
+    rate (B200's int8 dense rate is twice its bf16 rate), else twice the
+    fallback 1.59 PFLOP/s."""
+    from gprx_b200 import _lib as L
+
+    h = n // 2
+    out = np.zeros(4)
+    st = L.lib().gprx_probe_emu_gemm(h, h, h, 7, 10, L.ptr(out))
+    if st != 0 or out[0] <= 0:
+        return None
+    eq = 2.0 * h ** 3 / (out[0] * 1e-3) / 1e12
+    achieved = 28 * eq
+    bf16 = peaks.get("bf16_tflops")
+    peak = 2.0 * bf16 if bf16 else 2.0 * 1590.0
+    src = ("2 x measured dense bf16 burst (MEASURED_PEAKS.json bf16_tflops, of measured)" if bf16
+           else "2 x the fallback dense bf16 1.59 PFLOP/s (of fallback)")
+    return {"bound": "tensor", "kernel": "emu_gemm_kernel<7> (tcgen05.mma kind::i8, TMEM accumulators)",
+            "shape": "%d^3, 7 slices (the top-level coupling product at n = %d)" % (h, n),
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s (int8 tensor ops)", "frac": achieved / peak,
+            "peak_source": src, "ms_per_launch": out[0], "fp64_equivalent_tflops": eq,
+            "work": "28 int8 slice products x 2 (n/2)^3 ops per launch",
+            "traffic": traffic.get("emu_gemm_bytes_per_launch") if traffic else None,
+            "max_rel_err_vs_dmma": out[3]}
+
+
 def cpu_reference(n, d, x, y, thetas, steps, warmup, budget_s=6.0):
     """Times the oracle (a CPU restatement of the reference's algorithm)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -554,6 +584,16 @@ def main():
     torch.cuda.set_device(dev)
 
     if args.workload == "sgpr":
+        if args.profile_evals > 0:
+            x, yv, z, ls = sgpr_synth()
+            prec = gx.Precision.Fp64 if args.precision == "fp64" else gx.Precision.Mixed
+            mdl = gx.Sgpr(gx.RbfArdKernel(list(ls)), gx.GaussianLikelihood(0.1), precision=prec).with_optimizer(
+                gx.Fixed()).factor(x, 1_000_000, 4, yv, z, 1024)
+            theta = np.array(list(np.log(ls)) + [math.log(0.1)])
+            for _ in range(args.profile_evals):
+                mdl.value_and_gradient(theta)
+            torch.cuda.synchronize()
+            return
         out = sgpr_measure(torch, dev, args.steps, warm)
         out.update({"n_gpus": 1, "warmup": warm, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                     "dtype": "f64", "data": "synthetic"})
@@ -670,15 +710,24 @@ def main():
     achieved = (n ** 3) / (dmma_ms * 1e-3) / 1e12
     traffic = load_traffic()
     mixed = "mixed" in res
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp64_peak if fp64_peak else None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 has no entry in MEASURED_PEAKS.json)",
-                "kernel": ("emu_gemm_kernel<7> (int8 tcgen05, FP64-emulated) + dgemm_kernel (DMMA f64)" if mixed
-                           else "dgemm_kernel (DMMA m16n8k4 f64) inside potrf/trtri/lauum"),
-                "work": "n^3 FP64(-equivalent) flops per evaluation (potrf n^3/3 + trtri n^3/3 + lauum n^3/3)",
-                "traffic": traffic.get("bytes_per_eval") if traffic else None,
-                "stage_ms": {"fill": stage[0], "factor": stage[1], "inverse": stage[2], "gradient": stage[3],
-                             "total": stage[4]}}
+    stage_roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                      "frac": achieved / fp64_peak if fp64_peak else None,
+                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (of measured; FP64 has no entry "
+                                     "in MEASURED_PEAKS.json)",
+                      "kernel": ("factor + inverse stages: emu_gemm_kernel<7> + dgemm_kernel + potrf_diag_kernel"
+                                 if mixed else "dgemm_kernel (DMMA m16n8k4 f64) inside potrf/trtri/lauum"),
+                      "work": "n^3 FP64(-equivalent) flops per evaluation (potrf n^3/3 + trtri n^3/3 + lauum "
+                              "n^3/3) over the factor + inverse stage time",
+                      "stage_ms": {"fill": stage[0], "factor": stage[1], "inverse": stage[2], "gradient": stage[3],
+                                   "total": stage[4]}}
+    roofline = dict(stage_roofline)
+    if mixed and rank == 0:
+        k = emu_kernel_roofline(n, peaks, traffic)
+        if k is not None:
+            roofline = k
+            roofline["stage"] = stage_roofline
+    else:
+        roofline["traffic"] = traffic.get("dgemm_bytes_per_eval") if traffic else None
     if mixed:
         config["precision"] = ("mixed: factor and inverse by recursive halving, coupling products and K^-1 = X^T X "
                                "as FP64 products emulated on int8 tensor cores (7 slices); FP64 fill, 4096-row "
