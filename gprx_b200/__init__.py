@@ -18,6 +18,7 @@ from .api import (  # noqa: F401
     Fixed,
     FittedGpr,
     FittedSgpr,
+    sharded_value_and_gradient,
     GaussianLikelihood,
     Gpr,
     GprBatch,

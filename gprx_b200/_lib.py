@@ -145,6 +145,10 @@ _SIGS = {
     "gprx_batch_fit": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.POINTER(LbfgsOptions), D, C.POINTER(FitReport),
                                    I32]),
     "gprx_batch_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "gprx_sgpr_shard_sizes": (C.c_int32, [C.c_void_p, U64, U64]),
+    "gprx_sgpr_shard_assemble": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_void_p]),
+    "gprx_sgpr_shard_nlml": (C.c_int32, [C.c_void_p, C.c_void_p, D, C.c_void_p]),
+    "gprx_sgpr_shard_gradient": (C.c_int32, [C.c_void_p, C.c_void_p, D]),
     "gprx_batch_autotune": (C.c_int32, [C.c_void_p, D, C.c_uint64]),
     "gprx_batch_set_schedule": (C.c_int32, [C.c_void_p, I32]),
     "gprx_batch_schedule": (C.c_int32, [C.c_void_p, I32, C.POINTER(C.c_float), I32]),

@@ -666,11 +666,74 @@ class FittedSgpr:
         check(L.lib().gprx_sgpr_stage_times(self._h, L.ptr(out)))
         return dict(zip(("kmm_and_a", "b_and_sums", "gradient"), out))
 
+    # -- one shard of an evaluation over n split across processes ---------
+    # The model holds this process's points and the shared inducing inputs;
+    # the two exchange buffers are float64 tensors on the model's device that
+    # the caller sums over the processes between the calls
+    # (sharded_value_and_gradient does the sequence).
+
+    def shard_sizes(self):
+        """Lengths (doubles) of the two exchange buffers."""
+        a = np.zeros(1, dtype=np.uint64)
+        b = np.zeros(1, dtype=np.uint64)
+        check(L.lib().gprx_sgpr_shard_sizes(self._h, a.ctypes.data_as(L.U64), b.ctypes.data_as(L.U64)))
+        return int(a[0]), int(b[0])
+
+    def shard_assemble(self, params, exchange1):
+        """This shard's sums over n at θ = params, written to exchange1."""
+        p = L.f64(params)
+        check(L.lib().gprx_sgpr_shard_assemble(self._h, L.ptr(p), p.size, C.c_void_p(exchange1.data_ptr())))
+
+    def shard_nlml(self, exchange1, exchange2=None):
+        """NLML from the summed exchange1; with exchange2, this shard's
+        gradient sums are written there."""
+        v = np.zeros(1)
+        e2 = C.c_void_p(exchange2.data_ptr()) if exchange2 is not None else None
+        check(L.lib().gprx_sgpr_shard_nlml(self._h, C.c_void_p(exchange1.data_ptr()), L.ptr(v), e2))
+        return float(v[0])
+
+    def shard_gradient(self, exchange2):
+        """Gradient from the summed exchange2."""
+        g = np.zeros(self.num_params())
+        check(L.lib().gprx_sgpr_shard_gradient(self._h, C.c_void_p(exchange2.data_ptr()), L.ptr(g)))
+        return g
+
     def into_online(self):
         """FittedSgpr::into_online: the same device state, now updatable."""
         on = OnlineSgpr(self._h, self.d)
         self._h = None
         return on
+
+
+def sharded_value_and_gradient(shard, params, all_reduce, device=None, gradient=True):
+    """VFE NLML (and gradient) over n split across processes.
+
+    shard: this process's FittedSgpr (its points, the shared inducing
+    inputs); all_reduce(t): sums the tensor t over the processes in place
+    (e.g. torch.distributed.all_reduce over NCCL).  Every process returns
+    the same values, equal to the unsharded evaluation's.  The exchange
+    buffers are float64 tensors on `device` (the CUDA device of the model;
+    the work of each call has finished when it returns, and the all-reduce
+    is waited for before the next call reads its result)."""
+    import torch
+
+    n1, n2 = shard.shard_sizes()
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    ex1 = torch.empty(n1, dtype=torch.float64, device=dev)
+    ex2 = torch.empty(n2, dtype=torch.float64, device=dev) if gradient else None
+
+    def reduce(t):
+        all_reduce(t)
+        if t.is_cuda:
+            torch.cuda.current_stream(t.device).synchronize()
+
+    shard.shard_assemble(params, ex1)
+    reduce(ex1)
+    nl = shard.shard_nlml(ex1, ex2)
+    if not gradient:
+        return nl, None
+    reduce(ex2)
+    return nl, shard.shard_gradient(ex2)
 
 
 class OnlineSgpr(FittedSgpr):

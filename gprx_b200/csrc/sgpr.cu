@@ -334,6 +334,23 @@ struct SgprState {
   gprx_status insert(const double* xnew, double ynew, uint64_t* id);
   gprx_status remove(uint64_t id);
   gprx_status set_inducing(const double* zh, uint64_t mm);
+  // one shard of a VFE evaluation over n split across processes (the sums
+  // over n travel in two exchange buffers that the caller sums over shards)
+  gprx_status factor_kmm_and_a(EmuWork& ew, bool& emu);
+  gprx_status shard_assemble(const double* params, double* e1);
+  gprx_status shard_nlml(const double* e1, double* nlml_out, double* e2);
+  gprx_status shard_gradient(const double* e2, double* grad);
+  uint64_t shard_e1() const { return (uint64_t)m * m + m + 3; }
+  uint64_t shard_e2() const { return (uint64_t)m * m + kern.n_params + 1; }
+  double n_total = 0.0, shard_y2 = 0.0;  // Σ n and Σ y² over the shards of the last shard evaluation
+  bool shard_ready = false;
+  // the device state is a sharded evaluation's global posterior: predictions
+  // use it; the NLML and online steps of this handle reassemble its own points
+  bool sharded = false;
+  void drop_shard_state() {
+    if (sharded) assembled = false;
+    sharded = false;
+  }
   void get_params(double* out) const {
     for (int i = 0; i < kern.n_params; ++i) out[i] = kern.theta[i];
     out[kern.n_params] = log_noise;
@@ -391,10 +408,10 @@ gprx_status SgprState::create(const double* xh, uint64_t nn, uint64_t dd, const 
   int nblk = ceil_div(m, NB);
   if (z.alloc((size_t)m * d) || Lmm.alloc((size_t)ldm * m) || linv_mm.alloc((size_t)nblk * NB * NB) ||
       Bl.alloc((size_t)ldm * m) || linv_B.alloc((size_t)nblk * NB * NB) || w.alloc(ldm) || ay.alloc(ldm) ||
-      vtmp.alloc(ldm) || partials.alloc((size_t)grad_max_blocks() * 2 * 64 + 4096) || res.alloc(64) ||
+      vtmp.alloc(ldm) || partials.alloc((size_t)grad_max_blocks() * 2 * 64 + 4096) || res.alloc(128) ||
       slot_param.alloc(64) || status.alloc(1))
     return set_error(GPRX_OUT_OF_MEMORY, "device allocation failed");
-  GPRX_CUDA_TRY(res_h.ensure(64));
+  GPRX_CUDA_TRY(res_h.ensure(128));
   GPRX_CUDA_TRY(status_h.ensure(1));
   if ((st = ensure_points(n)) != GPRX_OK) return st;
   GPRX_CUDA_TRY(cudaMemcpy2DAsync(x.p, sizeof(double) * cap, xh, sizeof(double) * n, sizeof(double) * n, d,
@@ -620,6 +637,7 @@ gprx_status SgprState::assemble() {
   afro = res_h.p[1];
   kdiag_sum = (double)n * kern.diag_value();
   assembled = true;
+  sharded = false;
   st = solve_w();
   GPRX_CUDA_TRY(cudaEventRecord(ev[2], stream));
   return st;
@@ -634,6 +652,7 @@ gprx_status SgprState::solve_w() {
 
 gprx_status SgprState::nlml(double* out) {
   gprx_status st;
+  drop_shard_state();
   if (!assembled && (st = assemble()) != GPRX_OK) return st;
   if ((st = reset_status()) != GPRX_OK) return st;
   GPRX_CUDA_TRY(logdet_diag(Bl.p, ldm, m, false, res.p + 0, status.p, stream));
@@ -708,7 +727,7 @@ gprx_status SgprState::gradient(double* grad) {
   count_launch(2);
   GPRX_CUDA_TRY(dot_dev(w.p, w.p, m, res.p + 3, status.p, stream));
   GPRX_CUDA_TRY(dot_dev(ay.p, w.p, m, res.p + 4, status.p, stream));
-  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p, sizeof(double) * 60, cudaMemcpyDeviceToHost, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p, sizeof(double) * 128, cudaMemcpyDeviceToHost, stream));
   if (emu) GPRX_CUDA_TRY(cudaMemcpyAsync(emu_err_h.p, emu_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
   if ((st = sync_check(GPRX_STAGE_FIT)) != GPRX_OK) return st;
   if (emu && *emu_err_h.p) return set_error(GPRX_TIMEOUT, "an emulated product's bounded wait ran out");
@@ -798,6 +817,7 @@ gprx_status SgprState::insert(const double* xnew, double ynew, uint64_t* id) {
   if (!xnew || !id) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (!all_finite(xnew, d) || !std::isfinite(ynew)) return set_error(GPRX_NONFINITE_INPUT, "non-finite point");
   gprx_status st;
+  drop_shard_state();
   if (!assembled && (st = assemble()) != GPRX_OK) return st;
   if ((st = ensure_points(n + 1)) != GPRX_OK) return st;
   const long long slot = n;
@@ -842,6 +862,7 @@ gprx_status SgprState::remove(uint64_t id) {
   if (it == ids.end() || *it != id) return set_error(GPRX_INVALID_POINT_ID, "unknown point id");
   const long long idx = it - ids.begin();
   gprx_status st;
+  drop_shard_state();
   if (!assembled && (st = assemble()) != GPRX_OK) return st;
   const long long slot = order[idx], last = n - 1;
   const double ydel = y_host[slot];
@@ -922,6 +943,218 @@ gprx_status SgprState::set_inducing(const double* zh, uint64_t mm) {
   return assemble();
 }
 
+// ---------------------------------------------------------------------------
+// sharded evaluation (one shard = the points this handle holds; Z, K_mm and
+// L are replicated).  Exchange buffer 1 (m² + m + 3): B_s = A_s A_sᵀ (lower,
+// ld m, upper zero), A_s y_s, ‖A_s‖²_F, Σ y_s², n_s.  Exchange buffer 2
+// (m² + p): H_s = G_s A_sᵀ (ld m) and the θ-gradient of the cross term
+// ⟨L⁻ᵀ G_s, ∂K(Z, X_s)⟩.  Both are sums over n, so their sum over the shards
+// is the unsharded value (assemble_vfe, src/sgpr/factor/vfe.rs:191-277;
+// analytic_gradient, src/sgpr/factor/derivatives.rs:283-366).
+// ---------------------------------------------------------------------------
+gprx_status SgprState::factor_kmm_and_a(EmuWork& ew, bool& emu) {
+  const int nn = (int)n;
+  std::vector<double> js{0.0};
+  auto r = retry_list_sparse(opt);
+  js.insert(js.end(), r.begin(), r.end());
+  bool ok = false;
+  gprx_status st;
+  for (double j : js) {
+    if ((st = reset_status()) != GPRX_OK) return st;
+    GPRX_CUDA_TRY(fill_lower(kern, z.p, m, m, Lmm.p, ldm, j, status.p, stream));
+    GPRX_CUDA_TRY(potrf_blocked(Lmm.p, ldm, m, linv_mm.p, status.p, stream, &fctx));
+    DevStatus ds;
+    if ((st = read_status(&ds)) != GPRX_OK) return st;
+    if (ds.code == GPRX_OK) {
+      ok = true;
+      kmm_jitter = j;
+      break;
+    }
+    if (ds.code != GPRX_CHOLESKY_FAILED) return status_to_error(ds, j, m, GPRX_STAGE_FIT);
+  }
+  if (!ok) return set_cholesky_error(js.back(), m, GPRX_STAGE_FIT);
+  pivot_ratio_kernel<<<1, 1024, 0, stream>>>(Lmm.p, ldm, m, res.p + 10);
+  count_launch();
+  GPRX_CUDA_TRY(fill_cross(kern, z.p, m, m, x.p, cap, nn, Amat.p, ldm, status.p, stream));
+  emu = use_emu();
+  if (emu) {
+    if ((st = ensure_emu(ew)) != GPRX_OK) return st;
+    GPRX_CUDA_TRY(cudaMemsetAsync(emu_err.p, 0, sizeof(int), stream));
+  }
+  GPRX_CUDA_TRY(trsm_lower_rec(Lmm.p, ldm, m, linv_mm.p, Amat.p, ldm, nn, TRSM_LEAF, status.p, stream));
+  return GPRX_OK;
+}
+
+gprx_status SgprState::shard_assemble(const double* params, double* e1) {
+  if (!params || !e1) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (n > INT32_MAX) return set_error(GPRX_CAPACITY, "n too large for one assembly");
+  shard_ready = false;
+  gprx_status st = write_params(params);
+  if (st != GPRX_OK) return st;
+  const int nn = (int)n;
+  EmuWork ew;
+  bool emu = false;
+  if ((st = factor_kmm_and_a(ew, emu)) != GPRX_OK) return st;
+  const long long mm2 = (long long)m * m;
+  GPRX_CUDA_TRY(cudaMemsetAsync(e1, 0, sizeof(double) * mm2, stream));
+  if (emu) {
+    GPRX_CUDA_TRY(emu_gram(Amat.p, Amat.p, ldm, m, nn, true, e1, m, ew, emu_part.p, ldm, EMU_GROUP, EMU_PART_K,
+                           stream));
+  } else {
+    GPRX_CUDA_TRY(syrk_splitk(Amat.p, ldm, m, nn, Amat.p, ldm, true, 0.0, splitbuf, e1, m, status.p, stream));
+  }
+  int blocks = grid_for((long long)m * nn, 1024);
+  sumsq_kernel<<<blocks, 256, 0, stream>>>(Amat.p, ldm, m, nn, partials.p, status.p);
+  sum_partials_kernel<<<1, 1024, 0, stream>>>(partials.p, blocks, e1 + mm2 + m, status.p);
+  count_launch(2);
+  {
+    int S = (int)std::min<long long>(32, std::max<long long>(1, nn / 4096));
+    if (splitbuf.ensure((size_t)S * ldm) != cudaSuccess) return set_error(GPRX_OUT_OF_MEMORY, "split buffer");
+    GemmParams pp = gemm_params(m, 1, nn, Amat.p, ldm, y.p, nn, splitbuf.p, ldm, 1.0, 0.0, status.p);
+    pp.mode = GEMM_SPLIT_K;
+    pp.splits = S;
+    pp.split_stride = ldm;
+    GPRX_CUDA_TRY(dgemm(false, false, pp, stream));
+    split_reduce_kernel<<<grid_for(m, 256), 256, 0, stream>>>(splitbuf.p, S, ldm, m, 0, 0.0, false, e1 + mm2,
+                                                                status.p);
+    count_launch();
+  }
+  res_h.p[20] = y2;
+  res_h.p[21] = (double)n;
+  GPRX_CUDA_TRY(cudaMemcpyAsync(e1 + mm2 + m + 1, res_h.p + 20, sizeof(double) * 2, cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p + 10, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  if (emu) GPRX_CUDA_TRY(cudaMemcpyAsync(emu_err_h.p, emu_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  if ((st = sync_check(GPRX_STAGE_FIT)) != GPRX_OK) return st;
+  if (emu && *emu_err_h.p) return set_error(GPRX_TIMEOUT, "an emulated product's bounded wait ran out");
+  pivot_ratio = res_h.p[0];
+  assembled = false;  // the handle's B is not this shard's alone
+  sharded = false;
+  return GPRX_OK;
+}
+
+gprx_status SgprState::shard_nlml(const double* e1, double* nlml_out, double* e2) {
+  if (!e1 || !nlml_out) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  gprx_status st;
+  if ((st = reset_status()) != GPRX_OK) return st;
+  const long long mm2 = (long long)m * m;
+  const double noise_v = noise();
+  // B = Σ_s B_s + σ² I, L_B; Ay = Σ_s A_s y_s; the sums over n
+  GPRX_CUDA_TRY(cudaMemcpy2DAsync(Bl.p, sizeof(double) * ldm, e1, sizeof(double) * m, sizeof(double) * m, m,
+                                  cudaMemcpyDeviceToDevice, stream));
+  add_diag_kernel<<<ceil_div(m, 256), 256, 0, stream>>>(Bl.p, ldm, m, noise_v);
+  count_launch();
+  GPRX_CUDA_TRY(potrf_blocked(Bl.p, ldm, m, linv_B.p, status.p, stream, &fctx));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(ay.p, e1 + mm2, sizeof(double) * m, cudaMemcpyDeviceToDevice, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p + 20, e1 + mm2 + m, sizeof(double) * 3, cudaMemcpyDeviceToHost, stream));
+  if ((st = solve_w()) != GPRX_OK) return st;  // synchronises the stream
+  afro = res_h.p[20];
+  const double y2_total = res_h.p[21];
+  n_total = res_h.p[22];
+  kdiag_sum = n_total * kern.diag_value();
+  GPRX_CUDA_TRY(logdet_diag(Bl.p, ldm, m, false, res.p + 0, status.p, stream));
+  GPRX_CUDA_TRY(dot_dev(ay.p, w.p, m, res.p + 1, status.p, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+  if ((st = sync_check(GPRX_STAGE_FIT)) != GPRX_OK) return st;
+  shard_y2 = y2_total;
+  const double logdet = (n_total - (double)m) * std::log(noise_v) + res_h.p[0];
+  const double quad = (y2_total - res_h.p[1]) / noise_v;
+  const double trace = (kdiag_sum - afro) / (2.0 * noise_v);
+  *nlml_out = 0.5 * (n_total * std::log(2.0 * M_PI) + logdet + quad) + trace;
+  shard_ready = true;
+  assembled = true;  // L, L_B and w are the global posterior's
+  sharded = true;
+  if (!e2) return GPRX_OK;
+  // this shard's part of the gradient: G_s = B⁻¹A_s − (w r_sᵀ + A_s)/σ²,
+  // H_s = G_s A_sᵀ, and the cross term with L⁻ᵀ G_s
+  const int nn = (int)n;
+  if (G.ensure((size_t)ldm * std::max(cap, 1LL)) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "gradient buffers");
+  const bool emu = use_emu();
+  EmuWork ew;
+  if (emu) {
+    if ((st = ensure_emu(ew)) != GPRX_OK) return st;
+    GPRX_CUDA_TRY(cudaMemsetAsync(emu_err.p, 0, sizeof(int), stream));
+  }
+  GPRX_CUDA_TRY(cudaMemcpyAsync(G.p, Amat.p, sizeof(double) * ldm * nn, cudaMemcpyDeviceToDevice, stream));
+  GPRX_CUDA_TRY(trsm_lower_rec(Bl.p, ldm, m, linv_B.p, G.p, ldm, nn, TRSM_LEAF, status.p, stream));
+  GPRX_CUDA_TRY(trsm_lower_t_rec(Bl.p, ldm, m, linv_B.p, G.p, ldm, nn, TRSM_LEAF, status.p, stream));
+  adjoint_update_kernel<<<grid_for((long long)nn * 32, 256), 256, 0, stream>>>(Amat.p, G.p, ldm, m, nn, w.p, y.p,
+                                                                                1.0 / noise_v, status.p);
+  count_launch();
+  if (emu) {
+    GPRX_CUDA_TRY(emu_gram(G.p, Amat.p, ldm, m, nn, false, e2, m, ew, emu_part.p, ldm, EMU_GROUP, EMU_PART_K,
+                           stream));
+  } else {
+    GPRX_CUDA_TRY(syrk_splitk(G.p, ldm, m, nn, Amat.p, ldm, false, 0.0, splitbuf, e2, m, status.p, stream));
+  }
+  GPRX_CUDA_TRY(trsm_lower_t_rec(Lmm.p, ldm, m, linv_mm.p, G.p, ldm, nn, TRSM_LEAF, status.p, stream));
+  int b2 = 0;
+  GPRX_CUDA_TRY(cross_contract(kern, z.p, m, m, x.p, cap, nn, G.p, ldm, partials.p, &b2, status.p, stream));
+  GPRX_CUDA_TRY(grad_finalize(kern, partials.p, b2, slot_param.p, 1.0, 0.0, e2 + mm2, status.p, stream));
+  if (emu) GPRX_CUDA_TRY(cudaMemcpyAsync(emu_err_h.p, emu_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  if ((st = sync_check(GPRX_STAGE_FIT)) != GPRX_OK) return st;
+  if (emu && *emu_err_h.p) return set_error(GPRX_TIMEOUT, "an emulated product's bounded wait ran out");
+  return GPRX_OK;
+}
+
+gprx_status SgprState::shard_gradient(const double* e2, double* grad) {
+  if (!e2 || !grad) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (!shard_ready) return set_error(GPRX_INVALID_CONFIG, "shard gradient before the shard NLML");
+  gprx_status st;
+  if (H.ensure((size_t)ldm * m) != cudaSuccess || Wm.ensure((size_t)ldm * m) != cudaSuccess ||
+      Xb.ensure((size_t)ldm * m) != cudaSuccess || Xt.ensure((size_t)ldm * m) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "gradient buffers");
+  if ((st = reset_status()) != GPRX_OK) return st;
+  const long long mm2 = (long long)m * m;
+  const double noise_v = noise();
+  const int nk = kern.n_params;
+  // w_mm = −sym(L⁻ᵀ tril½(H) L⁻¹) from H = Σ_s H_s
+  GPRX_CUDA_TRY(cudaMemcpy2DAsync(H.p, sizeof(double) * ldm, e2, sizeof(double) * m, sizeof(double) * m, m,
+                                  cudaMemcpyDeviceToDevice, stream));
+  tril_half_kernel<<<grid_for((long long)m * m, 256), 256, 0, stream>>>(H.p, ldm, m, Xb.p);
+  count_launch();
+  GPRX_CUDA_TRY(trsm_lower_t(Lmm.p, ldm, m, linv_mm.p, Xb.p, ldm, m, status.p, stream));
+  {
+    dim3 tb(32, 8), tg(ceil_div(m, 32), ceil_div(m, 32));
+    transpose_kernel<<<tg, tb, 0, stream>>>(Xb.p, ldm, m, Xt.p);
+    count_launch();
+  }
+  GPRX_CUDA_TRY(trsm_lower_t(Lmm.p, ldm, m, linv_mm.p, Xt.p, ldm, m, status.p, stream));
+  neg_sym_half_kernel<<<grid_for((long long)m * m, 256), 256, 0, stream>>>(Xt.p, ldm, m, Wm.p);
+  count_launch();
+  int b1 = 0;
+  GPRX_CUDA_TRY(grad_contract(kern, z.p, m, m, Wm.p, ldm, nullptr, partials.p, &b1, status.p, stream));
+  GPRX_CUDA_TRY(grad_finalize(kern, partials.p, b1, slot_param.p, 1.0, 0.0, res.p + 20, status.p, stream));
+  // the cross term after the K_mm term's nk + 1 values (nk ≤ 8 leaves ≤ 46 fits in 128)
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res.p + 21 + nk, e2 + mm2, sizeof(double) * nk, cudaMemcpyDeviceToDevice, stream));
+  // tr(B⁻¹) = ‖L_B⁻¹‖²_F, ‖w‖², (Ay)ᵀw
+  GPRX_CUDA_TRY(cudaMemsetAsync(Xt.p, 0, sizeof(double) * ldm * m, stream));
+  if (H.ensure((size_t)((m + 1) / 2) * ((m + 1) / 2) + 1) != cudaSuccess) return set_error(GPRX_OUT_OF_MEMORY, "scratch");
+  GPRX_CUDA_TRY(trtri_blocked(Bl.p, ldm, m, linv_B.p, Xt.p, ldm, H.p, status.p, stream));
+  int blocks = grid_for((long long)m * m, 1024);
+  sumsq_kernel<<<blocks, 256, 0, stream>>>(Xt.p, ldm, m, m, partials.p + 8192, status.p);
+  sum_partials_kernel<<<1, 1024, 0, stream>>>(partials.p + 8192, blocks, res.p + 2, status.p);
+  count_launch(2);
+  GPRX_CUDA_TRY(dot_dev(w.p, w.p, m, res.p + 3, status.p, stream));
+  GPRX_CUDA_TRY(dot_dev(ay.p, w.p, m, res.p + 4, status.p, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p, sizeof(double) * 128, cudaMemcpyDeviceToHost, stream));
+  if ((st = sync_check(GPRX_STAGE_FIT)) != GPRX_OK) return st;
+  std::vector<double> dg;
+  diag_grad(kern, dg);
+  const double wdiag = 0.5 / noise_v;
+  for (int i = 0; i < nk; ++i) grad[i] = res_h.p[20 + i] + res_h.p[21 + nk + i] + wdiag * n_total * dg[i];
+  const double trb = res_h.p[2], ww = res_h.p[3], ayw = res_h.p[4];
+  const double quad = (shard_y2 - ayw) / noise_v;
+  const double trace = (kdiag_sum - afro) / (2.0 * noise_v);
+  const double dn = noise_v;
+  const double d_logdet_b = dn * trb;
+  const double d_q = -dn * ww;
+  const double d_quad = -d_q / noise_v - quad * dn / noise_v;
+  const double d_trace = -trace * dn / noise_v;
+  grad[nk] = 0.5 * ((n_total - (double)m) * dn / noise_v + d_logdet_b + d_quad) + d_trace;
+  return GPRX_OK;
+}
+
 static gprx_status sgpr_eval_cb(void* ctx, const double* lt, double* f, double* g) {
   return ((SgprState*)ctx)->eval(lt, f, g);
 }
@@ -985,6 +1218,30 @@ gprx_status gprx_sgpr_nlml(gprx_sgpr* h, double* nlml) {
   CHECK_SGPR(h);
   if (!nlml) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   return h->s.nlml(nlml);
+}
+
+gprx_status gprx_sgpr_shard_sizes(const gprx_sgpr* h, uint64_t* exchange1, uint64_t* exchange2) {
+  CHECK_SGPR(h);
+  if (!exchange1 || !exchange2) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  *exchange1 = h->s.shard_e1();
+  *exchange2 = h->s.shard_e2();
+  return GPRX_OK;
+}
+
+gprx_status gprx_sgpr_shard_assemble(gprx_sgpr* h, const double* params, uint64_t p, double* exchange1) {
+  CHECK_SGPR(h);
+  if (p != (uint64_t)h->s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
+  return h->s.shard_assemble(params, exchange1);
+}
+
+gprx_status gprx_sgpr_shard_nlml(gprx_sgpr* h, const double* exchange1, double* nlml, double* exchange2) {
+  CHECK_SGPR(h);
+  return h->s.shard_nlml(exchange1, nlml, exchange2);
+}
+
+gprx_status gprx_sgpr_shard_gradient(gprx_sgpr* h, const double* exchange2, double* grad) {
+  CHECK_SGPR(h);
+  return h->s.shard_gradient(exchange2, grad);
 }
 
 gprx_status gprx_sgpr_predict(gprx_sgpr* h, const double* xs, uint64_t q, int32_t kind, double* mean, double* var) {

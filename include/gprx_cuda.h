@@ -250,6 +250,27 @@ gprx_status gprx_sgpr_point_ids(gprx_sgpr* h, uint64_t* out, uint64_t n);
  * delete (OnlineSgpr::insert_inducing / delete_inducing, src/sgpr/online/mod.rs:1301,1943)
  * taken by reassembly. */
 gprx_status gprx_sgpr_set_inducing(gprx_sgpr* h, const double* z, uint64_t m);
+
+/* Sharded VFE evaluation: n split over processes (one GPU each), each
+ * process holding a handle created with ITS points and the SAME inducing
+ * inputs Z; K_mm and its factor are replicated.  The sums over n that the
+ * assembly and the gradient need (assemble_vfe, src/sgpr/factor/vfe.rs:191-277;
+ * analytic_gradient, src/sgpr/factor/derivatives.rs:283-366) travel in two
+ * device exchange buffers owned by the caller (doubles, sizes from
+ * gprx_sgpr_shard_sizes), which the caller sums over the processes (an
+ * all-reduce) between the calls:
+ *   gprx_sgpr_shard_assemble(h, θ, exchange1)   -> this shard's sums
+ *   all-reduce(exchange1)
+ *   gprx_sgpr_shard_nlml(h, exchange1, &nlml, exchange2 or NULL)
+ *   all-reduce(exchange2)
+ *   gprx_sgpr_shard_gradient(h, exchange2, grad)
+ * Every process gets the same NLML and gradient, equal to the unsharded
+ * evaluation's; afterwards the handle predicts with the global posterior.
+ * Each call returns after its work has finished on the handle's stream. */
+gprx_status gprx_sgpr_shard_sizes(const gprx_sgpr* h, uint64_t* exchange1, uint64_t* exchange2);
+gprx_status gprx_sgpr_shard_assemble(gprx_sgpr* h, const double* params, uint64_t p, double* exchange1);
+gprx_status gprx_sgpr_shard_nlml(gprx_sgpr* h, const double* exchange1, double* nlml, double* exchange2);
+gprx_status gprx_sgpr_shard_gradient(gprx_sgpr* h, const double* exchange2, double* grad);
 /* jitter j the K_mm factor took. */
 gprx_status gprx_sgpr_kmm_jitter(gprx_sgpr* h, double* jitter);
 /* The CUDA stream (a cudaStream_t) of the handle, for event timing. */
