@@ -29,6 +29,8 @@ from .api import (  # noqa: F401
     InvalidHyperparameter,
     KernelSpec,
     Lbfgs,
+    NonPositiveDefiniteMatrix,
+    PredictiveCovariance,
     NonFiniteInput,
     NonFiniteKernelValue,
     OnlineGpr,

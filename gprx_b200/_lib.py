@@ -34,6 +34,7 @@ INVALID_CONFIG = 12
 NOT_CONVERGED = 13
 INVALID_ARGUMENT = 14
 CAPACITY = 16
+NOT_POSITIVE_DEFINITE = 17
 
 # kernel node kinds
 NODE_SUM, NODE_PRODUCT = 1, 2
@@ -145,6 +146,9 @@ _SIGS = {
     "gprx_batch_fit": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.POINTER(LbfgsOptions), D, C.POINTER(FitReport),
                                    I32]),
     "gprx_batch_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "gprx_exact_loo": (C.c_int32, [C.c_void_p, C.c_int32, D, D]),
+    "gprx_exact_predict_covariance": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
+    "gprx_exact_sample": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, C.c_uint64, C.c_uint64, D]),
     "gprx_sgpr_shard_sizes": (C.c_int32, [C.c_void_p, U64, U64]),
     "gprx_sgpr_shard_assemble": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_void_p]),
     "gprx_sgpr_shard_nlml": (C.c_int32, [C.c_void_p, C.c_void_p, D, C.c_void_p]),

@@ -91,6 +91,10 @@ class DeviceTimeout(GprError):
     pass
 
 
+class NonPositiveDefiniteMatrix(GprError):
+    """GprError::NonPositiveDefiniteMatrix (a leave-one-out [K⁻¹]_ii ≤ 0)."""
+
+
 class OutOfDeviceMemory(GprError):
     pass
 
@@ -111,6 +115,7 @@ _ERRORS = {
     L.NOT_CONVERGED: OptimizationNotConverged,
     L.INVALID_ARGUMENT: ShapeMismatch,
     L.CAPACITY: InvalidConfig,
+    L.NOT_POSITIVE_DEFINITE: NonPositiveDefiniteMatrix,
 }
 
 
@@ -322,6 +327,15 @@ class Prediction:
         self.variance_kind = variance_kind
 
 
+class PredictiveCovariance:
+    """Predictive mean and the q×q query covariance (src/prediction.rs:172)."""
+
+    def __init__(self, mean, covariance, variance_kind):
+        self.mean = mean
+        self.covariance = covariance  # q×q ndarray (symmetric)
+        self.variance_kind = variance_kind
+
+
 class Precision(enum.IntEnum):
     Fp64 = L.PRECISION_FP64
     Mixed = L.PRECISION_MIXED
@@ -493,6 +507,50 @@ class FittedGpr:
         check(L.lib().gprx_exact_predict(self._h, L.ptr(xs), n_rows, int(options.variance_kind), L.ptr(mean),
                                          L.ptr(var)))
         return Prediction(mean, var, options.variance_kind)
+
+    def _query(self, xs, n_rows, n_cols):
+        if n_cols != self.d:
+            raise ShapeMismatch("query has %d features, model has %d" % (n_cols, self.d))
+        xs = L.f64(xs)
+        if xs.size != n_rows * n_cols:
+            raise ShapeMismatch("xs has %d values, expected %d×%d" % (xs.size, n_rows, n_cols))
+        return xs
+
+    def loo_predict(self):
+        """Leave-one-out mean and variance at every training point
+        (FittedGpr::loo_predict, src/gpr/fitted.rs:697)."""
+        return self.loo_predict_with(PredictOptions())
+
+    def loo_predict_with(self, options):
+        n = self.n()
+        mean = np.zeros(n)
+        var = np.zeros(n)
+        check(L.lib().gprx_exact_loo(self._h, int(options.variance_kind), L.ptr(mean), L.ptr(var)))
+        return Prediction(mean, var, options.variance_kind)
+
+    def predict_covariance(self, xs, n_rows, n_cols):
+        """Mean and query covariance K** − VᵀV (src/gpr/fitted.rs:971)."""
+        return self.predict_covariance_with(xs, n_rows, n_cols, PredictOptions())
+
+    def predict_covariance_with(self, xs, n_rows, n_cols, options):
+        xs = self._query(xs, n_rows, n_cols)
+        mean = np.zeros(n_rows)
+        cov = np.zeros(n_rows * n_rows)
+        check(L.lib().gprx_exact_predict_covariance(self._h, L.ptr(xs), n_rows, int(options.variance_kind),
+                                                    L.ptr(mean), L.ptr(cov)))
+        return PredictiveCovariance(mean, cov.reshape(n_rows, n_rows, order="F"), options.variance_kind)
+
+    def sample(self, xs, n_rows, n_cols, n_draws, seed):
+        """n_draws posterior draws, column-major n_rows × n_draws
+        (src/gpr/fitted.rs:1038)."""
+        return self.sample_with(xs, n_rows, n_cols, PredictOptions(), n_draws, seed)
+
+    def sample_with(self, xs, n_rows, n_cols, options, n_draws, seed):
+        xs = self._query(xs, n_rows, n_cols)
+        out = np.zeros(n_rows * n_draws)
+        check(L.lib().gprx_exact_sample(self._h, L.ptr(xs), n_rows, int(options.variance_kind), int(n_draws),
+                                        int(seed), L.ptr(out)))
+        return out
 
     def stream_ptr(self):
         """The cudaStream_t this model's kernels run on (for event timing)."""

@@ -309,6 +309,23 @@ gprx_status gprx_exact_predict(gprx_exact* h, const double* xs, uint64_t q, int3
   return h->s.predict(xs, q, kind, mean, var);
 }
 
+gprx_status gprx_exact_loo(gprx_exact* h, int32_t kind, double* mean, double* var) {
+  CHECK_HANDLE(h);
+  return h->s.loo(kind, mean, var);
+}
+
+gprx_status gprx_exact_predict_covariance(gprx_exact* h, const double* xs, uint64_t q, int32_t kind, double* mean,
+                                          double* cov) {
+  CHECK_HANDLE(h);
+  return h->s.predict_covariance(xs, q, kind, mean, cov);
+}
+
+gprx_status gprx_exact_sample(gprx_exact* h, const double* xs, uint64_t q, int32_t kind, uint64_t n_draws,
+                              uint64_t seed, double* out) {
+  CHECK_HANDLE(h);
+  return h->s.sample(xs, q, kind, n_draws, seed, out);
+}
+
 gprx_status gprx_exact_alpha(gprx_exact* h, double* out, uint64_t n) {
   CHECK_HANDLE(h);
   ExactState& s = h->s;

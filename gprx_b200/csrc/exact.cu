@@ -334,6 +334,220 @@ __global__ void extract_diag_kernel(const double* A, long long ld, int n, double
   if (i < n) out[i] = A[i + (long long)i * ld];
 }
 
+// ---------------------------------------------------------------------------
+// leave-one-out, query covariance and posterior draws
+// ---------------------------------------------------------------------------
+static unsigned blocks_for(long long count) { return (unsigned)((count + 255) / 256); }
+
+// The resident factor of the current θ: L (LLT) with α, or the online LDLT
+// with α solved and the unit diagonal-block inverses in linv.
+gprx_status ExactState::ready_for_query() {
+  gprx_status st;
+  if (online) {
+    if (!alpha_ok && (st = online_alpha()) != GPRX_OK) return st;
+    if (!linv_ok) {
+      if ((st = reset_status()) != GPRX_OK) return st;
+      GPRX_CUDA_TRY(tri_inv_blocks(A.p, ld, n, true, linv.p, status.p, stream));
+      linv_ok = true;
+    }
+    GPRX_CUDA_TRY(cudaMemsetAsync(status.p, 0, sizeof(DevStatus), stream));
+    extract_diag_kernel<<<ceil_div(n, 256), 256, 0, stream>>>(A.p, ld, n, tmpv.p);
+    count_launch();
+  } else if (!factor_ok || !alpha_ok) {
+    if ((st = factor_current()) != GPRX_OK) return st;
+  }
+  return GPRX_OK;
+}
+
+// mean_i = y_i − α_i / Q_ii, variance from 1 / Q_ii (src/gpr/shared.rs:538-555)
+__global__ void loo_kernel(const double* y, const double* alpha, const double* qd, int n, double noise, int kind,
+                           double* out, DevStatus* st) {
+  if (dev_failed(st)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double q = qd[i];
+  if (!(q > 0.0) || !isfinite(q)) {
+    dev_fail(st, GPRX_NOT_POSITIVE_DEFINITE, i);
+    return;
+  }
+  out[i] = y[i] - alpha[i] / q;
+  const double obs = 1.0 / q;
+  out[n + i] = kind == GPRX_VARIANCE_OBSERVATION ? obs : fmax(obs - noise, 0.0);
+}
+
+gprx_status ExactState::loo(int kind, double* mean, double* var) {
+  if (!mean || !var) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (kind != GPRX_VARIANCE_LATENT && kind != GPRX_VARIANCE_OBSERVATION)
+    return set_error(GPRX_INVALID_ARGUMENT, "variance kind");
+  gprx_status st;
+  if ((st = ready_for_query()) != GPRX_OK) return st;
+  const size_t nn = (size_t)ld * cap;
+  if (Xinv.n < nn) {
+    size_t half = (size_t)((n + 1) / 2) * ((n + 1) / 2);
+    if (Xinv.alloc(nn) != cudaSuccess || scratch.alloc(std::max<size_t>(half, 1)) != cudaSuccess) {
+      Xinv.reset();
+      return set_error(GPRX_OUT_OF_MEMORY, "device allocation of the inverse failed");
+    }
+    GPRX_CUDA_TRY(cudaMemsetAsync(Xinv.p, 0, sizeof(double) * nn, stream));
+  } else if (scratch.n < (size_t)((n + 1) / 2) * ((n + 1) / 2)) {
+    if (scratch.alloc((size_t)((n + 1) / 2) * ((n + 1) / 2)) != cudaSuccess)
+      return set_error(GPRX_OUT_OF_MEMORY, "scratch");
+  }
+  if (qx.ensure((size_t)3 * n) != cudaSuccess) return set_error(GPRX_OUT_OF_MEMORY, "scratch");
+  // Q_ii = Σ_k (L⁻¹)_ki² / w_k (w = 1 for LLT, D for the online LDLT)
+  GPRX_CUDA_TRY(trtri_blocked(A.p, ld, n, linv.p, Xinv.p, ld, scratch.p, status.p, stream));
+  GPRX_CUDA_TRY(col_sumsq(Xinv.p, ld, n, n, online ? tmpv.p : nullptr, qx.p, status.p, stream));
+  GPRX_LAUNCH(loo_kernel, ceil_div(n, 256), 256, 0, stream, y.p, alpha.p, qx.p, n, noise(), kind, qx.p + n,
+              status.p);
+  std::vector<double> h(2 * (size_t)n);
+  GPRX_CUDA_TRY(cudaMemcpyAsync(h.data(), qx.p + n, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, stream));
+  DevStatus ds;
+  if ((st = read_status(&ds)) != GPRX_OK) return st;
+  if (ds.code == GPRX_NOT_POSITIVE_DEFINITE)
+    return set_error(GPRX_NOT_POSITIVE_DEFINITE, "leave-one-out: [K⁻¹]_ii ≤ 0 at row " + std::to_string(ds.info));
+  if (ds.code != GPRX_OK) return status_to_error(ds, jitter, n, GPRX_STAGE_PREDICT);
+  std::copy(h.begin(), h.begin() + n, mean);
+  std::copy(h.begin() + n, h.end(), var);
+  return GPRX_OK;
+}
+
+// V := V ⊘ √w (row i scaled by 1 / √w_i)
+__global__ void scale_rows_kernel(double* V, long long ld, int n, int q, const double* w) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)n * q) return;
+  const int i = (int)(e % n), c = (int)(e / n);
+  V[i + c * ld] /= sqrt(w[i]);
+}
+
+// C (q×q, lower computed) → full symmetric; diagonal clipped at 0 (latent)
+// or plus σn² (observation)
+__global__ void cov_finish_kernel(double* C, int q, double noise, int kind) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)q * q) return;
+  const int i = (int)(e % q), j = (int)(e / q);
+  if (i < j) {
+    C[i + (long long)j * q] = C[j + (long long)i * q];
+  } else if (i == j) {
+    double v = C[i + (long long)i * q];
+    if (v < 0.0) v = 0.0;
+    C[i + (long long)i * q] = kind == GPRX_VARIANCE_OBSERVATION ? v + noise : v;
+  }
+}
+
+// covbuf (q×q, ld q) = predictive covariance; mean to the host
+gprx_status ExactState::covariance_dev(const double* xs, uint64_t q, int kind, double* mean_host) {
+  if (kind != GPRX_VARIANCE_LATENT && kind != GPRX_VARIANCE_OBSERVATION)
+    return set_error(GPRX_INVALID_ARGUMENT, "variance kind");
+  if (q > (uint64_t)INT32_MAX) return set_error(GPRX_CAPACITY, "too many query points");
+  if (!all_finite(xs, q * d)) return set_error(GPRX_NONFINITE_INPUT, "non-finite query");
+  gprx_status st;
+  if ((st = ready_for_query()) != GPRX_OK) return st;
+  const int qi = (int)q;
+  if (qbuf.ensure((size_t)ld * q) != cudaSuccess || qx.ensure((size_t)q * (d + 1)) != cudaSuccess ||
+      covbuf.ensure((size_t)q * q) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "covariance buffers");
+  double* xq = qx.p;  // q × d
+  double* mdev = qx.p + (size_t)q * d;
+  GPRX_CUDA_TRY(cudaMemcpyAsync(xq, xs, sizeof(double) * q * d, cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(fill_cross(kern, x.p, cap, n, xq, qi, qi, qbuf.p, ld, status.p, stream));
+  GPRX_CUDA_TRY(gemv_t(qbuf.p, ld, n, qi, false, alpha.p, mdev, status.p, stream));
+  GPRX_CUDA_TRY(trsm_lower(A.p, ld, n, linv.p, qbuf.p, ld, qi, status.p, stream));
+  if (online) GPRX_LAUNCH(scale_rows_kernel, blocks_for((long long)n * qi), 256, 0, stream, qbuf.p, ld, n, qi, tmpv.p);
+  // K** (lower), then K** − VᵀV on the lower tiles
+  GPRX_CUDA_TRY(fill_lower(kern, xq, qi, qi, covbuf.p, qi, 0.0, status.p, stream));
+  GemmParams p = gemm_params(qi, qi, n, qbuf.p, ld, qbuf.p, ld, covbuf.p, qi, -1.0, 1.0, status.p);
+  p.mode = GEMM_LOWER_TILES;
+  GPRX_CUDA_TRY(dgemm(true, false, p, stream));
+  GPRX_LAUNCH(cov_finish_kernel, blocks_for((long long)qi * qi), 256, 0, stream, covbuf.p, qi, noise(), kind);
+  GPRX_CUDA_TRY(cudaMemcpyAsync(mean_host, mdev, sizeof(double) * q, cudaMemcpyDeviceToHost, stream));
+  DevStatus ds;
+  if ((st = read_status(&ds)) != GPRX_OK) return st;
+  if (ds.code != GPRX_OK) return status_to_error(ds, jitter, n, GPRX_STAGE_PREDICT);
+  return GPRX_OK;
+}
+
+gprx_status ExactState::predict_covariance(const double* xs, uint64_t q, int kind, double* mean, double* cov) {
+  if (!xs || !mean || !cov) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (q == 0) return GPRX_OK;
+  gprx_status st = covariance_dev(xs, q, kind, mean);
+  if (st != GPRX_OK) return st;
+  GPRX_CUDA_TRY(cudaMemcpyAsync(cov, covbuf.p, sizeof(double) * q * q, cudaMemcpyDeviceToHost, stream));
+  GPRX_CUDA_TRY(cudaStreamSynchronize(stream));
+  return GPRX_OK;
+}
+
+// out(:, k) = μ + L z_k (L lower, its upper part zeroed first)
+__global__ void zero_upper_kernel(double* L, int q) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)q * q) return;
+  const int i = (int)(e % q), j = (int)(e / q);
+  if (i < j) L[i + (long long)j * q] = 0.0;
+}
+__global__ void add_mean_kernel(double* out, const double* mean, int q, long long count) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e < count) out[e] += mean[e % q];
+}
+__global__ void add_diag_q_kernel(double* C, int q, double v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < q) C[i + (long long)i * q] += v;
+}
+
+gprx_status ExactState::sample(const double* xs, uint64_t q, int kind, uint64_t n_draws, uint64_t seed,
+                               double* out) {
+  if (!xs || (n_draws > 0 && !out)) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (q == 0) return GPRX_OK;
+  if (n_draws > (uint64_t)INT32_MAX) return set_error(GPRX_CAPACITY, "too many draws");
+  std::vector<double> mean(q);
+  gprx_status st = covariance_dev(xs, q, kind, mean.data());
+  if (st != GPRX_OK || n_draws == 0) return st;
+  const int qi = (int)q, nd = (int)n_draws;
+  const size_t nblk = (size_t)ceil_div(qi, NB);
+  if (covl.ensure((size_t)q * q) != cudaSuccess || covlinv.ensure(nblk * NB * NB) != cudaSuccess ||
+      zbuf.ensure((size_t)q * n_draws * 2 + q) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "draw buffers");
+  // LLT of the covariance with the model's jitter retries (src/linalg/chol.rs:20-43,83-103)
+  std::vector<double> js{0.0};
+  auto r = retry_list(opt);
+  js.insert(js.end(), r.begin(), r.end());
+  bool ok = false;
+  double last = 0.0;
+  for (double j : js) {
+    last = j;
+    if ((st = reset_status()) != GPRX_OK) return st;
+    GPRX_CUDA_TRY(cudaMemcpyAsync(covl.p, covbuf.p, sizeof(double) * q * q, cudaMemcpyDeviceToDevice, stream));
+    if (j != 0.0) GPRX_LAUNCH(add_diag_q_kernel, ceil_div(qi, 256), 256, 0, stream, covl.p, qi, j);
+    GPRX_CUDA_TRY(potrf_blocked(covl.p, qi, qi, covlinv.p, status.p, stream, nullptr));
+    DevStatus ds;
+    if ((st = read_status(&ds)) != GPRX_OK) return st;
+    if (ds.code == GPRX_OK) {
+      ok = true;
+      break;
+    }
+    if (ds.code != GPRX_CHOLESKY_FAILED) return status_to_error(ds, j, q, GPRX_STAGE_PREDICT);
+  }
+  if (!ok) return set_cholesky_error(last, q, GPRX_STAGE_PREDICT);
+  // z: q unit normals per draw from the seeded generator (src/rng.rs:83-87)
+  std::vector<double> z((size_t)q * n_draws);
+  gprx_rng rng;
+  gprx_rng_seed(&rng, seed);
+  gprx_rng_fill_normal(&rng, z.data(), z.size());
+  double* zd = zbuf.p;
+  double* od = zbuf.p + (size_t)q * n_draws;
+  double* md = od + (size_t)q * n_draws;
+  GPRX_CUDA_TRY(cudaMemcpyAsync(zd, z.data(), sizeof(double) * z.size(), cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(md, mean.data(), sizeof(double) * q, cudaMemcpyHostToDevice, stream));
+  GPRX_LAUNCH(zero_upper_kernel, blocks_for((long long)qi * qi), 256, 0, stream, covl.p, qi);
+  GemmParams p = gemm_params(qi, nd, qi, covl.p, qi, zd, qi, od, qi, 1.0, 0.0, status.p);
+  p.mode = GEMM_K_TO_ROW;
+  GPRX_CUDA_TRY(dgemm(false, false, p, stream));
+  GPRX_LAUNCH(add_mean_kernel, blocks_for((long long)qi * nd), 256, 0, stream, od, md, qi, (long long)qi * nd);
+  GPRX_CUDA_TRY(cudaMemcpyAsync(out, od, sizeof(double) * q * n_draws, cudaMemcpyDeviceToHost, stream));
+  DevStatus ds;
+  if ((st = read_status(&ds)) != GPRX_OK) return st;
+  if (ds.code != GPRX_OK) return status_to_error(ds, jitter, q, GPRX_STAGE_PREDICT);
+  return GPRX_OK;
+}
+
 gprx_status ExactState::predict(const double* xs, uint64_t q, int kind, double* mean, double* var) {
   if (!xs || !mean || !var) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (kind != GPRX_VARIANCE_LATENT && kind != GPRX_VARIANCE_OBSERVATION)

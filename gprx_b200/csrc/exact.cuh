@@ -87,6 +87,13 @@ struct ExactState {
   gprx_status eval(const double* params, double* nlml, double* grad);
   gprx_status nlml(double* out);
   gprx_status predict(const double* xs, uint64_t q, int kind, double* mean, double* var);
+  // leave-one-out, query covariance and posterior draws from the resident factor
+  DevBuf<double> covbuf, covl, covlinv, zbuf;
+  gprx_status ready_for_query();
+  gprx_status loo(int kind, double* mean, double* var);
+  gprx_status covariance_dev(const double* xs, uint64_t q, int kind, double* mean_host);
+  gprx_status predict_covariance(const double* xs, uint64_t q, int kind, double* mean, double* cov);
+  gprx_status sample(const double* xs, uint64_t q, int kind, uint64_t n_draws, uint64_t seed, double* out);
   gprx_status reset_status();
   gprx_status read_status(DevStatus* out);
   gprx_status stage_times(double* out5);

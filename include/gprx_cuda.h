@@ -51,7 +51,8 @@ enum {
   GPRX_NOT_CONVERGED = 13,         /* OptimizationNotConverged{iterations} */
   GPRX_INVALID_ARGUMENT = 14,      /* null handle / null pointer / bad enum */
   GPRX_STALE_FACTOR = 15,          /* internal: the factor was consumed by a gradient */
-  GPRX_CAPACITY = 16               /* a fixed-size buffer was too small for the request */
+  GPRX_CAPACITY = 16,              /* a fixed-size buffer was too small for the request */
+  GPRX_NOT_POSITIVE_DEFINITE = 17  /* GprError::NonPositiveDefiniteMatrix (a leave-one-out [K⁻¹]_ii ≤ 0) */
 };
 
 /* CholeskyStage (src/error.rs:31-39) */
@@ -185,6 +186,29 @@ gprx_status gprx_exact_factor_jitter(gprx_exact* h, double* jitter);
  * (GprCore::write_moments, src/gpr/shared.rs:754-820). */
 gprx_status gprx_exact_predict(gprx_exact* h, const double* xs, uint64_t q, int32_t variance_kind,
                                double* mean, double* var);
+
+/* Leave-one-out mean and variance at every training point (GPML §5.4.2):
+ * mean_i = y_i − α_i / Q_ii, observation variance 1 / Q_ii, latent
+ * max(0, 1 / Q_ii − σn²), Q = (K + σn² I)⁻¹ (FittedGpr::loo_predict_with,
+ * src/gpr/fitted.rs:712; GprCore::loo_predict_with, src/gpr/shared.rs:522-567;
+ * OnlineGpr::loo_predict_with, src/gpr/online.rs:716).  mean, var: n values
+ * in training (index) order.  Q_ii ≤ 0 → GPRX_NOT_POSITIVE_DEFINITE. */
+gprx_status gprx_exact_loo(gprx_exact* h, int32_t variance_kind, double* mean, double* var);
+/* Predictive mean and the q×q query covariance K** − VᵀV, V = L⁻¹K(X, X*)
+ * (D-weighted for an online LDLT model); latent diagonal clipped at 0,
+ * observation adds σn² on the diagonal (FittedGpr::predict_covariance_with,
+ * src/gpr/fitted.rs:992; GprCore::write_covariance, src/gpr/shared.rs:425-520).
+ * cov: column-major q×q. */
+gprx_status gprx_exact_predict_covariance(gprx_exact* h, const double* xs, uint64_t q, int32_t variance_kind,
+                                          double* mean, double* cov);
+/* n_draws posterior draws at the queries, column-major q × n_draws: column k
+ * is μ + L z_k with L the Cholesky factor of the predictive covariance
+ * (retried with the model's jitter policy, stage PREDICT) and z_k the next q
+ * unit normals of the seeded generator at `seed` (FittedGpr::sample_with,
+ * src/gpr/fitted.rs:1056; PredictiveCovariance::draw, src/prediction.rs:206-243).
+ * Zero draws form the covariance and write nothing. */
+gprx_status gprx_exact_sample(gprx_exact* h, const double* xs, uint64_t q, int32_t variance_kind, uint64_t n_draws,
+                              uint64_t seed, double* out);
 /* α = A⁻¹ y of the current factor (n values). */
 gprx_status gprx_exact_alpha(gprx_exact* h, double* out, uint64_t n);
 /* Gpr::fit with the default Lbfgs (src/gpr/trainer.rs:533-613, src/optimizer/lbfgs.rs:126-172):

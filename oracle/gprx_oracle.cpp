@@ -636,6 +636,137 @@ int orc_exact_predict(const int32_t* nodes, int n_nodes, const double* params, i
   return 0;
 }
 
+// Leave-one-out at every training point (GprCore::loo_predict_with,
+// src/gpr/shared.rs:522-567; GPML §5.4.2): Q = (K + σn² I)⁻¹,
+// mean_i = y_i − α_i / Q_ii, observation variance 1 / Q_ii, latent
+// max(0, 1 / Q_ii − σn²).  Returns 17 when a Q_ii is not positive.
+int orc_exact_loo(const int32_t* nodes, int n_nodes, const double* params, int n_params, const double* x, int64_t n,
+                  int d, const double* y, int jitter_kind, double jitter_initial, double jitter_mult,
+                  int jitter_retries, double jitter_max, int kind, double* mean, double* var) {
+  Tree t;
+  int nk = n_params - 1;
+  if (!build_tree(t, nodes, n_nodes, params, nk)) return 3;
+  double noise = std::exp(params[nk]);
+  Factor f;
+  double last_j = 0.0;
+  int st = factor_exact(t, x, n, d, y, noise,
+                        retry_jitters(jitter_kind, jitter_initial, jitter_mult, jitter_retries, jitter_max),
+                        f, &last_j);
+  if (st != 0) return st;
+  Mat kinv((size_t)n * n, 0.0);
+  llt_inverse(f.l.data(), n, n, kinv.data(), n);
+  for (int64_t i = 0; i < n; ++i) {
+    double q = AT(kinv, n, i, i);
+    if (!(q > 0.0) || !std::isfinite(q)) return 17;
+    mean[i] = y[i] - f.alpha[i] / q;
+    double obs = 1.0 / q;
+    var[i] = kind == 1 ? obs : std::max(obs - noise, 0.0);
+  }
+  return 0;
+}
+
+// Mean and the q×q query covariance K** − VᵀV, V = L⁻¹K* (GprCore::write_covariance,
+// src/gpr/shared.rs:425-520): latent diagonal clipped at 0, observation adds σn².
+static int exact_covariance(const Tree& t, double noise, const Factor& f, const double* x, int64_t n, int d,
+                            const double* xs, int64_t q, int kind, double* mean, double* cov) {
+  Mat ks((size_t)n * q);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < q; ++c)
+    for (int64_t i = 0; i < n; ++i) AT(ks, n, i, c) = kval(t, x + i, n, xs + c, q, d);
+  for (int64_t c = 0; c < q; ++c) {
+    double m = 0.0;
+    for (int64_t i = 0; i < n; ++i) m += AT(ks, n, i, c) * f.alpha[i];
+    mean[c] = m;
+  }
+  trsm_lower(f.l.data(), n, n, ks.data(), q, n);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < q; ++c)
+    for (int64_t r = 0; r < q; ++r) {
+      double dot = 0.0;
+      for (int64_t k = 0; k < n; ++k) dot += AT(ks, n, k, r) * AT(ks, n, k, c);
+      cov[r + c * q] = kval(t, xs + r, q, xs + c, q, d) - dot;
+    }
+  for (int64_t i = 0; i < q; ++i) {
+    double v = cov[i + i * q];
+    if (v < 0.0) v = 0.0;
+    cov[i + i * q] = kind == 1 ? v + noise : v;
+  }
+  return 0;
+}
+
+int orc_exact_covariance(const int32_t* nodes, int n_nodes, const double* params, int n_params, const double* x,
+                         int64_t n, int d, const double* y, int jitter_kind, double jitter_initial,
+                         double jitter_mult, int jitter_retries, double jitter_max, const double* xs, int64_t q,
+                         int kind, double* mean, double* cov) {
+  Tree t;
+  int nk = n_params - 1;
+  if (!build_tree(t, nodes, n_nodes, params, nk)) return 3;
+  double noise = std::exp(params[nk]);
+  Factor f;
+  double last_j = 0.0;
+  int st = factor_exact(t, x, n, d, y, noise,
+                        retry_jitters(jitter_kind, jitter_initial, jitter_mult, jitter_retries, jitter_max),
+                        f, &last_j);
+  if (st != 0) return st;
+  return exact_covariance(t, noise, f, x, n, d, xs, q, kind, mean, cov);
+}
+
+// Posterior draws (PredictiveCovariance::draw, src/prediction.rs:206-243):
+// LLT of the covariance retried with the jitter list (src/linalg/chol.rs:20-43),
+// then column k = μ + L z_k, z_k the next q unit normals (src/rng.rs:72-87),
+// L z summed column by column as mul_lower_vec (src/linalg/dense.rs:409-422).
+int orc_exact_sample(const int32_t* nodes, int n_nodes, const double* params, int n_params, const double* x,
+                     int64_t n, int d, const double* y, int jitter_kind, double jitter_initial, double jitter_mult,
+                     int jitter_retries, double jitter_max, const double* xs, int64_t q, int kind, int64_t n_draws,
+                     uint64_t seed, double* out) {
+  Tree t;
+  int nk = n_params - 1;
+  if (!build_tree(t, nodes, n_nodes, params, nk)) return 3;
+  double noise = std::exp(params[nk]);
+  auto jl = retry_jitters(jitter_kind, jitter_initial, jitter_mult, jitter_retries, jitter_max);
+  Factor f;
+  double last_j = 0.0;
+  int st = factor_exact(t, x, n, d, y, noise, jl, f, &last_j);
+  if (st != 0) return st;
+  std::vector<double> mean(q), cov((size_t)q * q);
+  exact_covariance(t, noise, f, x, n, d, xs, q, kind, mean.data(), cov.data());
+  if (n_draws == 0) return 0;
+  std::vector<double> js{0.0};
+  js.insert(js.end(), jl.begin(), jl.end());
+  Mat l((size_t)q * q);
+  bool ok = false;
+  for (double j : js) {
+    l.assign(cov.begin(), cov.end());
+    for (int64_t i = 0; i < q; ++i) AT(l, q, i, i) += j;
+    if (potrf(l.data(), q, q)) {
+      ok = true;
+      break;
+    }
+  }
+  if (!ok) return 1;
+  Rng r;
+  rng_seed(r, seed);
+  auto unit = [&]() { return (double)(rng_next(r) >> 11) * (1.0 / 9007199254740992.0); };
+  auto open_unit = [&]() {
+    double u = unit();
+    const double eps = 1.0 / 9007199254740992.0;
+    return u <= eps ? eps : (u >= 1.0 - eps ? 1.0 - eps : u);
+  };
+  std::vector<double> z(q), lz(q);
+  for (int64_t k = 0; k < n_draws; ++k) {
+    for (int64_t i = 0; i < q; ++i) {
+      double u1 = std::max(open_unit(), 2.2250738585072014e-308);
+      double u2 = open_unit();
+      z[i] = std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2);
+    }
+    std::fill(lz.begin(), lz.end(), 0.0);
+    for (int64_t j = 0; j < q; ++j)
+      for (int64_t i = j; i < q; ++i) lz[i] += AT(l, q, i, j) * z[j];
+    for (int64_t i = 0; i < q; ++i) out[k * q + i] = mean[i] + lz[i];
+  }
+  return 0;
+}
+
 // ---------------------------------------------------------------------------
 // Online exact GPR: LDLT store (src/gpr/factor_store.rs:100-260, src/linalg/ldlt.rs)
 // ---------------------------------------------------------------------------

@@ -37,6 +37,12 @@ def lib():
                                  C.c_double, C.c_int, C.c_double, D, D, D, D]
     L.orc_exact_predict.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D, C.c_int, C.c_double,
                                     C.c_double, C.c_int, C.c_double, D, C.c_int64, C.c_int, D, D]
+    L.orc_exact_loo.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D, C.c_int, C.c_double,
+                                C.c_double, C.c_int, C.c_double, C.c_int, D, D]
+    L.orc_exact_covariance.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D, C.c_int, C.c_double,
+                                       C.c_double, C.c_int, C.c_double, D, C.c_int64, C.c_int, D, D]
+    L.orc_exact_sample.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D, C.c_int, C.c_double,
+                                   C.c_double, C.c_int, C.c_double, D, C.c_int64, C.c_int, C.c_int64, C.c_uint64, D]
     L.orc_gram_lower.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D]
     L.orc_cross.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, D, C.c_int64, C.c_int, D]
     L.orc_potrf.argtypes = [D, C.c_int64]
@@ -111,6 +117,44 @@ def exact_eval(nodes, params, x, n, d, y, grad=True, jitter=FIXED):
     if st != 0:
         raise OracleError(st)
     return nl[0], g, a, ju[0]
+
+
+def exact_loo(nodes, params, x, n, d, y, kind, jitter=FIXED):
+    L = lib()
+    nd = _nodes(nodes)
+    p = _f(params)
+    mean = np.zeros(n)
+    var = np.zeros(n)
+    st = L.orc_exact_loo(_ptr(nd, I32), len(nd) // 2, _ptr(p), len(p), _ptr(_f(x)), n, d, _ptr(_f(y)), *jitter,
+                         kind, _ptr(mean), _ptr(var))
+    if st != 0:
+        raise OracleError(st)
+    return mean, var
+
+
+def exact_covariance(nodes, params, x, n, d, y, xs, q, kind, jitter=FIXED):
+    L = lib()
+    nd = _nodes(nodes)
+    p = _f(params)
+    mean = np.zeros(q)
+    cov = np.zeros(q * q)
+    st = L.orc_exact_covariance(_ptr(nd, I32), len(nd) // 2, _ptr(p), len(p), _ptr(_f(x)), n, d, _ptr(_f(y)),
+                                *jitter, _ptr(_f(xs)), q, kind, _ptr(mean), _ptr(cov))
+    if st != 0:
+        raise OracleError(st)
+    return mean, cov.reshape(q, q, order="F")
+
+
+def exact_sample(nodes, params, x, n, d, y, xs, q, kind, n_draws, seed, jitter=FIXED):
+    L = lib()
+    nd = _nodes(nodes)
+    p = _f(params)
+    out = np.zeros(q * n_draws)
+    st = L.orc_exact_sample(_ptr(nd, I32), len(nd) // 2, _ptr(p), len(p), _ptr(_f(x)), n, d, _ptr(_f(y)),
+                            *jitter, _ptr(_f(xs)), q, kind, n_draws, seed, _ptr(out))
+    if st != 0:
+        raise OracleError(st)
+    return out
 
 
 def exact_predict(nodes, params, x, n, d, y, xs, q, kind, jitter=FIXED):
