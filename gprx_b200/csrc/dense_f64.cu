@@ -25,6 +25,17 @@ cudaError_t dgemm(bool ta, bool tb, const GemmParams& p, cudaStream_t s, int bat
   return launch_dgemm<128, 128, 16, 64, 32, 3, true, true>(p, batch, s);
 }
 
+cudaError_t dgemm_nn_fill(const GemmParams& p, cudaStream_t s, int batch) {
+  const long long tiles128 = (long long)ceil_div(p.M, 128) * ceil_div(p.N, 128) * batch;
+  if (tiles128 >= 2 * 148) return launch_dgemm<128, 128, 16, 64, 32, 3, false, false>(p, batch, s);
+  return launch_dgemm<64, 64, 16, 32, 16, 3, false, false>(p, batch, s);
+}
+
+cudaError_t dgemm_nt_small(const GemmParams& p, cudaStream_t s, int tile) {
+  if (tile == 1) return launch_dgemm<64, 128, 16, 32, 32, 3, false, true>(p, 1, s);
+  return launch_dgemm<64, 64, 16, 32, 16, 3, false, true>(p, 1, s);
+}
+
 GemmParams gemm_params(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
                        double* C, long long ldc, double alpha, double beta, const DevStatus* st) {
   GemmParams p{};
@@ -185,9 +196,10 @@ static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double
   int rest = n - k0 - nbk;
   if (rest > 0) {
     double* P = A + (k0 + nbk) + (long long)k0 * ld;
-    // panel: P := P · L_kk⁻ᵀ (in place; the 128-wide tile covers all nbk columns)
+    // panel: P := P · L_kk⁻ᵀ (in place; a 64×128 tile covers all nbk columns
+    // of its rows, and twice the CTAs of 128×128 tiles shorten the chain)
     GemmParams pp = gemm_params(rest, nbk, nbk, P, ld, lk, NB, P, ld, 1.0, 0.0, st);
-    CK(dgemm(false, true, pp, s));
+    CK(dgemm_nt_small(pp, s, 1));
   }
   return cudaGetLastError();
 }
@@ -233,7 +245,7 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
       int m = n - c1, w = min(NB, n - c1);
       GemmParams pc = gemm_params(m, w, NB, Pk, ld, Pk, ld, A + c1 + (long long)c1 * ld, ld, -1.0, 1.0, st);
       pc.mode = GEMM_LOWER_TILES;
-      CK(dgemm(false, true, pc, X));
+      CK(dgemm_nt_small(pc, X, 2));  // 64×64 tiles: four times the CTAs on the chain
     }
     CK(diag_and_panel(A, ld, n, c1, linv, st, X));
     CK(cudaEventRecord(Ep[k + 1], X));
@@ -328,7 +340,7 @@ cudaError_t trtri_blocked(const double* L, long long ld, int n, const double* li
       p1.strideA = b + b * ld;
       p1.strideB = b + b * ldx;
       p1.strideC = h2 * h;
-      CK(dgemm(false, false, p1, s, (int)cnt));
+      CK(dgemm_nn_fill(p1, s, (int)cnt));
       // X21 = −X22 · T   (h2 × h, K = h2; X22 lower → k up to the row)
       GemmParams p2 = gemm_params((int)h2, (int)h, (int)h2, X + (s0 + h) + (s0 + h) * ldx, ldx, scratch, h2,
                                   X + (s0 + h) + s0 * ldx, ldx, -1.0, 0.0, st);
@@ -336,7 +348,7 @@ cudaError_t trtri_blocked(const double* L, long long ld, int n, const double* li
       p2.strideA = b + b * ldx;
       p2.strideB = h2 * h;
       p2.strideC = b + b * ldx;
-      CK(dgemm(false, false, p2, s, (int)cnt));
+      CK(dgemm_nn_fill(p2, s, (int)cnt));
     }
   }
   return cudaGetLastError();
@@ -371,14 +383,14 @@ cudaError_t trtri_blocked_emu(const double* L, long long ld, int n, const double
         p1.strideA = b + b * ld;
         p1.strideB = b + b * ldx;
         p1.strideC = h2 * h;
-        CK(dgemm(false, false, p1, s, (int)cnt));
+        CK(dgemm_nn_fill(p1, s, (int)cnt));
         GemmParams p2 = gemm_params((int)h2, (int)h, (int)h2, X + (s0 + h) + (s0 + h) * ldx, ldx, scratch, h2,
                                     X + (s0 + h) + s0 * ldx, ldx, -1.0, 0.0, st);
         p2.mode = GEMM_K_TO_ROW;
         p2.strideA = b + b * ldx;
         p2.strideB = h2 * h;
         p2.strideC = b + b * ldx;
-        CK(dgemm(false, false, p2, s, (int)cnt));
+        CK(dgemm_nn_fill(p2, s, (int)cnt));
         continue;
       }
       for (long long c = 0; c < cnt; ++c) {
