@@ -29,6 +29,9 @@ from .api import (  # noqa: F401
     InvalidHyperparameter,
     KernelSpec,
     Lbfgs,
+    LoadedGpr,
+    PersistFailed,
+    UnsupportedPersistVersion,
     NonPositiveDefiniteMatrix,
     PredictiveCovariance,
     NonFiniteInput,

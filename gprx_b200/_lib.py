@@ -35,6 +35,8 @@ NOT_CONVERGED = 13
 INVALID_ARGUMENT = 14
 CAPACITY = 16
 NOT_POSITIVE_DEFINITE = 17
+PERSIST_FAILED = 18
+UNSUPPORTED_PERSIST_VERSION = 19
 
 # kernel node kinds
 NODE_SUM, NODE_PRODUCT = 1, 2
@@ -52,6 +54,12 @@ class Options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("jitter_kind", C.c_int32), ("jitter_initial", C.c_double),
                 ("jitter_multiplier", C.c_double), ("jitter_max_retries", C.c_int32), ("jitter_max", C.c_double),
                 ("device", C.c_int32), ("block_size", C.c_int32)]
+
+
+class PersistInfo(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("d", C.c_uint64), ("n_nodes", C.c_int32), ("n_theta", C.c_int32),
+                ("has_factor", C.c_int32), ("factor_kind", C.c_int32), ("factor_jitter", C.c_double),
+                ("jitter", Options), ("next_point_id", C.c_uint64)]
 
 
 class LbfgsOptions(C.Structure):
@@ -146,6 +154,13 @@ _SIGS = {
     "gprx_batch_fit": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.POINTER(LbfgsOptions), D, C.POINTER(FitReport),
                                    I32]),
     "gprx_batch_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "gprx_exact_save": (C.c_int32, [C.c_void_p, C.c_char_p, C.c_int32]),
+    "gprx_exact_load": (C.c_int32, [C.c_char_p, C.c_int32, C.POINTER(C.c_void_p)]),
+    "gprx_persist_inspect": (C.c_int32, [C.c_char_p, C.POINTER(PersistInfo)]),
+    "gprx_persist_read": (C.c_int32, [C.c_char_p, C.POINTER(KernelNode), D, D, D, D, D, U64]),
+    "gprx_persist_write": (C.c_int32, [C.c_char_p, D, C.c_uint64, C.c_uint64, D, C.POINTER(KernelNode), C.c_int32,
+                                       D, C.c_int32, C.POINTER(Options), D, D, C.c_int32, C.c_double, U64,
+                                       C.c_uint64]),
     "gprx_exact_loo": (C.c_int32, [C.c_void_p, C.c_int32, D, D]),
     "gprx_exact_predict_covariance": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
     "gprx_exact_sample": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, C.c_uint64, C.c_uint64, D]),

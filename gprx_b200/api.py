@@ -95,6 +95,14 @@ class NonPositiveDefiniteMatrix(GprError):
     """GprError::NonPositiveDefiniteMatrix (a leave-one-out [K⁻¹]_ii ≤ 0)."""
 
 
+class PersistFailed(GprError):
+    """GprError::PersistFailed (a saved model that cannot be read or written)."""
+
+
+class UnsupportedPersistVersion(GprError):
+    """GprError::UnsupportedPersistVersion."""
+
+
 class OutOfDeviceMemory(GprError):
     pass
 
@@ -116,6 +124,8 @@ _ERRORS = {
     L.INVALID_ARGUMENT: ShapeMismatch,
     L.CAPACITY: InvalidConfig,
     L.NOT_POSITIVE_DEFINITE: NonPositiveDefiniteMatrix,
+    L.PERSIST_FAILED: PersistFailed,
+    L.UNSUPPORTED_PERSIST_VERSION: UnsupportedPersistVersion,
 }
 
 
@@ -224,6 +234,22 @@ class KernelSpec:
     def copy(self):
         k = KernelSpec(self.kind, [c.copy() for c in self.children], self._params, self.dims)
         return k
+
+    @staticmethod
+    def from_nodes(nodes, log_theta):
+        """The tree of a prefix node list [(kind, arg), …] with its log θ."""
+        it = iter([(int(k), int(a)) for k, a in nodes])
+        th = [float(v) for v in log_theta]
+
+        def build():
+            kind, arg = next(it)
+            if kind in (L.NODE_SUM, L.NODE_PRODUCT):
+                return KernelSpec(kind, [build() for _ in range(arg)])
+            take = arg if kind == L.LEAF_RBF_ARD else (2 if kind == L.LEAF_PERIODIC else 1)
+            params = [th.pop(0) for _ in range(take)]
+            return KernelSpec(kind, params=params, dims=arg if kind == L.LEAF_RBF_ARD else 0)
+
+        return build()
 
 
 def RbfKernel(lengthscale):
@@ -516,6 +542,15 @@ class FittedGpr:
             raise ShapeMismatch("xs has %d values, expected %d×%d" % (xs.size, n_rows, n_cols))
         return xs
 
+    def save(self, directory):
+        """Writes <directory>/config.json and model.safetensors: x, y and the
+        model's settings (FittedGpr::save, src/gpr/fitted.rs)."""
+        check(L.lib().gprx_exact_save(self._h, str(directory).encode(), 0))
+
+    def save_with_factor(self, directory):
+        """save, plus the factor and α, so a load predicts without factoring."""
+        check(L.lib().gprx_exact_save(self._h, str(directory).encode(), 1))
+
     def loo_predict(self):
         """Leave-one-out mean and variance at every training point
         (FittedGpr::loo_predict, src/gpr/fitted.rs:697)."""
@@ -761,6 +796,32 @@ class FittedSgpr:
         on = OnlineSgpr(self._h, self.d)
         self._h = None
         return on
+
+
+class LoadedGpr:
+    """LoadedGpr::load (src/persist/mod.rs): a saved exact model as a
+    resident FittedGpr (factor_kind llt) or OnlineGpr (ldlt)."""
+
+    @staticmethod
+    def inspect(directory):
+        info = L.PersistInfo()
+        check(L.lib().gprx_persist_inspect(str(directory).encode(), C.byref(info)))
+        return info
+
+    @staticmethod
+    def load(directory, device=0):
+        info = LoadedGpr.inspect(directory)
+        nodes = (L.KernelNode * info.n_nodes)()
+        theta = np.zeros(info.n_theta)
+        x = np.zeros(info.n * info.d)
+        y = np.zeros(info.n)
+        check(L.lib().gprx_persist_read(str(directory).encode(), nodes, L.ptr(theta), L.ptr(x), L.ptr(y), None, None,
+                                        None))
+        kernel = KernelSpec.from_nodes([(nd.kind, nd.arg) for nd in nodes], theta[:-1])
+        h = C.c_void_p()
+        check(L.lib().gprx_exact_load(str(directory).encode(), int(device), C.byref(h)))
+        cls = OnlineGpr if info.factor_kind == 1 else FittedGpr
+        return cls(h, int(info.d), kernel)
 
 
 def sharded_value_and_gradient(shard, params, all_reduce, device=None, gradient=True):

@@ -11,6 +11,7 @@
 #include <string>
 
 #include "exact.cuh"
+#include "persist.h"
 #include "lbfgs.h"
 
 namespace gprx {
@@ -307,6 +308,45 @@ gprx_status gprx_exact_factor_jitter(gprx_exact* h, double* jitter) {
 gprx_status gprx_exact_predict(gprx_exact* h, const double* xs, uint64_t q, int32_t kind, double* mean, double* var) {
   CHECK_HANDLE(h);
   return h->s.predict(xs, q, kind, mean, var);
+}
+
+gprx_status gprx_exact_save(gprx_exact* h, const char* dir, int32_t with_factor) {
+  CHECK_HANDLE(h);
+  return h->s.save(dir, with_factor != 0);
+}
+
+gprx_status gprx_exact_load(const char* dir, int32_t device, gprx_exact** out) {
+  if (!dir || !out) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  *out = nullptr;
+  PersistModel m;
+  gprx_status st = persist_read(dir, m, true);
+  if (st != GPRX_OK) return st;
+  gprx_options o;
+  gprx_options_default(&o);
+  o.jitter_kind = m.jitter.jitter_kind;
+  o.jitter_initial = m.jitter.jitter_initial;
+  o.jitter_multiplier = m.jitter.jitter_multiplier;
+  o.jitter_max_retries = m.jitter.jitter_max_retries;
+  o.jitter_max = m.jitter.jitter_max;
+  o.device = device;
+  std::vector<double> theta(m.theta);
+  theta.push_back(m.log_noise);
+  std::unique_ptr<gprx_exact> h(new (std::nothrow) gprx_exact());
+  if (!h) return set_error(GPRX_OUT_OF_MEMORY, "host allocation");
+  st = h->s.create(m.x.data(), (uint64_t)m.n, (uint64_t)m.d, m.y.data(), m.nodes.data(), (int)m.nodes.size(),
+                   theta.data(), (int)theta.size(), &o);
+  if (st != GPRX_OK) return st;
+  if (m.has_factor) {
+    st = h->s.adopt_factor(m.l_map, m.alpha.data(), m.ldlt, m.factor_jitter, m.ids, m.next_id);
+    if (st != GPRX_OK) return st;
+  } else if (m.ldlt) {
+    // an online model saved without its factor: factor, go online, keep the ids
+    if ((st = h->s.online_begin()) != GPRX_OK) return st;
+    h->s.ids = m.ids;
+    h->s.next_id = m.next_id;
+  }
+  *out = h.release();
+  return GPRX_OK;
 }
 
 gprx_status gprx_exact_loo(gprx_exact* h, int32_t kind, double* mean, double* var) {

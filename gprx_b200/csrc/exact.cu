@@ -17,6 +17,7 @@
 #include <cmath>
 
 #include "exact.cuh"
+#include "persist.h"
 
 namespace gprx {
 
@@ -545,6 +546,81 @@ gprx_status ExactState::sample(const double* xs, uint64_t q, int kind, uint64_t 
   DevStatus ds;
   if ((st = read_status(&ds)) != GPRX_OK) return st;
   if (ds.code != GPRX_OK) return status_to_error(ds, jitter, q, GPRX_STAGE_PREDICT);
+  return GPRX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// saved models (FittedGpr::save / save_with_factor, OnlineGpr::save;
+// LoadedGpr::load, src/persist/mod.rs)
+// ---------------------------------------------------------------------------
+gprx_status ExactState::save(const char* dir, bool with_factor) {
+  if (!dir) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  gprx_status st;
+  PersistModel m;
+  m.n = n;
+  m.d = d;
+  m.nodes = kern.nodes;
+  m.theta = kern.theta;
+  m.log_noise = log_noise;
+  m.jitter = opt;
+  m.x.resize((size_t)n * d);
+  GPRX_CUDA_TRY(cudaMemcpy2DAsync(m.x.data(), sizeof(double) * n, x.p, sizeof(double) * cap, sizeof(double) * n, d,
+                                  cudaMemcpyDeviceToHost, stream));
+  m.y.resize(n);
+  GPRX_CUDA_TRY(cudaMemcpyAsync(m.y.data(), y.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+  m.ldlt = online;
+  if (online) {
+    m.ids = ids;
+    m.next_id = next_id;
+  }
+  if (with_factor) {
+    if (online) {
+      if (!alpha_ok && (st = online_alpha()) != GPRX_OK) return st;
+    } else if (!factor_ok || !alpha_ok) {
+      if ((st = factor_current()) != GPRX_OK) return st;
+    }
+    m.has_factor = true;
+    m.factor_jitter = online ? 0.0 : jitter;
+    m.l.resize((size_t)n * n);
+    m.alpha.resize(n);
+    GPRX_CUDA_TRY(cudaMemcpy2DAsync(m.l.data(), sizeof(double) * n, A.p, sizeof(double) * ld, sizeof(double) * n, n,
+                                    cudaMemcpyDeviceToHost, stream));
+    GPRX_CUDA_TRY(cudaMemcpyAsync(m.alpha.data(), alpha.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+  }
+  GPRX_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (m.has_factor)
+    for (long long j = 0; j < n; ++j)  // the stored layout: zero above the diagonal
+      for (long long i = 0; i < j; ++i) m.l[i + j * n] = 0.0;
+  return persist_write(dir, m);
+}
+
+// L (LLT) or unit-lower L with D on the diagonal (LDLT), n×n column-major on
+// the host (a file mapping), and α: the handle then predicts without factoring.
+gprx_status ExactState::adopt_factor(const double* l_host, const double* alpha_host, bool ldlt, double factor_jitter,
+                                     const std::vector<uint64_t>& point_ids, uint64_t next_point_id) {
+  gprx_status st;
+  if ((st = reset_status()) != GPRX_OK) return st;
+  GPRX_CUDA_TRY(cudaMemcpy2DAsync(A.p, sizeof(double) * ld, l_host, sizeof(double) * n, sizeof(double) * n, n,
+                                  cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(alpha.p, alpha_host, sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+  if (ldlt) {
+    online = true;
+    factor_ok = false;
+    linv_ok = false;
+    alpha_ok = true;
+    ids = point_ids;
+    next_id = next_point_id;
+  } else {
+    GPRX_CUDA_TRY(tri_inv_blocks(A.p, ld, n, false, linv.p, status.p, stream));
+    online = false;
+    factor_ok = true;
+    linv_ok = true;
+    alpha_ok = true;
+    jitter = factor_jitter;
+  }
+  DevStatus ds;
+  if ((st = read_status(&ds)) != GPRX_OK) return st;
+  if (ds.code != GPRX_OK) return status_to_error(ds, factor_jitter, n, GPRX_STAGE_PREDICT);
   return GPRX_OK;
 }
 

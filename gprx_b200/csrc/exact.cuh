@@ -94,6 +94,10 @@ struct ExactState {
   gprx_status covariance_dev(const double* xs, uint64_t q, int kind, double* mean_host);
   gprx_status predict_covariance(const double* xs, uint64_t q, int kind, double* mean, double* cov);
   gprx_status sample(const double* xs, uint64_t q, int kind, uint64_t n_draws, uint64_t seed, double* out);
+  // saved models (persist.cpp): write this model; read a stored factor in
+  gprx_status save(const char* dir, bool with_factor);
+  gprx_status adopt_factor(const double* l_host, const double* alpha_host, bool ldlt, double factor_jitter,
+                           const std::vector<uint64_t>& point_ids, uint64_t next_point_id);
   gprx_status reset_status();
   gprx_status read_status(DevStatus* out);
   gprx_status stage_times(double* out5);

@@ -52,7 +52,9 @@ enum {
   GPRX_INVALID_ARGUMENT = 14,      /* null handle / null pointer / bad enum */
   GPRX_STALE_FACTOR = 15,          /* internal: the factor was consumed by a gradient */
   GPRX_CAPACITY = 16,              /* a fixed-size buffer was too small for the request */
-  GPRX_NOT_POSITIVE_DEFINITE = 17  /* GprError::NonPositiveDefiniteMatrix (a leave-one-out [K⁻¹]_ii ≤ 0) */
+  GPRX_NOT_POSITIVE_DEFINITE = 17, /* GprError::NonPositiveDefiniteMatrix (a leave-one-out [K⁻¹]_ii ≤ 0) */
+  GPRX_PERSIST_FAILED = 18,        /* GprError::PersistFailed{kind, reason} (src/persist/mod.rs) */
+  GPRX_UNSUPPORTED_PERSIST_VERSION = 19 /* GprError::UnsupportedPersistVersion */
 };
 
 /* CholeskyStage (src/error.rs:31-39) */
@@ -186,6 +188,42 @@ gprx_status gprx_exact_factor_jitter(gprx_exact* h, double* jitter);
  * (GprCore::write_moments, src/gpr/shared.rs:754-820). */
 gprx_status gprx_exact_predict(gprx_exact* h, const double* xs, uint64_t q, int32_t variance_kind,
                                double* mean, double* var);
+
+/* Saved models (gprx's format_version 1: <dir>/config.json and
+ * <dir>/model.safetensors, docs/persist-format.md; src/persist/mod.rs).
+ * gprx_exact_save writes x, y, the kernel tree, noise and jitter policy
+ * (FittedGpr::save, OnlineGpr::save); with_factor also writes l and α
+ * (save_with_factor: l is L of an LLT model, or the unit-lower L with D on
+ * the diagonal of an online LDLT model with its point ids).  gprx_exact_load
+ * reads such a directory into a resident handle on `device` (LoadedGpr::load):
+ * a stored factor is copied to the device straight from the mapped file and
+ * the model predicts without refactoring; without one the first use factors.
+ * This backend reads and writes rbf / rbf_ard / constant / periodic leaves
+ * under sum / product, identity input and target maps and double precision;
+ * other files are refused with GPRX_PERSIST_FAILED naming what is missing. */
+gprx_status gprx_exact_save(gprx_exact* h, const char* dir, int32_t with_factor);
+gprx_status gprx_exact_load(const char* dir, int32_t device, gprx_exact** out);
+/* Host-side access to a saved directory (no GPU needed). */
+typedef struct {
+  uint64_t n, d;
+  int32_t n_nodes, n_theta;   /* n_theta = kernel parameters + 1 */
+  int32_t has_factor;         /* 1: l and alpha are stored */
+  int32_t factor_kind;        /* 0 llt, 1 ldlt */
+  double factor_jitter;
+  gprx_options jitter;        /* the stored jitter policy (other fields default) */
+  uint64_t next_point_id;     /* ldlt only */
+} gprx_persist_info;
+gprx_status gprx_persist_inspect(const char* dir, gprx_persist_info* out);
+/* nodes[n_nodes], theta[n_theta] (log), x[n·d] column-major, y[n]; l[n·n]
+ * and alpha[n] when has_factor (nullable), point_ids[n] when ldlt (nullable). */
+gprx_status gprx_persist_read(const char* dir, gprx_kernel_node* nodes, double* theta, double* x, double* y,
+                              double* l, double* alpha, uint64_t* point_ids);
+/* Writes a model directory from host arrays (factor_kind 0 llt / 1 ldlt;
+ * l and alpha nullable = no factor; point_ids required for ldlt). */
+gprx_status gprx_persist_write(const char* dir, const double* x, uint64_t n, uint64_t d, const double* y,
+                               const gprx_kernel_node* nodes, int32_t n_nodes, const double* theta, int32_t n_theta,
+                               const gprx_options* jitter, const double* l, const double* alpha, int32_t factor_kind,
+                               double factor_jitter, const uint64_t* point_ids, uint64_t next_point_id);
 
 /* Leave-one-out mean and variance at every training point (GPML §5.4.2):
  * mean_i = y_i − α_i / Q_ii, observation variance 1 / Q_ii, latent
