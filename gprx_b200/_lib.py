@@ -164,6 +164,10 @@ _SIGS = {
     "gprx_exact_loo": (C.c_int32, [C.c_void_p, C.c_int32, D, D]),
     "gprx_exact_predict_covariance": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
     "gprx_exact_sample": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, C.c_uint64, C.c_uint64, D]),
+    "gprx_sgpr_insert_inducing": (C.c_int32, [C.c_void_p, D, U64]),
+    "gprx_sgpr_delete_inducing": (C.c_int32, [C.c_void_p, C.c_uint64]),
+    "gprx_sgpr_m": (C.c_uint64, [C.c_void_p]),
+    "gprx_sgpr_inducing_ids": (C.c_int32, [C.c_void_p, U64, C.c_uint64]),
     "gprx_sgpr_shard_sizes": (C.c_int32, [C.c_void_p, U64, U64]),
     "gprx_sgpr_shard_assemble": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_void_p]),
     "gprx_sgpr_shard_nlml": (C.c_int32, [C.c_void_p, C.c_void_p, D, C.c_void_p]),

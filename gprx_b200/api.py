@@ -883,6 +883,28 @@ class OnlineSgpr(FittedSgpr):
         z = _check_points(z, m, self.d)
         check(L.lib().gprx_sgpr_set_inducing(self._h, L.ptr(z), m))
 
+    def m(self):
+        return int(L.lib().gprx_sgpr_m(self._h))
+
+    def inducing_ids(self):
+        m = self.m()
+        out = np.zeros(m, dtype=np.uint64)
+        check(L.lib().gprx_sgpr_inducing_ids(self._h, out.ctypes.data_as(L.U64), m))
+        return out
+
+    def insert_inducing(self, z_new):
+        """Appends one inducing point; returns its id (OnlineSgpr::insert_inducing)."""
+        z = L.f64(z_new)
+        if z.size != self.d:
+            raise ShapeMismatch("inducing point has %d features, model has %d" % (z.size, self.d))
+        iid = C.c_uint64(0)
+        check(L.lib().gprx_sgpr_insert_inducing(self._h, L.ptr(z), C.byref(iid)))
+        return int(iid.value)
+
+    def delete_inducing(self, inducing_id):
+        """Removes the inducing point with this id (OnlineSgpr::delete_inducing)."""
+        check(L.lib().gprx_sgpr_delete_inducing(self._h, int(inducing_id)))
+
 
 # ---------------------------------------------------------------------------
 # batched exact GPR: many independent problems sharing one kernel tree

@@ -334,6 +334,12 @@ struct SgprState {
   gprx_status insert(const double* xnew, double ynew, uint64_t* id);
   gprx_status remove(uint64_t id);
   gprx_status set_inducing(const double* zh, uint64_t mm);
+  // OnlineSgpr::insert_inducing / delete_inducing (src/sgpr/online/mod.rs:1301,1943)
+  std::vector<uint64_t> inducing_ids;
+  uint64_t next_inducing_id = 0;
+  gprx_status insert_inducing(const double* znew, uint64_t* id);
+  gprx_status delete_inducing(uint64_t id);
+  gprx_status replace_inducing(const std::vector<double>& znew, int mm);
   // one shard of a VFE evaluation over n split across processes (the sums
   // over n travel in two exchange buffers that the caller sums over shards)
   gprx_status factor_kmm_and_a(EmuWork& ew, bool& emu);
@@ -429,6 +435,7 @@ gprx_status SgprState::create(const double* xh, uint64_t nn, uint64_t dd, const 
     order.push_back(i);
     ids.push_back(next_id++);
   }
+  for (int i = 0; i < m; ++i) inducing_ids.push_back(next_inducing_id++);
   return GPRX_OK;
 }
 
@@ -918,6 +925,65 @@ gprx_status SgprState::remove(uint64_t id) {
   return solve_w();
 }
 
+// The inducing points as the host sees them (m×d column-major).
+static gprx_status download_z(SgprState& s, std::vector<double>& out) {
+  out.resize((size_t)s.m * s.d);
+  GPRX_CUDA_TRY(cudaMemcpyAsync(out.data(), s.z.p, sizeof(double) * out.size(), cudaMemcpyDeviceToHost, s.stream));
+  GPRX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+  return GPRX_OK;
+}
+
+// Assembles the VFE system of a changed inducing set; on failure the model
+// goes back to the set it had (OnlineSgpr::atomically).  Every change is the
+// assembly of the new set (the reference's own fallback, O(n m²)), so its
+// results are those of Sgpr::factor at the same θ, X and Z.
+gprx_status SgprState::replace_inducing(const std::vector<double>& znew, int mm) {
+  std::vector<double> old;
+  gprx_status st = download_z(*this, old);
+  if (st != GPRX_OK) return st;
+  const int m_old = m;
+  st = set_inducing(znew.data(), (uint64_t)mm);
+  if (st != GPRX_OK) {
+    gprx_error_info saved = last_error();
+    set_inducing(old.data(), (uint64_t)m_old);
+    last_error() = saved;
+  }
+  return st;
+}
+
+gprx_status SgprState::insert_inducing(const double* znew, uint64_t* id) {
+  if (!znew || !id) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (!all_finite(znew, d)) return set_error(GPRX_NONFINITE_INPUT, "non-finite inducing point");
+  std::vector<double> zo, zn((size_t)(m + 1) * d);
+  gprx_status st = download_z(*this, zo);
+  if (st != GPRX_OK) return st;
+  for (int f = 0; f < d; ++f) {  // append a row (column-major)
+    std::copy(zo.begin() + (size_t)f * m, zo.begin() + (size_t)(f + 1) * m, zn.begin() + (size_t)f * (m + 1));
+    zn[(size_t)f * (m + 1) + m] = znew[f];
+  }
+  if ((st = replace_inducing(zn, m + 1)) != GPRX_OK) return st;
+  *id = next_inducing_id++;
+  inducing_ids.push_back(*id);
+  return GPRX_OK;
+}
+
+gprx_status SgprState::delete_inducing(uint64_t id) {
+  if (m <= 1) return set_error(GPRX_INSUFFICIENT_DATA, "an inducing delete needs at least 2 inducing points");
+  auto it = std::find(inducing_ids.begin(), inducing_ids.end(), id);
+  if (it == inducing_ids.end()) return set_error(GPRX_INVALID_POINT_ID, "unknown inducing id " + std::to_string(id));
+  const int idx = (int)(it - inducing_ids.begin());
+  std::vector<double> zo, zn;
+  gprx_status st = download_z(*this, zo);
+  if (st != GPRX_OK) return st;
+  zn.reserve((size_t)(m - 1) * d);
+  for (int f = 0; f < d; ++f)
+    for (int i = 0; i < m; ++i)
+      if (i != idx) zn.push_back(zo[(size_t)f * m + i]);
+  if ((st = replace_inducing(zn, m - 1)) != GPRX_OK) return st;
+  inducing_ids.erase(inducing_ids.begin() + idx);
+  return GPRX_OK;
+}
+
 gprx_status SgprState::set_inducing(const double* zh, uint64_t mm) {
   if (!zh) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (mm == 0) return set_error(GPRX_EMPTY_INPUT, "no inducing points");
@@ -1281,7 +1347,32 @@ gprx_status gprx_sgpr_delete(gprx_sgpr* h, uint64_t id) {
 
 gprx_status gprx_sgpr_set_inducing(gprx_sgpr* h, const double* z, uint64_t m) {
   CHECK_SGPR(h);
-  return h->s.set_inducing(z, m);
+  SgprState& st = h->s;
+  const gprx_status r = st.set_inducing(z, m);
+  if (r == GPRX_OK) {  // a new set: new ids
+    st.inducing_ids.clear();
+    for (int i = 0; i < st.m; ++i) st.inducing_ids.push_back(st.next_inducing_id++);
+  }
+  return r;
+}
+
+gprx_status gprx_sgpr_insert_inducing(gprx_sgpr* h, const double* z_new, uint64_t* id) {
+  CHECK_SGPR(h);
+  return h->s.insert_inducing(z_new, id);
+}
+
+gprx_status gprx_sgpr_delete_inducing(gprx_sgpr* h, uint64_t id) {
+  CHECK_SGPR(h);
+  return h->s.delete_inducing(id);
+}
+
+uint64_t gprx_sgpr_m(const gprx_sgpr* h) { return h ? (uint64_t)h->s.m : 0; }
+
+gprx_status gprx_sgpr_inducing_ids(const gprx_sgpr* h, uint64_t* out, uint64_t m) {
+  CHECK_SGPR(h);
+  if (!out || m != (uint64_t)h->s.m) return set_error(GPRX_SHAPE_MISMATCH, "inducing id count");
+  std::copy(h->s.inducing_ids.begin(), h->s.inducing_ids.end(), out);
+  return GPRX_OK;
 }
 
 uint64_t gprx_sgpr_n(const gprx_sgpr* h) { return h ? (uint64_t)h->s.n : 0; }

@@ -312,6 +312,17 @@ gprx_status gprx_sgpr_point_ids(gprx_sgpr* h, uint64_t* out, uint64_t n);
  * delete (OnlineSgpr::insert_inducing / delete_inducing, src/sgpr/online/mod.rs:1301,1943)
  * taken by reassembly. */
 gprx_status gprx_sgpr_set_inducing(gprx_sgpr* h, const double* z, uint64_t m);
+/* OnlineSgpr::insert_inducing / delete_inducing / inducing_ids
+ * (src/sgpr/online/mod.rs:1943,1301,694): append one inducing point (its id
+ * is returned; ids are never reused) or remove one by id (m ≤ 1 →
+ * GPRX_INSUFFICIENT_DATA, unknown id → GPRX_INVALID_POINT_ID).  Each change
+ * assembles the VFE system of the new set (O(n m²), the reference's own path
+ * when its bordered update does not apply), so the model equals Sgpr::factor
+ * at the same θ, X and Z; on an error the model keeps its inducing set. */
+gprx_status gprx_sgpr_insert_inducing(gprx_sgpr* h, const double* z_new, uint64_t* id);
+gprx_status gprx_sgpr_delete_inducing(gprx_sgpr* h, uint64_t id);
+uint64_t gprx_sgpr_m(const gprx_sgpr* h);
+gprx_status gprx_sgpr_inducing_ids(const gprx_sgpr* h, uint64_t* out, uint64_t m);
 
 /* Sharded VFE evaluation: n split over processes (one GPU each), each
  * process holding a handle created with ITS points and the SAME inducing

@@ -132,10 +132,11 @@ def test_online_sgpr_golden_through_abi(case):
                 on.delete(on.point_ids()[op["slot"]])
             elif op["kind"] == "insert_inducing":
                 z.append(zall[:, op["pop_index"]])
-                on.set_inducing(np.array(z).T.reshape(-1), len(z))
+                assert on.insert_inducing(zall[:, op["pop_index"]]) == max(on.inducing_ids())
             else:
                 z.pop(op["slot"])
-                on.set_inducing(np.array(z).T.reshape(-1), len(z))
+                on.delete_inducing(on.inducing_ids()[op["slot"]])
+            assert on.m() == len(z)
         assert on.n() == step["n"]
         assert O.rel_err(on.neg_log_marginal_likelihood(), step["neg_log_marginal_likelihood"]) <= TOL_GOLD, k
         for kind, key in ((0, "latent_variance"), (1, "observation_variance")):
@@ -198,3 +199,41 @@ def test_sgpr_fit_decreases_nlml_and_matches_oracle_at_optimum():
     assert O.rel_err(nl, orc.nlml()) <= 1e-9
     g0 = O.Sgpr([[11, 2]], s.kernel.get_params() + [math.log(0.5)], x, n, d, y, z, m).grad()
     assert np.linalg.norm(orc.grad()) < 1e-2 * np.linalg.norm(g0)
+
+
+def test_inducing_ids_changes_and_errors():
+    # ids are never reused; each change equals a fresh factor at the new Z
+    # (the oracle's set_inducing), and a failed change keeps the old set
+    rs = np.random.RandomState(21)
+    d, n, m = 2, 300, 12
+    nodes, theta = [[11, 2]], [math.log(0.4), math.log(0.6)]
+    params = theta + [math.log(0.05)]
+    x = rs.uniform(0, 1, size=(n, d))
+    y = np.sin(4 * x.sum(1)) + 0.05 * rs.standard_normal(n)
+    z = [x[i] for i in range(m)]
+    on = model(nodes, theta, 0.05, x.T.reshape(-1), n, d, y, np.array(z).T.reshape(-1), m).into_online()
+    assert list(on.inducing_ids()) == list(range(m))
+    orc = O.Sgpr(nodes, params, x.T.reshape(-1), n, d, y, np.array(z).T.reshape(-1), m)
+    xs = rs.uniform(0, 1, size=(15, d)).T.reshape(-1)
+    new = rs.uniform(0, 1, size=(3, d))
+    for k in range(3):
+        assert on.insert_inducing(new[k]) == m + k
+        z.append(new[k])
+    for iid in (3, 0, 13):
+        slot = list(on.inducing_ids()).index(iid)
+        on.delete_inducing(iid)
+        z.pop(slot)
+    assert list(on.inducing_ids()) == [1, 2, 4, 5, 6, 7, 8, 9, 10, 11, 12, 14]
+    orc.set_inducing(np.array(z).T.reshape(-1), len(z))
+    assert O.rel_err(on.neg_log_marginal_likelihood(), orc.nlml()) <= TOL
+    p = on.predict(xs, 15, d)
+    mo, vo = orc.predict(xs, 15, 1)
+    assert np.all(O.rel_err(p.mean, mo) <= TOL) and np.all(O.rel_err(p.variance, vo) <= TOL)
+    with pytest.raises(gx.IndexOutOfRange):
+        on.delete_inducing(3)
+    with pytest.raises(gx.NonFiniteInput):
+        on.insert_inducing([float("nan"), 0.0])
+    assert on.m() == len(z)
+    one = model(nodes, theta, 0.05, x.T.reshape(-1), n, d, y, x[:1].T.reshape(-1), 1).into_online()
+    with pytest.raises(gx.InsufficientData):
+        one.delete_inducing(0)
