@@ -307,7 +307,7 @@ cudaError_t fill_cross(const HostKernel& k, const double* x1, long long ldx1, in
 // ---------------------------------------------------------------------------
 // device: gradient contraction
 // ---------------------------------------------------------------------------
-constexpr int GRAD_THREADS = 256;
+constexpr int GRAD_THREADS = 256;  // two blocks per SM for trees of ARD width ≤ 8 (128 registers, no spills)
 constexpr int GRAD_MAX_BLOCKS = 148 * 4;
 
 int grad_max_blocks() { return GRAD_MAX_BLOCKS; }
@@ -334,7 +334,7 @@ __device__ __forceinline__ void store_slots(double (&vals)[NS], double (*red)[NS
 // With alpha: W_ij = α_i α_j − M_ij (the exact-GPR weight, M = K⁻¹) and the
 // last slot collects Σ W_ii; without: W_ij = M_ij.
 template <int ARD_D>
-__global__ void __launch_bounds__(GRAD_THREADS) grad_contract_kernel(KTree t, const double* x, long long ldx, int n,
+__global__ void __launch_bounds__(GRAD_THREADS, ARD_D <= 8 ? 2 : 1) grad_contract_kernel(KTree t, const double* x, long long ldx, int n,
                                                                      const double* kinv, long long ld,
                                                                      const double* alpha, double* partials,
                                                                      const DevStatus* st) {
@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(GRAD_THREADS) grad_contract_kernel(KTree t, co
 
 // Rectangle contraction Σ_{i,c} W_ic ∂k(z_i, x_c)/∂θ (W is m×n, ldw).
 template <int ARD_D>
-__global__ void __launch_bounds__(GRAD_THREADS) cross_contract_kernel(KTree t, const double* z, long long ldz, int m,
+__global__ void __launch_bounds__(GRAD_THREADS, ARD_D <= 8 ? 2 : 1) cross_contract_kernel(KTree t, const double* z, long long ldz, int m,
                                                                       const double* x, long long ldx, int n,
                                                                       const double* W, long long ldw, double* partials,
                                                                       const DevStatus* st) {
