@@ -554,32 +554,43 @@ cudaError_t logdet_diag(const double* L, long long ld, int n, bool ldlt, double*
 
 // z_i = Σ_{j ≤ i} X_ij y_j: a block owns 32 rows and walks the columns.
 constexpr int TRMV_ROWS = 32;
-__global__ void trmv_lower_kernel(const double* X, long long ld, int n, const double* y, double* z,
-                                  const DevStatus* st) {
-  __shared__ double part[8][TRMV_ROWS];
+__global__ void __launch_bounds__(1024) trmv_lower_kernel(const double* X, long long ld, int n, const double* y,
+                                                            double* z, const DevStatus* st) {
+  constexpr int CG = 32;  // column groups: 32 rows × 32 groups, four loads in flight per thread
+  __shared__ double part[CG][TRMV_ROWS + 1];
   if (dev_failed(st)) return;
-  int r = threadIdx.x % TRMV_ROWS, cg = threadIdx.x / TRMV_ROWS;  // 8 column groups
-  int i = blockIdx.x * TRMV_ROWS + r;
-  int jmax = min(n, (blockIdx.x + 1) * TRMV_ROWS);
-  double acc = 0.0;
+  const int r = threadIdx.x % TRMV_ROWS, cg = threadIdx.x / TRMV_ROWS;
+  const int i = blockIdx.x * TRMV_ROWS + r;
+  const int jmax = min(n, (blockIdx.x + 1) * TRMV_ROWS);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   if (i < n) {
-    for (int j = cg; j < jmax; j += 8) {
-      if (j <= i) acc = fma(X[i + (long long)j * ld], y[j], acc);
+    int j = cg;
+    for (; j + 3 * CG < jmax; j += 4 * CG) {
+      const double x0 = j <= i ? X[i + (long long)j * ld] : 0.0;
+      const double x1 = j + CG <= i ? X[i + (long long)(j + CG) * ld] : 0.0;
+      const double x2 = j + 2 * CG <= i ? X[i + (long long)(j + 2 * CG) * ld] : 0.0;
+      const double x3 = j + 3 * CG <= i ? X[i + (long long)(j + 3 * CG) * ld] : 0.0;
+      a0 = fma(x0, y[j], a0);
+      a1 = fma(x1, y[j + CG], a1);
+      a2 = fma(x2, y[j + 2 * CG], a2);
+      a3 = fma(x3, y[j + 3 * CG], a3);
     }
+    for (; j < jmax; j += CG)
+      if (j <= i) a0 = fma(X[i + (long long)j * ld], y[j], a0);
   }
-  part[cg][r] = acc;
+  part[cg][r] = (a0 + a1) + (a2 + a3);
   __syncthreads();
   if (cg == 0 && i < n) {
     double s = 0.0;
 #pragma unroll
-    for (int c = 0; c < 8; ++c) s += part[c][r];
+    for (int c = 0; c < CG; ++c) s += part[c][r];
     z[i] = s;
   }
 }
 
 cudaError_t trmv_lower(const double* X, long long ld, int n, const double* y, double* z, DevStatus* st,
                        cudaStream_t s) {
-  GPRX_LAUNCH(trmv_lower_kernel, ceil_div(n, TRMV_ROWS), TRMV_ROWS * 8, 0, s, X, ld, n, y, z, st);
+  GPRX_LAUNCH(trmv_lower_kernel, ceil_div(n, TRMV_ROWS), TRMV_ROWS * 32, 0, s, X, ld, n, y, z, st);
   return cudaGetLastError();
 }
 
