@@ -234,7 +234,15 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
   __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
   __shared__ uint32_t tmem_sh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const long long i0 = (long long)blockIdx.x * EMU_M, j0 = (long long)blockIdx.y * EMU_N;
+  // bands of 8 row tiles: the CTAs launched together share their A rows and
+  // sweep the column tiles, so a band's A slices stay in L2 while B streams
+  // (a bijection of the grid onto the tiles)
+  constexpr int BAND = 8;
+  const long long lid = blockIdx.x + (long long)blockIdx.y * gridDim.x;
+  const long long band = lid / ((long long)BAND * gridDim.y), within = lid % ((long long)BAND * gridDim.y);
+  const int rows_in_band = (int)min((long long)BAND, (long long)gridDim.x - band * BAND);
+  const int bx = (int)(band * BAND + within % rows_in_band), by = (int)(within / rows_in_band);
+  const long long i0 = (long long)bx * EMU_M, j0 = (long long)by * EMU_N;
   if (g.lower && i0 + g.row0 + EMU_M - 1 < j0 + g.col0) return;  // wholly above the diagonal
   const int nkc = g.Kpad / EMU_KC;
   int kc0 = 0, kc1 = nkc;
@@ -270,8 +278,8 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
   // warp 0 issues the MMAs as soon as a stage is full, so the tensor pipe
   // holds the next chunk's MMAs while the current chunk's run
   if (warp == 1 && lane == 0) {
-    const int8_t* Ab = g.A + ((size_t)blockIdx.x * nkc) * 8192;
-    const int8_t* Bb = g.B + ((size_t)(blockIdx.y >> 1) * nkc) * 8192 + (blockIdx.y & 1) * 4096;
+    const int8_t* Ab = g.A + ((size_t)bx * nkc) * 8192;
+    const int8_t* Bb = g.B + ((size_t)(by >> 1) * nkc) * 8192 + (by & 1) * 4096;
     const size_t planeA = (size_t)g.ntrA * nkc * 8192, planeB = (size_t)g.ntrB * nkc * 8192;
     int issued = 0;
     for (int c = 0; c < nch; ++c) {
