@@ -152,6 +152,33 @@ def fp64_peak_tflops(torch, dev):
     return best
 
 
+def int8_peak_tops(torch, dev):
+    """Dense int8 tensor throughput of this GPU through cuBLASLt
+    (torch._int_mm, 8192³, int32 accumulate): the denominator of the
+    emulated GEMM, whose work is int8 slice products.  None when the call
+    is not available."""
+    try:
+        n = 8192
+        a = torch.randint(-64, 64, (n, n), dtype=torch.int8, device=dev)
+        b = torch.randint(-64, 64, (n, n), dtype=torch.int8, device=dev)
+        for _ in range(2):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            e1.synchronize()
+            best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+        del a, b
+        torch.cuda.empty_cache()
+        return best
+    except Exception:
+        return None
+
+
 def load_traffic():
     path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(path):
@@ -160,14 +187,15 @@ def load_traffic():
     return None
 
 
-def emu_kernel_roofline(n, peaks, traffic):
+def emu_kernel_roofline(n, peaks, traffic, int8_peak=None):
     """The dominant kernel of the mixed form, emu_gemm_kernel<7>, timed with
     CUDA events on its own stream (gprx_probe_emu_gemm) at the shape of the
     evaluation's largest product: the top-level coupling L21 = A21 X11ᵀ,
     (n/2)³.  Work per launch: 28 int8 slice products of 2·(n/2)³ ops (the
-    FP64-equivalent rate is that ÷ 28).  Peak: twice the measured dense bf16
-    rate (B200's int8 dense rate is twice its bf16 rate), else twice the
-    fallback 1.59 PFLOP/s."""
+    FP64-equivalent rate is that ÷ 28).  Peak: cuBLASLt's dense int8 GEMM
+    measured in the same run; without it, twice the measured dense bf16 rate
+    (B200's int8 dense rate is twice its bf16 rate), else twice the fallback
+    1.59 PFLOP/s."""
     from gprx_b200 import _lib as L
 
     h = n // 2
@@ -178,9 +206,12 @@ def emu_kernel_roofline(n, peaks, traffic):
     eq = 2.0 * h ** 3 / (out[0] * 1e-3) / 1e12
     achieved = 28 * eq
     bf16 = peaks.get("bf16_tflops")
-    peak = 2.0 * bf16 if bf16 else 2.0 * 1590.0
-    src = ("2 x measured dense bf16 burst (MEASURED_PEAKS.json bf16_tflops, of measured)" if bf16
-           else "2 x the fallback dense bf16 1.59 PFLOP/s (of fallback)")
+    if int8_peak:
+        peak, src = int8_peak, "cuBLASLt int8 GEMM 8192^3 measured in this run (torch._int_mm; of measured)"
+    elif bf16:
+        peak, src = 2.0 * bf16, "2 x measured dense bf16 burst (MEASURED_PEAKS.json bf16_tflops, of measured)"
+    else:
+        peak, src = 2.0 * 1590.0, "2 x the fallback dense bf16 1.59 PFLOP/s (of fallback)"
     return {"bound": "tensor", "kernel": "emu_gemm_kernel<7> (tcgen05.mma kind::i8, TMEM accumulators)",
             "shape": "%d^3, 7 slices (the top-level coupling product at n = %d)" % (h, n),
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s (int8 tensor ops)", "frac": achieved / peak,
@@ -722,7 +753,7 @@ def main():
                                    "total": stage[4]}}
     roofline = dict(stage_roofline)
     if mixed and rank == 0:
-        k = emu_kernel_roofline(n, peaks, traffic)
+        k = emu_kernel_roofline(n, peaks, traffic, int8_peak_tops(torch, dev))
         if k is not None:
             roofline = k
             roofline["stage"] = stage_roofline
