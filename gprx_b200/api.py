@@ -500,6 +500,16 @@ class FittedGpr:
         check(L.lib().gprx_exact_eval(self._h, L.ptr(p), p.size, L.ptr(v), None))
         return float(v[0])
 
+    def hessian(self, params):
+        """Hessian of the NLML at `params`, p × p (FittedGpr::hessian_into,
+        src/gpr/fitted.rs:665; src/gpr/exact_fit.rs:443-637)."""
+        p = L.f64(params)
+        if p.size != self.num_params():
+            raise ShapeMismatch("expected %d parameters" % self.num_params())
+        out = np.zeros(p.size * p.size)
+        check(L.lib().gprx_exact_hessian(self._h, L.ptr(p), p.size, L.ptr(out)))
+        return out.reshape(p.size, p.size)
+
     def neg_log_marginal_likelihood(self):
         v = np.zeros(1)
         check(L.lib().gprx_exact_nlml(self._h, L.ptr(v)))

@@ -292,6 +292,13 @@ gprx_status gprx_exact_eval(gprx_exact* h, const double* params, uint64_t p, dou
   return h->s.eval(params, nlml, grad);
 }
 
+gprx_status gprx_exact_hessian(gprx_exact* h, const double* params, uint64_t p, double* out) {
+  CHECK_HANDLE(h);
+  if (!params || !out) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (p != (uint64_t)h->s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
+  return h->s.hessian(params, out);
+}
+
 gprx_status gprx_exact_nlml(gprx_exact* h, double* nlml) {
   CHECK_HANDLE(h);
   if (!nlml) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");

@@ -17,6 +17,7 @@
 #include <cmath>
 
 #include "exact.cuh"
+#include "hessian.cuh"
 #include "persist.h"
 
 namespace gprx {
@@ -299,6 +300,97 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
   write_params(prev.data());
   factor_current();
   return set_cholesky_error(last, n, GPRX_STAGE_FIT);
+}
+
+// ExactFit::hessian_into_fit (src/gpr/exact_fit.rs:443-637): one evaluation
+// at θ leaves K⁻¹ (lower) in A, L⁻¹ in Xinv and α; the second-order part is
+// −½ ⟨ααᵀ − K⁻¹, ∂²K/∂θ_i∂θ_j⟩ over the lower triangle (weight 2 off the
+// diagonal), the first-order part −½ ⟨S_i, S_j⟩_F + v_iᵀ v_j with
+// S_i = L⁻¹ A_i L⁻ᵀ and v_i = L⁻¹ A_i α (A_i = ∂K/∂θ_i, or σn² I for the
+// noise).  out is row-major p × p.
+gprx_status ExactState::hessian(const double* params, double* out) {
+  const int p = num_params(), pk = kern.n_params;
+  if (online) return set_error(GPRX_INVALID_CONFIG, "an online model takes no hyperparameter evaluation");
+  std::vector<double> g(p);
+  double v = 0.0;
+  gprx_status st = eval(params, &v, g.data());
+  if (st != GPRX_OK) return st;
+  const size_t nn = (size_t)ld * n;
+  const int SEC = 0, TR = HESS_MAX_PARAMS * HESS_MAX_PARAMS, AA = TR + 1, FRO = TR + 2, VD = FRO + p * p;
+  const int nres = VD + p * p;
+  if (hs_s.ensure(nn * p) || hs_p.ensure(nn) || hs_v.ensure((size_t)n * (p + 1)) ||
+      hs_part.ensure((size_t)HESS_MAX_BLOCKS * HESS_MAX_PARAMS) || hs_res.ensure(nres)) {
+    hs_s.reset();
+    hs_p.reset();
+    return set_error(GPRX_OUT_OF_MEMORY, "device allocation of the Hessian scratch failed");
+  }
+  GPRX_CUDA_TRY(hs_res_h.ensure(nres));
+  if ((st = reset_status()) != GPRX_OK) return st;
+  HessMap hm{};
+  hm.n_par = pk;
+  for (int l = 0; l < kern.tree.n_leaves; ++l) {
+    const KLeaf& lf = kern.tree.leaf[l];
+    const int cnt = lf.kind == GPRX_LEAF_PERIODIC ? 2 : lf.kind == GPRX_LEAF_RBF_ARD ? kern.tree.d : 1;
+    for (int a = 0; a < cnt; ++a) {
+      hm.leaf_of[lf.param + a] = l;
+      hm.local_of[lf.param + a] = a;
+    }
+  }
+  // second-order part, one launch per row
+  for (int i = 0; i < pk; ++i) {
+    int blocks = 0;
+    GPRX_CUDA_TRY(hess_second(kern, hm, i, x.p, cap, n, A.p, ld, alpha.p, hs_part.p, &blocks, stream));
+    GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, HESS_MAX_PARAMS, pk - i, hs_res.p + SEC + i * HESS_MAX_PARAMS,
+                               stream));
+  }
+  GPRX_CUDA_TRY(trace_dev(A.p, ld, n, hs_res.p + TR, stream));
+  GPRX_CUDA_TRY(dot_dev(alpha.p, alpha.p, n, hs_res.p + AA, status.p, stream));
+  // first-order part: S_i in hs_s (slot i), v_i in column i of hs_v; the
+  // noise's v (column pk) is L⁻¹ α, scaled by σn² on the host
+  double* u = hs_v.p + (size_t)p * n;
+  for (int i = 0; i < pk; ++i) {
+    double* Si = hs_s.p + (size_t)i * nn;
+    GPRX_CUDA_TRY(fill_deriv(kern, hm, i, x.p, cap, n, Si, ld, stream));
+    GPRX_CUDA_TRY(gemv_t(Si, ld, n, n, false, alpha.p, u, status.p, stream));
+    GPRX_CUDA_TRY(trmv_lower(Xinv.p, ld, n, u, hs_v.p + (size_t)i * n, status.p, stream));
+    GPRX_CUDA_TRY(dgemm(false, false, gemm_params(n, n, n, Xinv.p, ld, Si, ld, hs_p.p, ld, 1.0, 0.0, status.p),
+                        stream));
+    GPRX_CUDA_TRY(dgemm(false, true, gemm_params(n, n, n, hs_p.p, ld, Xinv.p, ld, Si, ld, 1.0, 0.0, status.p),
+                        stream));
+  }
+  double* Sn = hs_s.p + (size_t)pk * nn;
+  GPRX_CUDA_TRY(dgemm(false, true, gemm_params(n, n, n, Xinv.p, ld, Xinv.p, ld, Sn, ld, noise(), 0.0, status.p),
+                      stream));
+  GPRX_CUDA_TRY(trmv_lower(Xinv.p, ld, n, alpha.p, hs_v.p + (size_t)pk * n, status.p, stream));
+  for (int i = 0; i < p; ++i)
+    for (int j = 0; j <= i; ++j) {
+      int blocks = 0;
+      GPRX_CUDA_TRY(dot_nn(hs_s.p + (size_t)i * nn, hs_s.p + (size_t)j * nn, ld, n, hs_part.p, &blocks, stream));
+      GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, 1, 1, hs_res.p + FRO + i * p + j, stream));
+      GPRX_CUDA_TRY(dot_dev(hs_v.p + (size_t)i * n, hs_v.p + (size_t)j * n, n, hs_res.p + VD + i * p + j, status.p,
+                            stream));
+    }
+  GPRX_CUDA_TRY(cudaMemcpyAsync(hs_res_h.p, hs_res.p, sizeof(double) * nres, cudaMemcpyDeviceToHost, stream));
+  DevStatus ds;
+  if ((st = read_status(&ds)) != GPRX_OK) return st;
+  if (ds.code != GPRX_OK) return status_to_error(ds, jitter, n, GPRX_STAGE_FIT);
+  const double* r = hs_res_h.p;
+  const double s2 = noise();
+  std::vector<double> h((size_t)p * p, 0.0);
+  for (int i = 0; i < pk; ++i)
+    for (int j = i; j < pk; ++j) h[(size_t)i * p + j] = h[(size_t)j * p + i] = -0.5 * r[SEC + i * HESS_MAX_PARAMS + (j - i)];
+  h[(size_t)pk * p + pk] = -0.5 * s2 * (r[AA] - r[TR]);
+  for (int i = 0; i < p; ++i)
+    for (int j = 0; j <= i; ++j) {
+      const double sc = (i == pk ? s2 : 1.0) * (j == pk ? s2 : 1.0);
+      const double add = -0.5 * r[FRO + i * p + j] + sc * r[VD + i * p + j];
+      h[(size_t)i * p + j] += add;
+      if (i != j) h[(size_t)j * p + i] += add;
+    }
+  for (size_t e = 0; e < h.size(); ++e)
+    if (!std::isfinite(h[e])) return set_error(GPRX_NOT_CONVERGED, "non-finite Hessian entry");
+  std::copy(h.begin(), h.end(), out);
+  return GPRX_OK;
 }
 
 gprx_status ExactState::nlml(double* out) {

@@ -180,6 +180,11 @@ gprx_status gprx_exact_factor(gprx_exact* h);
  * src/gpr/exact_fit.rs:319-341).  `grad` may be NULL (value only). */
 gprx_status gprx_exact_eval(gprx_exact* h, const double* params, uint64_t p,
                             double* nlml, double* grad);
+/* Hessian of the NLML at `params`, row-major p × p into `out`
+ * (FittedGpr::hessian_into, src/gpr/fitted.rs:665; ExactFit::hessian_into_fit,
+ * src/gpr/exact_fit.rs:443-637).  Leaves the model at `params` as
+ * gprx_exact_eval with a gradient does. */
+gprx_status gprx_exact_hessian(gprx_exact* h, const double* params, uint64_t p, double* out);
 /* NLML of the current factor (GprCore::neg_log_marginal_likelihood, src/gpr/shared.rs:245-260). */
 gprx_status gprx_exact_nlml(gprx_exact* h, double* nlml);
 /* jitter j the current factor took (ExactFit factor_jitter). */

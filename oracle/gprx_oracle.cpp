@@ -488,6 +488,99 @@ uint64_t rng_next(Rng& r) {
   return result;
 }
 
+// Value, gradient and Hessian (in the log parameters, dense over all np
+// kernel parameters) of node idx at one pair.  A Sum adds its children's
+// triples; a Product folds them with (f, g, H)·(c, gc, Hc) = (f c,
+// f gc + c g, f Hc + c H + g gcᵀ + gc gᵀ).  Leaf second derivatives
+// (u = r²/ℓ², u_f = Δ_f²/ℓ_f², φ = π r / p, s = sin φ, c = cos φ):
+//   constant k = e^θ: ∂ = ∂² = k;  rbf: ∂ = k u, ∂² = k (u² − 2u);
+//   rbf_ard: ∂_f = k u_f, ∂_fg = k u_f u_g − 2 δ_fg k u_f;
+//   periodic (a = 4 s²/ℓ², b = 4 s c φ/ℓ²): ∂_ℓ = k a, ∂_p = k b,
+//   ∂_ℓℓ = k (a² − 2a), ∂_ℓp = k b (a − 2),
+//   ∂_pp = k (b² + 4 (φ² (s² − c²) − s c φ)/ℓ²).
+// These are the second-order kernel walks of CompiledKernel::hess_gram
+// (src/kernel/compiled/, used by src/gpr/exact_fit.rs:583-610).
+void node_vgh(const Tree& t, int idx, const double* x1, int64_t s1, const double* x2, int64_t s2, int d,
+              double& f, std::vector<double>& g, std::vector<double>& h) {
+  const int np = t.n_params;
+  const Node& nd = t.nodes[idx];
+  g.assign(np, 0.0);
+  h.assign((size_t)np * np, 0.0);
+  if (nd.kind == SUM || nd.kind == PRODUCT) {
+    f = nd.kind == SUM ? 0.0 : 1.0;
+    double c;
+    std::vector<double> gc, hc;
+    for (int ch : nd.children) {
+      node_vgh(t, ch, x1, s1, x2, s2, d, c, gc, hc);
+      if (nd.kind == SUM) {
+        f += c;
+        for (int a = 0; a < np; ++a) g[a] += gc[a];
+        for (size_t e = 0; e < h.size(); ++e) h[e] += hc[e];
+      } else {
+        for (int a = 0; a < np; ++a)
+          for (int b = 0; b < np; ++b)
+            h[(size_t)a * np + b] = f * hc[(size_t)a * np + b] + c * h[(size_t)a * np + b] + g[a] * gc[b] +
+                                    gc[a] * g[b];
+        for (int a = 0; a < np; ++a) g[a] = f * gc[a] + c * g[a];
+        f *= c;
+      }
+    }
+    return;
+  }
+  const double* th = t.theta.data() + nd.param;
+  const int p0 = nd.param;
+  double r2 = 0.0;
+  for (int q = 0; q < d; ++q) { double df = x1[q * s1] - x2[q * s2]; r2 += df * df; }
+  switch (nd.kind) {
+    case CONSTANT:
+      f = std::exp(th[0]);
+      g[p0] = f;
+      h[(size_t)p0 * np + p0] = f;
+      return;
+    case RBF: {
+      double ell = std::exp(th[0]);
+      double u = r2 / (ell * ell);
+      f = std::exp(-0.5 * u);
+      g[p0] = f * u;
+      h[(size_t)p0 * np + p0] = f * (u * u - 2.0 * u);
+      return;
+    }
+    case RBF_ARD: {
+      std::vector<double> u(d);
+      double q = 0.0;
+      for (int a = 0; a < d; ++a) {
+        double ell = std::exp(th[a]);
+        double df = (x1[a * s1] - x2[a * s2]) / ell;
+        u[a] = df * df;
+        q += u[a];
+      }
+      f = std::exp(-0.5 * q);
+      for (int a = 0; a < d; ++a) {
+        g[p0 + a] = f * u[a];
+        for (int b = 0; b < d; ++b)
+          h[(size_t)(p0 + a) * np + p0 + b] = f * u[a] * u[b] - (a == b ? 2.0 * f * u[a] : 0.0);
+      }
+      return;
+    }
+    case PERIODIC: {
+      double r = std::sqrt(std::max(r2, 0.0));
+      double ell = std::exp(th[0]), per = std::exp(th[1]);
+      double inv = 1.0 / (ell * ell);
+      double phi = M_PI * r / per;
+      double sn = std::sin(phi), cs = std::cos(phi);
+      f = std::exp(-2.0 * sn * sn * inv);
+      double a = 4.0 * sn * sn * inv, b = 4.0 * sn * cs * phi * inv;
+      g[p0] = f * a;
+      g[p0 + 1] = f * b;
+      h[(size_t)p0 * np + p0] = f * (a * a - 2.0 * a);
+      h[(size_t)p0 * np + p0 + 1] = h[(size_t)(p0 + 1) * np + p0] = f * b * (a - 2.0);
+      h[(size_t)(p0 + 1) * np + p0 + 1] = f * (b * b + 4.0 * inv * (phi * phi * (sn * sn - cs * cs) - sn * cs * phi));
+      return;
+    }
+  }
+  f = NAN;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -662,6 +755,74 @@ int orc_exact_loo(const int32_t* nodes, int n_nodes, const double* params, int n
     double obs = 1.0 / q;
     var[i] = kind == 1 ? obs : std::max(obs - noise, 0.0);
   }
+  return 0;
+}
+
+// Hessian of the NLML at params, row-major p × p (ExactFit::fill_hessian_from_factor
+// and add_first_order, src/gpr/exact_fit.rs:483-579):
+//   H_ij = −½ Σ_{a≥b} c_ab W_ab ∂²A_ab/∂θ_i∂θ_j − ½ ⟨S_i, S_j⟩_F + v_iᵀ v_j,
+// W = ααᵀ − A⁻¹, c = 1 on the diagonal and 2 off it, S_i = L⁻¹ A_i L⁻ᵀ,
+// v_i = L⁻¹ A_i α, A_i = ∂K/∂θ_i or σn² I for the noise (whose second
+// derivative is σn² I, and 0 mixed with a kernel parameter).
+int orc_exact_hessian(const int32_t* nodes, int n_nodes, const double* params, int n_params, const double* x,
+                      int64_t n, int d, const double* y, int jitter_kind, double jitter_initial, double jitter_mult,
+                      int jitter_retries, double jitter_max, double* hess) {
+  Tree t;
+  const int nk = n_params - 1, np = n_params;
+  if (!build_tree(t, nodes, n_nodes, params, nk)) return 3;
+  const double noise = std::exp(params[nk]);
+  Factor f;
+  double last_j = 0.0;
+  int st = factor_exact(t, x, n, d, y, noise,
+                        retry_jitters(jitter_kind, jitter_initial, jitter_mult, jitter_retries, jitter_max),
+                        f, &last_j);
+  if (st != 0) return st;
+  Mat kinv((size_t)n * n, 0.0);
+  llt_inverse(f.l.data(), n, n, kinv.data(), n);
+  // dK/dθ_i (full, one n×n per kernel parameter) and the second-order sum
+  std::vector<Mat> da(np, Mat((size_t)n * n, 0.0));
+  std::vector<double> sec((size_t)np * np, 0.0);
+  std::vector<double> g, h;
+  double kv;
+  for (int64_t b = 0; b < n; ++b)
+    for (int64_t a = b; a < n; ++a) {
+      node_vgh(t, 0, x + a, n, x + b, n, d, kv, g, h);
+      const double w = f.alpha[a] * f.alpha[b] - AT(kinv, n, a, b);
+      const double cw = a == b ? w : 2.0 * w;
+      for (int i = 0; i < nk; ++i) {
+        AT(da[i], n, a, b) = AT(da[i], n, b, a) = g[i];
+        for (int j = 0; j < nk; ++j) sec[(size_t)i * np + j] += cw * h[(size_t)i * nk + j];
+      }
+    }
+  double trw = 0.0;
+  for (int64_t a = 0; a < n; ++a) trw += f.alpha[a] * f.alpha[a] - AT(kinv, n, a, a);
+  sec[(size_t)nk * np + nk] = noise * trw;
+  for (int64_t a = 0; a < n; ++a) AT(da[nk], n, a, a) = noise;
+  // S_i = L⁻¹ A_i L⁻ᵀ (two triangular solves) and v_i = L⁻¹ A_i α
+  std::vector<Mat> sm(np);
+  std::vector<std::vector<double>> vv(np, std::vector<double>(n, 0.0));
+  for (int i = 0; i < np; ++i) {
+    for (int64_t a = 0; a < n; ++a) {
+      double acc = 0.0;
+      for (int64_t b = 0; b < n; ++b) acc += AT(da[i], n, a, b) * f.alpha[b];
+      vv[i][a] = acc;
+    }
+    trsm_lower(f.l.data(), n, n, vv[i].data(), 1, n);
+    Mat m = da[i];
+    trsm_lower(f.l.data(), n, n, m.data(), n, n);
+    Mat mt((size_t)n * n);
+    for (int64_t a = 0; a < n; ++a)
+      for (int64_t b = 0; b < n; ++b) AT(mt, n, a, b) = AT(m, n, b, a);
+    trsm_lower(f.l.data(), n, n, mt.data(), n, n);
+    sm[i] = std::move(mt);
+  }
+  for (int i = 0; i < np; ++i)
+    for (int j = 0; j < np; ++j) {
+      double fro = 0.0, vd = 0.0;
+      for (size_t e = 0; e < (size_t)n * n; ++e) fro += sm[i][e] * sm[j][e];
+      for (int64_t a = 0; a < n; ++a) vd += vv[i][a] * vv[j][a];
+      hess[(size_t)i * np + j] = -0.5 * sec[(size_t)i * np + j] - 0.5 * fro + vd;
+    }
   return 0;
 }
 

@@ -35,6 +35,8 @@ def lib():
     L = C.CDLL(ORACLE_SO)
     L.orc_exact_eval.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D, C.c_int, C.c_double,
                                  C.c_double, C.c_int, C.c_double, D, D, D, D]
+    L.orc_exact_hessian.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D, C.c_int, C.c_double,
+                                    C.c_double, C.c_int, C.c_double, D]
     L.orc_exact_predict.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D, C.c_int, C.c_double,
                                     C.c_double, C.c_int, C.c_double, D, C.c_int64, C.c_int, D, D]
     L.orc_exact_loo.argtypes = [I32, C.c_int, D, C.c_int, D, C.c_int64, C.c_int, D, C.c_int, C.c_double,
@@ -117,6 +119,19 @@ def exact_eval(nodes, params, x, n, d, y, grad=True, jitter=FIXED):
     if st != 0:
         raise OracleError(st)
     return nl[0], g, a, ju[0]
+
+
+def exact_hessian(nodes, params, x, n, d, y, jitter=FIXED):
+    """Analytic NLML Hessian, p × p."""
+    L = lib()
+    nd = _nodes(nodes)
+    p = _f(params)
+    h = np.zeros(len(p) * len(p))
+    st = L.orc_exact_hessian(_ptr(nd, I32), len(nd) // 2, _ptr(p), len(p), _ptr(_f(x)), n, d, _ptr(_f(y)), *jitter,
+                             _ptr(h))
+    if st != 0:
+        raise OracleError(st)
+    return h.reshape(len(p), len(p))
 
 
 def exact_loo(nodes, params, x, n, d, y, kind, jitter=FIXED):
