@@ -307,7 +307,8 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
 // −½ ⟨ααᵀ − K⁻¹, ∂²K/∂θ_i∂θ_j⟩ over the lower triangle (weight 2 off the
 // diagonal), the first-order part −½ ⟨S_i, S_j⟩_F + v_iᵀ v_j with
 // S_i = L⁻¹ A_i L⁻ᵀ and v_i = L⁻¹ A_i α (A_i = ∂K/∂θ_i, or σn² I for the
-// noise).  out is row-major p × p.
+// noise), evaluated as −½ tr(T_i T_j) + u_iᵀ A⁻¹ u_j with T_i = A⁻¹ A_i and
+// u_i = A_i α: one n³ product per parameter.  out is row-major p × p.
 gprx_status ExactState::hessian(const double* params, double* out) {
   const int p = num_params(), pk = kern.n_params;
   if (online) return set_error(GPRX_INVALID_CONFIG, "an online model takes no hyperparameter evaluation");
@@ -318,10 +319,11 @@ gprx_status ExactState::hessian(const double* params, double* out) {
   const size_t nn = (size_t)ld * n;
   const int SEC = 0, TR = HESS_MAX_PARAMS * HESS_MAX_PARAMS, AA = TR + 1, FRO = TR + 2, VD = FRO + p * p;
   const int nres = VD + p * p;
-  if (hs_s.ensure(nn * p) || hs_p.ensure(nn) || hs_v.ensure((size_t)n * (p + 1)) ||
+  if (hs_s.ensure(nn * std::max(pk, 1)) || hs_p.ensure(nn) || hs_d.ensure(nn) || hs_v.ensure((size_t)2 * n * p) ||
       hs_part.ensure((size_t)HESS_MAX_BLOCKS * HESS_MAX_PARAMS) || hs_res.ensure(nres)) {
     hs_s.reset();
     hs_p.reset();
+    hs_d.reset();
     return set_error(GPRX_OUT_OF_MEMORY, "device allocation of the Hessian scratch failed");
   }
   GPRX_CUDA_TRY(hs_res_h.ensure(nres));
@@ -345,35 +347,59 @@ gprx_status ExactState::hessian(const double* params, double* out) {
   }
   GPRX_CUDA_TRY(trace_dev(A.p, ld, n, hs_res.p + TR, stream));
   GPRX_CUDA_TRY(dot_dev(alpha.p, alpha.p, n, hs_res.p + AA, status.p, stream));
-  // first-order part: S_i in hs_s (slot i), v_i in column i of hs_v; the
-  // noise's v (column pk) is L⁻¹ α, scaled by σn² on the host
-  double* u = hs_v.p + (size_t)p * n;
-  for (int i = 0; i < pk; ++i) {
-    double* Si = hs_s.p + (size_t)i * nn;
-    GPRX_CUDA_TRY(fill_deriv(kern, hm, i, x.p, cap, n, Si, ld, stream));
-    GPRX_CUDA_TRY(gemv_t(Si, ld, n, n, false, alpha.p, u, status.p, stream));
-    GPRX_CUDA_TRY(trmv_lower(Xinv.p, ld, n, u, hs_v.p + (size_t)i * n, status.p, stream));
-    GPRX_CUDA_TRY(dgemm(false, false, gemm_params(n, n, n, Xinv.p, ld, Si, ld, hs_p.p, ld, 1.0, 0.0, status.p),
-                        stream));
-    GPRX_CUDA_TRY(dgemm(false, true, gemm_params(n, n, n, hs_p.p, ld, Xinv.p, ld, Si, ld, 1.0, 0.0, status.p),
-                        stream));
+  // first-order part with M = A⁻¹ (both triangles, hs_p) and T_i = M A_i:
+  // ⟨S_i, S_j⟩ = tr(T_i T_j) and v_iᵀ v_j = u_iᵀ M u_j with u_i = A_i α.  The
+  // noise's T is σn² M and its u is σn² α: both scaled on the host.
+  double* Mf = hs_p.p;
+  double* D = hs_d.p;
+  double* U = hs_v.p;                   // n × p
+  double* Q = hs_v.p + (size_t)n * p;   // n × p: M u_j
+  GPRX_CUDA_TRY(symmetrize(A.p, ld, n, Mf, ld, stream));
+  const bool emu = use_emu();
+  EmuWork ew;
+  EmuOperand ea;
+  if (emu) {
+    // the mixed form emulates the n³ products T_i = M A_i on the int8 tensor cores
+    if ((st = ensure_emu()) != GPRX_OK) return st;
+    ew.sa = emu_sa.p; ew.sb = emu_sb.p; ew.ea = emu_ea.p; ew.eb = emu_eb.p; ew.ma = emu_ma.p; ew.mb = emu_mb.p;
+    ew.err = emu_err.p;
+    ew.S = 7;
+    GPRX_CUDA_TRY(cudaMemsetAsync(emu_err.p, 0, sizeof(int), stream));
+    ea = ew.op_a(n, n);
+    GPRX_CUDA_TRY(emu_slice(Mf, ld, false, ea, stream));
   }
-  double* Sn = hs_s.p + (size_t)pk * nn;
-  GPRX_CUDA_TRY(dgemm(false, true, gemm_params(n, n, n, Xinv.p, ld, Xinv.p, ld, Sn, ld, noise(), 0.0, status.p),
-                      stream));
-  GPRX_CUDA_TRY(trmv_lower(Xinv.p, ld, n, alpha.p, hs_v.p + (size_t)pk * n, status.p, stream));
+  for (int i = 0; i < pk; ++i) {
+    double* Ti = hs_s.p + (size_t)i * nn;
+    GPRX_CUDA_TRY(fill_deriv(kern, hm, i, x.p, cap, n, D, ld, stream));
+    GPRX_CUDA_TRY(gemv_t(D, ld, n, n, false, alpha.p, U + (size_t)i * n, status.p, stream));
+    if (emu) {
+      EmuOperand eb = ew.op_b(n, n);
+      GPRX_CUDA_TRY(emu_slice(D, ld, true, eb, stream));
+      GPRX_CUDA_TRY(emu_gemm(ea, eb, Ti, ld, 1.0, 0.0, false, 0, 0, 0, ew.err, stream));
+    } else {
+      GPRX_CUDA_TRY(dgemm(false, false, gemm_params(n, n, n, Mf, ld, D, ld, Ti, ld, 1.0, 0.0, status.p), stream));
+    }
+  }
+  GPRX_CUDA_TRY(cudaMemcpyAsync(U + (size_t)pk * n, alpha.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+  GPRX_CUDA_TRY(dgemm(false, false, gemm_params(n, p, n, Mf, ld, U, n, Q, n, 1.0, 0.0, status.p), stream));
   for (int i = 0; i < p; ++i)
     for (int j = 0; j <= i; ++j) {
       int blocks = 0;
-      GPRX_CUDA_TRY(dot_nn(hs_s.p + (size_t)i * nn, hs_s.p + (size_t)j * nn, ld, n, hs_part.p, &blocks, stream));
+      if (i < pk)
+        GPRX_CUDA_TRY(dot_nt(hs_s.p + (size_t)i * nn, hs_s.p + (size_t)j * nn, ld, n, hs_part.p, &blocks, stream));
+      else if (j < pk)
+        GPRX_CUDA_TRY(dot_nn(hs_s.p + (size_t)j * nn, Mf, ld, n, hs_part.p, &blocks, stream));
+      else
+        GPRX_CUDA_TRY(dot_nn(Mf, Mf, ld, n, hs_part.p, &blocks, stream));
       GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, 1, 1, hs_res.p + FRO + i * p + j, stream));
-      GPRX_CUDA_TRY(dot_dev(hs_v.p + (size_t)i * n, hs_v.p + (size_t)j * n, n, hs_res.p + VD + i * p + j, status.p,
-                            stream));
+      GPRX_CUDA_TRY(dot_dev(U + (size_t)i * n, Q + (size_t)j * n, n, hs_res.p + VD + i * p + j, status.p, stream));
     }
+  if (emu) GPRX_CUDA_TRY(cudaMemcpyAsync(emu_err_h.p, emu_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
   GPRX_CUDA_TRY(cudaMemcpyAsync(hs_res_h.p, hs_res.p, sizeof(double) * nres, cudaMemcpyDeviceToHost, stream));
   DevStatus ds;
   if ((st = read_status(&ds)) != GPRX_OK) return st;
   if (ds.code != GPRX_OK) return status_to_error(ds, jitter, n, GPRX_STAGE_FIT);
+  if (use_emu() && *emu_err_h.p != 0) return set_error(GPRX_TIMEOUT, "an emulated product's bounded wait ran out");
   const double* r = hs_res_h.p;
   const double s2 = noise();
   std::vector<double> h((size_t)p * p, 0.0);
@@ -383,7 +409,7 @@ gprx_status ExactState::hessian(const double* params, double* out) {
   for (int i = 0; i < p; ++i)
     for (int j = 0; j <= i; ++j) {
       const double sc = (i == pk ? s2 : 1.0) * (j == pk ? s2 : 1.0);
-      const double add = -0.5 * r[FRO + i * p + j] + sc * r[VD + i * p + j];
+      const double add = sc * (-0.5 * r[FRO + i * p + j] + r[VD + i * p + j]);
       h[(size_t)i * p + j] += add;
       if (i != j) h[(size_t)j * p + i] += add;
     }

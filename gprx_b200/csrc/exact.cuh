@@ -87,7 +87,7 @@ struct ExactState {
   gprx_status eval(const double* params, double* nlml, double* grad);
   gprx_status nlml(double* out);
   // Hessian of the NLML at params (row-major p × p)
-  DevBuf<double> hs_s, hs_p, hs_v, hs_part, hs_res;
+  DevBuf<double> hs_s, hs_p, hs_d, hs_v, hs_part, hs_res;
   HostPinned<double> hs_res_h;
   gprx_status hessian(const double* params, double* out);
   gprx_status predict(const double* xs, uint64_t q, int kind, double* mean, double* var);

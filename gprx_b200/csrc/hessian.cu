@@ -243,6 +243,47 @@ __global__ void __launch_bounds__(256) dot_nn_kernel(const double* X, const doub
   if (threadIdx.x == 0) partials[blockIdx.x] = s;
 }
 
+// Σ_{a,b < n} X(a,b) Y(b,a): 32×32 tiles, Y's tile staged transposed in
+// shared memory so that both reads are coalesced.  One partial per block.
+__global__ void __launch_bounds__(256) dot_nt_kernel(const double* X, const double* Y, long long ld, int n,
+                                                     double* partials) {
+  __shared__ double ys[32][33];
+  __shared__ double red[32];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int nt = (n + 31) / 32;
+  const long long ntiles = (long long)nt * nt;
+  double acc = 0.0;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int r0 = (int)(t % nt) * 32, c0 = (int)(t / nt) * 32;
+    __syncthreads();
+    // ys[a][b] = Y(c0 + b, r0 + a)
+    for (int yy = ty; yy < 32; yy += 8) {
+      const int b = c0 + tx, a = r0 + yy;
+      ys[yy][tx] = (a < n && b < n) ? Y[b + (long long)a * ld] : 0.0;
+    }
+    __syncthreads();
+    const int a = r0 + tx;
+    if (a < n)
+      for (int yy = ty; yy < 32; yy += 8) {
+        const int b = c0 + yy;
+        if (b < n) acc = fma(X[a + (long long)b * ld], ys[tx][yy], acc);
+      }
+  }
+  const double s = block_sum(acc, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// M(a, b) = M(b, a) = L(max(a,b), min(a,b)): the full symmetric matrix from
+// a lower triangle.
+__global__ void symmetrize_kernel(const double* Lw, long long ldl, int n, double* M, long long ldm) {
+  const long long total = (long long)n * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int a = (int)(e % n), b = (int)(e / n);
+    M[a + (long long)b * ldm] = a >= b ? Lw[a + (long long)b * ldl] : Lw[b + (long long)a * ldl];
+  }
+}
+
 // out[q] = Σ_b partials[b·stride + q] for q < nq (fixed order).
 __global__ void reduce_slots_kernel(const double* partials, int blocks, int stride, int nq, double* out) {
   for (int q = threadIdx.x; q < nq; q += blockDim.x) {
@@ -305,6 +346,21 @@ cudaError_t dot_nn(const double* X, const double* Y, long long ld, int n, double
   const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)n * n + 255) / 256, HESS_MAX_BLOCKS));
   *blocks_out = grid;
   GPRX_LAUNCH(dot_nn_kernel, grid, 256, 0, s, X, Y, ld, n, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t dot_nt(const double* X, const double* Y, long long ld, int n, double* partials, int* blocks_out,
+                   cudaStream_t s) {
+  const long long nt = (n + 31) / 32;
+  const int grid = (int)std::max<long long>(1, std::min<long long>(nt * nt, HESS_MAX_BLOCKS));
+  *blocks_out = grid;
+  GPRX_LAUNCH(dot_nt_kernel, grid, 256, 0, s, X, Y, ld, n, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t symmetrize(const double* Lw, long long ldl, int n, double* M, long long ldm, cudaStream_t s) {
+  const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)n * n + 255) / 256, 148 * 8));
+  GPRX_LAUNCH(symmetrize_kernel, grid, 256, 0, s, Lw, ldl, n, M, ldm);
   return cudaGetLastError();
 }
 

@@ -32,6 +32,11 @@ cudaError_t fill_deriv(const HostKernel& k, const HessMap& hm, int i, const doub
 cudaError_t dot_nn(const double* X, const double* Y, long long ld, int n, double* partials, int* blocks_out,
                    cudaStream_t s);
 
+// Partial sums of Σ_{a,b} X(a,b) Y(b,a) = tr(X Y) over the n×n blocks (ld).
+cudaError_t dot_nt(const double* X, const double* Y, long long ld, int n, double* partials, int* blocks_out,
+                   cudaStream_t s);
+// M (n×n, ldm, both triangles) from the lower triangle of Lw (ldl).
+cudaError_t symmetrize(const double* Lw, long long ldl, int n, double* M, long long ldm, cudaStream_t s);
 // out[q] = Σ_b partials[b·stride + q], q < nq.
 cudaError_t reduce_slots(const double* partials, int blocks, int stride, int nq, double* out, cudaStream_t s);
 // out = trace of M (n×n, ld).
