@@ -9,14 +9,15 @@ in log space (100 perturbations, cycled).  All data are synthetic, from the
 restated SeededRng; no dataset is read.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
-                    [--workload all|exact|batched] [--impl ours|reference]
+                    [--workload all|exact|batched|serving|sgpr|hessian] [--impl ours|reference]
 
 The default line's value is the mixed form (FP64 products emulated on the
 int8 tensor cores); the plain FP64 form is timed beside it ("fp64") with the
 largest error of the mixed results against it.  The other workloads ride in
 the same line: "batched" (4096 ragged exact fits), "serving" (a Poisson
 request stream, p50/p99) and "sgpr" (VFE at n = 10⁶, m = 1024); each is also
-available alone through --workload.
+available alone through --workload.  "hessian" (alone only) times the NLML
+Hessian (gprx_exact_hessian) at the exact workload's θ in both forms.
 
 N > 1 runs N independent replicas (one exact problem does not shard; launched
 by torchrun, one rank per GPU); `value` is the aggregate evals/s over ranks,
@@ -568,7 +569,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-evals", type=int, default=0,
                     help="only factor once and run this many evaluations (for an ncu launch list), no JSON line")
-    ap.add_argument("--workload", default="all", choices=["all", "exact", "batched", "serving", "sgpr"],
+    ap.add_argument("--workload", default="all", choices=["all", "exact", "batched", "serving", "sgpr", "hessian"],
                     help="all: the exact line with the batched measurement as its 'batched' key")
     ap.add_argument("--batch-problems", type=int, default=BATCH_P)
     ap.add_argument("--serve-rates", default="2,4,8", help="arrival rates (requests/s) of the serving sweep")
@@ -667,6 +668,47 @@ def main():
         return
 
     spec = gx.ConstantKernel(CONST) * gx.RbfArdKernel(list(np.exp(theta[1:1 + d])))
+
+    if args.workload == "hessian":
+        # NLML Hessians (gprx_exact_hessian) at the exact workload's θ
+        forms = ["fp64"] if args.precision == "fp64" else ["mixed"] if args.precision == "mixed" else ["fp64", "mixed"]
+        per = {}
+        for f in forms:
+            prec = gx.Precision.Fp64 if f == "fp64" else gx.Precision.Mixed
+            model = gx.Gpr(spec, gx.GaussianLikelihood(NOISE), precision=prec, device=local) \
+                .with_optimizer(gx.Fixed()).factor(x, n, d, y)
+            if args.profile_evals > 0:
+                for i in range(args.profile_evals):
+                    model.hessian(theta)
+                torch.cuda.synchronize()
+                return
+            stream = torch.cuda.ExternalStream(model.stream_ptr(), device=dev)
+            for i in range(warm):
+                model.hessian(theta)
+            torch.cuda.synchronize()
+            l0 = L.lib().gprx_launch_count()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for i in range(args.steps):
+                h = model.hessian(theta)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            per[f] = {"ms_per_hessian": ms, "launches_per_hessian": (L.lib().gprx_launch_count() - l0) / args.steps,
+                      "h00": float(h[0, 0])}
+            del model
+            torch.cuda.empty_cache()
+        head = per["mixed"] if "mixed" in per else per["fp64"]
+        p = theta.size
+        print(json.dumps({
+            "metric": "NLML Hessians/s n=%d p=%d" % (n, p), "value": 1e3 / head["ms_per_hessian"],
+            "unit": "hessians/s", "n_gpus": 1, "steps": args.steps, "warmup": warm, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "exact_gpr_nlml_hessian_n%d_d%d_const_rbfard" % (n, d), "n": n, "d": d, "p": p},
+            "forms": per,
+            "work": "one evaluation with gradient, p - 1 products A^-1 dK/dθ_i of 2 n^3 flops, "
+                    "p - 1 second-order kernel walks over the n(n+1)/2 pairs"}), flush=True)
+        return
 
     def barrier():
         if dist is not None:
