@@ -29,6 +29,7 @@ from .api import (  # noqa: F401
     InvalidHyperparameter,
     KernelSpec,
     Lbfgs,
+    TrustRegion,
     LoadedGpr,
     PersistFailed,
     UnsupportedPersistVersion,

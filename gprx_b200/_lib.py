@@ -68,6 +68,12 @@ class LbfgsOptions(C.Structure):
                 ("interval_hi", C.c_double)]
 
 
+class TrustRegionOptions(C.Structure):
+    _fields_ = [("max_iterations", C.c_uint64), ("tolerance", C.c_double), ("initial_radius", C.c_double),
+                ("max_radius", C.c_double), ("restarts", C.c_int32), ("seed", C.c_uint64),
+                ("interval_lo", C.c_double), ("interval_hi", C.c_double)]
+
+
 class FitReport(C.Structure):
     _fields_ = [("nlml", C.c_double), ("iterations", C.c_uint64), ("evaluations", C.c_uint64),
                 ("grad_norm", C.c_double), ("converged", C.c_int32)]
@@ -104,6 +110,7 @@ _SIGS = {
     "gprx_options_default": (None, [C.POINTER(Options)]),
     "gprx_options_default_sparse": (None, [C.POINTER(Options)]),
     "gprx_lbfgs_options_default": (None, [C.POINTER(LbfgsOptions)]),
+    "gprx_trust_region_options_default": (None, [C.POINTER(TrustRegionOptions)]),
     "gprx_last_error": (C.c_int32, [C.POINTER(ErrorInfo)]),
     "gprx_launch_count": (C.c_uint64, []),
     "gprx_exact_create": (C.c_int32, [D, C.c_uint64, C.c_uint64, D, C.POINTER(KernelNode), C.c_int32, D, C.c_int32,
@@ -121,6 +128,8 @@ _SIGS = {
     "gprx_exact_predict": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
     "gprx_exact_alpha": (C.c_int32, [C.c_void_p, D, C.c_uint64]),
     "gprx_exact_fit": (C.c_int32, [C.c_void_p, C.POINTER(LbfgsOptions), C.POINTER(FitReport)]),
+    "gprx_exact_fit_trust_region": (C.c_int32, [C.c_void_p, C.POINTER(TrustRegionOptions), C.POINTER(FitReport)]),
+    "gprx_exact_value_gradient_hessian": (C.c_int32, [C.c_void_p, D, C.c_uint64, D, D, D]),
     "gprx_exact_stage_times": (C.c_int32, [C.c_void_p, D]),
     "gprx_exact_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "gprx_online_begin": (C.c_int32, [C.c_void_p]),

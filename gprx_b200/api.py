@@ -330,6 +330,59 @@ class Lbfgs:
         return o
 
 
+class TrustRegion:
+    """Trust region with the Steihaug subproblem over the analytic Hessian, in
+    logit coordinates (src/optimizer/trust_region.rs:19-130).  Exact models
+    only: the Sgpr Hessian is not part of this backend."""
+
+    def __init__(self, max_iterations=100, tolerance=math.sqrt(2.220446049250313e-16), initial_radius=1.0,
+                 max_radius=100.0, restarts=0, seed=0):
+        if not (math.isfinite(tolerance) and tolerance >= 0.0):
+            raise InvalidConfig("trust-region gradient tolerance must be finite and >= 0")
+        self._check_radii(initial_radius, max_radius)
+        self.max_iterations = int(max_iterations)
+        self.tolerance = float(tolerance)
+        self.initial_radius = float(initial_radius)
+        self.max_radius = float(max_radius)
+        self.restarts = int(restarts)
+        self.seed = int(seed)
+
+    @staticmethod
+    def _check_radii(initial_radius, max_radius):
+        if not (math.isfinite(initial_radius) and math.isfinite(max_radius) and initial_radius > 0.0
+                and initial_radius <= max_radius):
+            raise InvalidConfig("trust radii must satisfy 0 < initial <= max and be finite")
+
+    def with_max_iterations(self, n):
+        self.max_iterations = int(n)
+        return self
+
+    def with_tolerance(self, tol):
+        return TrustRegion(self.max_iterations, tol, self.initial_radius, self.max_radius, self.restarts, self.seed)
+
+    def with_radii(self, initial_radius, max_radius):
+        self._check_radii(initial_radius, max_radius)
+        self.initial_radius = float(initial_radius)
+        self.max_radius = float(max_radius)
+        return self
+
+    def with_restarts(self, n, seed):
+        self.restarts = int(n)
+        self.seed = int(seed)
+        return self
+
+    def _c(self):
+        o = L.TrustRegionOptions()
+        L.lib().gprx_trust_region_options_default(C.byref(o))
+        o.max_iterations = self.max_iterations
+        o.tolerance = self.tolerance
+        o.initial_radius = self.initial_radius
+        o.max_radius = self.max_radius
+        o.restarts = self.restarts
+        o.seed = self.seed
+        return o
+
+
 class Fixed:
     """No optimization: factor at the given θ (src/optimizer/mod.rs)."""
 
@@ -450,7 +503,10 @@ class Gpr:
             return f
         rep = L.FitReport()
         opt = self.optimizer._c()
-        check(L.lib().gprx_exact_fit(f._h, C.byref(opt), C.byref(rep)))
+        if isinstance(self.optimizer, TrustRegion):
+            check(L.lib().gprx_exact_fit_trust_region(f._h, C.byref(opt), C.byref(rep)))
+        else:
+            check(L.lib().gprx_exact_fit(f._h, C.byref(opt), C.byref(rep)))
         f.report = rep
         return f
 
@@ -499,6 +555,18 @@ class FittedGpr:
         v = np.zeros(1)
         check(L.lib().gprx_exact_eval(self._h, L.ptr(p), p.size, L.ptr(v), None))
         return float(v[0])
+
+    def value_gradient_hessian(self, params):
+        """NLML, gradient and Hessian of one evaluation at `params`
+        (TwiceDifferentiable::value_gradient_hessian_into, src/objective.rs:427)."""
+        p = L.f64(params)
+        if p.size != self.num_params():
+            raise ShapeMismatch("expected %d parameters" % self.num_params())
+        v = np.zeros(1)
+        g = np.zeros(p.size)
+        h = np.zeros(p.size * p.size)
+        check(L.lib().gprx_exact_value_gradient_hessian(self._h, L.ptr(p), p.size, L.ptr(v), L.ptr(g), L.ptr(h)))
+        return float(v[0]), g, h.reshape(p.size, p.size)
 
     def hessian(self, params):
         """Hessian of the NLML at `params`, p × p (FittedGpr::hessian_into,
@@ -685,6 +753,8 @@ class Sgpr:
         return f
 
     def fit(self, x, n_rows, n_cols, y, z, m):
+        if isinstance(self.optimizer, TrustRegion):
+            raise InvalidConfig("TrustRegion needs the Hessian, which this backend builds for exact models only")
         f = self._create(x, n_rows, n_cols, y, z, m)
         if isinstance(self.optimizer, Fixed):
             check(L.lib().gprx_sgpr_factor(f._h))

@@ -13,6 +13,7 @@
 #include "exact.cuh"
 #include "persist.h"
 #include "lbfgs.h"
+#include "trust_region.h"
 
 namespace gprx {
 
@@ -159,6 +160,99 @@ gprx_status fit_lbfgs(void* ctx, EvalFn eval, int p, const double* theta0, const
   return GPRX_OK;
 }
 
+// fit: trust region (host) over the joint value / gradient / Hessian
+gprx_status fit_trust_region(ExactState& s, int p, const double* theta0, const gprx_trust_region_options* o,
+                             gprx_fit_report* rep, std::vector<double>& best_theta) {
+  gprx_trust_region_options opt;
+  if (o) opt = *o;
+  else gprx_trust_region_options_default(&opt);
+  if (!(opt.interval_lo > 0.0) || !(opt.interval_hi > opt.interval_lo) || !std::isfinite(opt.interval_hi))
+    return set_error(GPRX_INVALID_CONFIG, "parameter interval must be 0 < lo < hi");
+  if (!(opt.tolerance >= 0.0) || !std::isfinite(opt.tolerance))
+    return set_error(GPRX_INVALID_CONFIG, "trust-region gradient tolerance must be finite and >= 0");
+  if (!(std::isfinite(opt.initial_radius) && std::isfinite(opt.max_radius) && opt.initial_radius > 0.0 &&
+        opt.initial_radius <= opt.max_radius))
+    return set_error(GPRX_INVALID_CONFIG, "trust radii must satisfy 0 < initial <= max and be finite");
+  LogitMap map;
+  map.init(opt.interval_lo, opt.interval_hi);
+  TrustRegionConfig cfg;
+  cfg.max_iterations = opt.max_iterations;
+  cfg.tol_grad = opt.tolerance;
+  cfg.initial_radius = opt.initial_radius;
+  cfg.max_radius = opt.max_radius;
+  std::vector<double> z0(p);
+  if (!map.from_log(theta0, p, z0.data())) return set_error(GPRX_INVALID_HYPERPARAMETER, "initial θ outside the interval");
+  std::vector<double> logt(p), jac(p), jac2(p), gl(p), hl((size_t)p * p);
+  gprx_status fatal = GPRX_OK, last = GPRX_OK;
+  // joint evaluation in z: g_z = J g, H_z = J H J + diag(g ∘ d²logθ/dz²)
+  // (chain_logit_hess, src/optimizer/logit.rs:139-157)
+  TrJointFn joint = [&](const double* z, double* f, double* g, double* h) -> bool {
+    if (fatal != GPRX_OK) return false;
+    map.to_log(z, p, logt.data(), jac.data());
+    map.second(z, p, jac2.data());
+    gprx_status st = s.hessian(logt.data(), hl.data(), f, gl.data());
+    if (st == GPRX_CUDA_ERROR || st == GPRX_OUT_OF_MEMORY || st == GPRX_TIMEOUT) {
+      fatal = st;
+      return false;
+    }
+    if (st != GPRX_OK || !std::isfinite(*f)) {
+      last = st != GPRX_OK ? st : GPRX_NOT_CONVERGED;
+      return false;
+    }
+    for (int i = 0; i < p; ++i) {
+      for (int j = 0; j < p; ++j) h[(size_t)i * p + j] = hl[(size_t)i * p + j] * jac[i] * jac[j];
+      h[(size_t)i * p + i] += gl[i] * jac2[i];
+      g[i] = gl[i] * jac[i];
+    }
+    return true;
+  };
+  gprx_rng rng;
+  gprx_rng_seed(&rng, opt.seed);
+  TrustRegionResult best;
+  bool have = false;
+  uint64_t total_evals = 0;
+  for (int run = 0; run <= opt.restarts; ++run) {
+    std::vector<double> zs(p);
+    if (run == 0) {
+      zs = z0;
+    } else {
+      for (int i = 0; i < p; ++i) {
+        double u = gprx_rng_unit(&rng);
+        const double eps = 1.0 / 9007199254740992.0;
+        u = std::min(std::max(u, eps), 1.0 - eps);
+        double lt = map.ln_lo + u * (map.ln_hi - map.ln_lo);
+        map.from_log(&lt, 1, &zs[i]);
+      }
+    }
+    TrustRegionResult r;
+    const bool ok = trust_region_run(cfg, zs, joint, r);
+    total_evals += r.evaluations;
+    if (fatal != GPRX_OK) return fatal;
+    if (!ok) {
+      // the first start must be evaluable (its error is the caller's); a
+      // restart that cannot start is skipped (src/optimizer/mod.rs:218-224)
+      if (run == 0) return set_error(last != GPRX_OK ? last : GPRX_NOT_CONVERGED, "the initial θ cannot be evaluated");
+      continue;
+    }
+    if (!have || r.best_value < best.best_value) {
+      best = r;
+      have = true;
+    }
+  }
+  if (!have || !(best.best_value < BARRIER_COST))
+    return set_error(GPRX_NOT_CONVERGED, "no evaluable point was found");
+  best_theta.resize(p);
+  map.to_log(best.best.data(), p, best_theta.data(), nullptr);
+  if (rep) {
+    rep->nlml = best.best_value;
+    rep->iterations = best.iterations;
+    rep->evaluations = total_evals;
+    rep->grad_norm = best.grad_norm;
+    rep->converged = best.converged ? 1 : 0;
+  }
+  return GPRX_OK;
+}
+
 static gprx_status exact_eval_cb(void* ctx, const double* lt, double* f, double* g) {
   return ((ExactState*)ctx)->eval(lt, f, g);
 }
@@ -202,6 +296,18 @@ void gprx_lbfgs_options_default(gprx_lbfgs_options* o) {
   o->max_iterations = 100;
   o->tolerance = 1.4901161193847656e-08;
   o->history_size = 10;
+  o->restarts = 0;
+  o->seed = 0;
+  o->interval_lo = 1e-5;
+  o->interval_hi = 1e5;
+}
+
+void gprx_trust_region_options_default(gprx_trust_region_options* o) {
+  if (!o) return;
+  o->max_iterations = 100;
+  o->tolerance = 1.4901161193847656e-08;
+  o->initial_radius = 1.0;
+  o->max_radius = 100.0;
   o->restarts = 0;
   o->seed = 0;
   o->interval_lo = 1e-5;
@@ -297,6 +403,14 @@ gprx_status gprx_exact_hessian(gprx_exact* h, const double* params, uint64_t p, 
   if (!params || !out) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (p != (uint64_t)h->s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
   return h->s.hessian(params, out);
+}
+
+gprx_status gprx_exact_value_gradient_hessian(gprx_exact* h, const double* params, uint64_t p, double* nlml,
+                                              double* grad, double* hess) {
+  CHECK_HANDLE(h);
+  if (!params || !nlml || !grad || !hess) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (p != (uint64_t)h->s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
+  return h->s.hessian(params, hess, nlml, grad);
 }
 
 gprx_status gprx_exact_nlml(gprx_exact* h, double* nlml) {
@@ -404,6 +518,28 @@ gprx_status gprx_exact_fit(gprx_exact* h, const gprx_lbfgs_options* opt, gprx_fi
     return st;
   }
   // commit at the optimizer's best θ and publish α (exact_fit.rs:743-773, shared.rs:203)
+  st = s.write_params(best.data());
+  if (st == GPRX_OK) st = s.factor_current();
+  if (st == GPRX_OK && report) st = s.nlml(&report->nlml);
+  return st;
+}
+
+gprx_status gprx_exact_fit_trust_region(gprx_exact* h, const gprx_trust_region_options* opt,
+                                        gprx_fit_report* report) {
+  CHECK_HANDLE(h);
+  ExactState& s = h->s;
+  if (s.online) return set_error(GPRX_INVALID_CONFIG, "an online model is not refitted");
+  int p = s.num_params();
+  std::vector<double> theta0(p), best;
+  s.get_params(theta0.data());
+  gprx_status st = fit_trust_region(s, p, theta0.data(), opt, report, best);
+  if (st != GPRX_OK) {
+    gprx_error_info saved = last_error();
+    s.write_params(theta0.data());
+    s.factor_current();
+    last_error() = saved;
+    return st;
+  }
   st = s.write_params(best.data());
   if (st == GPRX_OK) st = s.factor_current();
   if (st == GPRX_OK && report) st = s.nlml(&report->nlml);

@@ -309,13 +309,15 @@ gprx_status ExactState::eval(const double* params, double* nlml_out, double* gra
 // S_i = L⁻¹ A_i L⁻ᵀ and v_i = L⁻¹ A_i α (A_i = ∂K/∂θ_i, or σn² I for the
 // noise), evaluated as −½ tr(T_i T_j) + u_iᵀ A⁻¹ u_j with T_i = A⁻¹ A_i and
 // u_i = A_i α: one n³ product per parameter.  out is row-major p × p.
-gprx_status ExactState::hessian(const double* params, double* out) {
+gprx_status ExactState::hessian(const double* params, double* out, double* nlml_out, double* grad_out) {
   const int p = num_params(), pk = kern.n_params;
   if (online) return set_error(GPRX_INVALID_CONFIG, "an online model takes no hyperparameter evaluation");
   std::vector<double> g(p);
   double v = 0.0;
   gprx_status st = eval(params, &v, g.data());
   if (st != GPRX_OK) return st;
+  if (nlml_out) *nlml_out = v;
+  if (grad_out) std::copy(g.begin(), g.end(), grad_out);
   const size_t nn = (size_t)ld * n;
   const int SEC = 0, TR = HESS_MAX_PARAMS * HESS_MAX_PARAMS, AA = TR + 1, FRO = TR + 2, VD = FRO + p * p;
   const int nres = VD + p * p;

@@ -86,10 +86,11 @@ struct ExactState {
   gprx_status factor_current();
   gprx_status eval(const double* params, double* nlml, double* grad);
   gprx_status nlml(double* out);
-  // Hessian of the NLML at params (row-major p × p)
+  // Hessian of the NLML at params (row-major p × p); the value and the
+  // gradient of the same evaluation when nlml_out / grad_out are given
   DevBuf<double> hs_s, hs_p, hs_d, hs_v, hs_part, hs_res;
   HostPinned<double> hs_res_h;
-  gprx_status hessian(const double* params, double* out);
+  gprx_status hessian(const double* params, double* out, double* nlml_out = nullptr, double* grad_out = nullptr);
   gprx_status predict(const double* xs, uint64_t q, int kind, double* mean, double* var);
   // leave-one-out, query covariance and posterior draws from the resident factor
   DevBuf<double> covbuf, covl, covlinv, zbuf;

@@ -58,6 +58,15 @@ struct LogitMap {
       if (jac) jac[i] = span * u * (1.0 - u) / s;
     }
   }
+  // d²logθ/dz² (the chain rule's second-order term of the Hessian,
+  // src/optimizer/logit.rs:139-157)
+  GPRX_HD void second(const double* z, int n, double* d2) const {
+    const double s = scale(), span = ln_hi - ln_lo;
+    for (int i = 0; i < n; ++i) {
+      double u = sigmoid(z[i] / s);
+      d2[i] = span * u * (1.0 - u) * (1.0 - 2.0 * u) / (s * s);
+    }
+  }
   // log θ → z (fails when θ is outside the open interval)
   GPRX_HD bool from_log(const double* log_theta, int n, double* z) const {
     const double eps = 2.220446049250313e-16;

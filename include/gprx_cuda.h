@@ -132,6 +132,20 @@ typedef struct {
   double interval_hi;
 } gprx_lbfgs_options;
 
+/* TrustRegion settings (src/optimizer/trust_region.rs:32-51): ≤100
+ * iterations, gradient tolerance √ε, initial radius 1, maximum radius 100
+ * (logit coordinates), the same logit map as L-BFGS. */
+typedef struct {
+  uint64_t max_iterations;
+  double tolerance;
+  double initial_radius;  /* 0 < initial_radius <= max_radius < inf */
+  double max_radius;
+  int32_t restarts;       /* extra starts (0 = none) */
+  uint64_t seed;
+  double interval_lo;
+  double interval_hi;
+} gprx_trust_region_options;
+
 typedef struct {
   double nlml;
   uint64_t iterations;
@@ -147,6 +161,7 @@ int32_t gprx_abi_version(void);
 void gprx_options_default(gprx_options* opt);
 void gprx_options_default_sparse(gprx_options* opt);
 void gprx_lbfgs_options_default(gprx_lbfgs_options* opt);
+void gprx_trust_region_options_default(gprx_trust_region_options* opt);
 /* Details of the last failed call on this thread. */
 gprx_status gprx_last_error(gprx_error_info* out);
 /* Number of kernels this library launched since load (instrumentation). */
@@ -185,6 +200,11 @@ gprx_status gprx_exact_eval(gprx_exact* h, const double* params, uint64_t p,
  * src/gpr/exact_fit.rs:443-637).  Leaves the model at `params` as
  * gprx_exact_eval with a gradient does. */
 gprx_status gprx_exact_hessian(gprx_exact* h, const double* params, uint64_t p, double* out);
+/* NLML, gradient and Hessian of one evaluation at `params`
+ * (TwiceDifferentiable::value_gradient_hessian_into, src/objective.rs:427;
+ * ExactFit::value_gradient_hessian_into_fit, src/gpr/exact_fit.rs:468-482). */
+gprx_status gprx_exact_value_gradient_hessian(gprx_exact* h, const double* params, uint64_t p, double* nlml,
+                                              double* grad, double* hess);
 /* NLML of the current factor (GprCore::neg_log_marginal_likelihood, src/gpr/shared.rs:245-260). */
 gprx_status gprx_exact_nlml(gprx_exact* h, double* nlml);
 /* jitter j the current factor took (ExactFit factor_jitter). */
@@ -257,6 +277,11 @@ gprx_status gprx_exact_alpha(gprx_exact* h, double* out, uint64_t n);
 /* Gpr::fit with the default Lbfgs (src/gpr/trainer.rs:533-613, src/optimizer/lbfgs.rs:126-172):
  * optimizes θ, then refactors at the best θ and publishes α for predict. */
 gprx_status gprx_exact_fit(gprx_exact* h, const gprx_lbfgs_options* opt, gprx_fit_report* report);
+/* Gpr::fit with the TrustRegion optimizer (src/optimizer/trust_region.rs:143-258):
+ * trust region with the Steihaug subproblem over gprx_exact_value_gradient_hessian
+ * in logit coordinates, then the factor at the best θ.  NULL opt = defaults. */
+gprx_status gprx_exact_fit_trust_region(gprx_exact* h, const gprx_trust_region_options* opt,
+                                        gprx_fit_report* report);
 /* Per-stage device time of the last eval in milliseconds:
  * [fill, factor, inverse, gradient, total] (the reference's insert-stages idea). */
 gprx_status gprx_exact_stage_times(gprx_exact* h, double* out5);
