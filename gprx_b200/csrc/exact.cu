@@ -320,9 +320,11 @@ gprx_status ExactState::hessian(const double* params, double* out, double* nlml_
   if (grad_out) std::copy(g.begin(), g.end(), grad_out);
   const size_t nn = (size_t)ld * n;
   const int SEC = 0, TR = HESS_MAX_PARAMS * HESS_MAX_PARAMS, AA = TR + 1, FRO = TR + 2, VD = FRO + p * p;
-  const int nres = VD + p * p;
+  const int FUS = VD + p * p, TRF = FUS + HESS_FUSE_SLOTS;
+  const int nres = TRF + HESS_TRACE_SLOTS;
+  const bool fuse_second = pk <= HESS_FUSE_K, fuse_trace = p <= HESS_FUSE_P;
   if (hs_s.ensure(nn * std::max(pk, 1)) || hs_p.ensure(nn) || hs_d.ensure(nn) || hs_v.ensure((size_t)2 * n * p) ||
-      hs_part.ensure((size_t)HESS_MAX_BLOCKS * HESS_MAX_PARAMS) || hs_res.ensure(nres)) {
+      hs_part.ensure((size_t)HESS_MAX_BLOCKS * std::max(HESS_MAX_PARAMS, HESS_TRACE_SLOTS)) || hs_res.ensure(nres)) {
     hs_s.reset();
     hs_p.reset();
     hs_d.reset();
@@ -335,17 +337,27 @@ gprx_status ExactState::hessian(const double* params, double* out, double* nlml_
   for (int l = 0; l < kern.tree.n_leaves; ++l) {
     const KLeaf& lf = kern.tree.leaf[l];
     const int cnt = lf.kind == GPRX_LEAF_PERIODIC ? 2 : lf.kind == GPRX_LEAF_RBF_ARD ? kern.tree.d : 1;
+    unsigned tm = 0;
+    for (int t = 0; t < kern.tree.n_terms; ++t)
+      if ((kern.tree.term_mask[t] >> l) & 1u) tm |= 1u << t;
     for (int a = 0; a < cnt; ++a) {
       hm.leaf_of[lf.param + a] = l;
       hm.local_of[lf.param + a] = a;
+      hm.terms_of[lf.param + a] = tm;
     }
   }
-  // second-order part, one launch per row
-  for (int i = 0; i < pk; ++i) {
+  // second-order part: every row in one launch, or one launch per row
+  if (fuse_second && pk > 0) {
     int blocks = 0;
-    GPRX_CUDA_TRY(hess_second(kern, hm, i, x.p, cap, n, A.p, ld, alpha.p, hs_part.p, &blocks, stream));
-    GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, HESS_MAX_PARAMS, pk - i, hs_res.p + SEC + i * HESS_MAX_PARAMS,
-                               stream));
+    GPRX_CUDA_TRY(hess_second_all(kern, hm, x.p, cap, n, A.p, ld, alpha.p, hs_part.p, &blocks, stream));
+    GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, HESS_FUSE_SLOTS, HESS_FUSE_SLOTS, hs_res.p + FUS, stream));
+  } else {
+    for (int i = 0; i < pk; ++i) {
+      int blocks = 0;
+      GPRX_CUDA_TRY(hess_second(kern, hm, i, x.p, cap, n, A.p, ld, alpha.p, hs_part.p, &blocks, stream));
+      GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, HESS_MAX_PARAMS, pk - i, hs_res.p + SEC + i * HESS_MAX_PARAMS,
+                                 stream));
+    }
   }
   GPRX_CUDA_TRY(trace_dev(A.p, ld, n, hs_res.p + TR, stream));
   GPRX_CUDA_TRY(dot_dev(alpha.p, alpha.p, n, hs_res.p + AA, status.p, stream));
@@ -384,18 +396,28 @@ gprx_status ExactState::hessian(const double* params, double* out, double* nlml_
   }
   GPRX_CUDA_TRY(cudaMemcpyAsync(U + (size_t)pk * n, alpha.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
   GPRX_CUDA_TRY(dgemm(false, false, gemm_params(n, p, n, Mf, ld, U, n, Q, n, 1.0, 0.0, status.p), stream));
-  for (int i = 0; i < p; ++i)
-    for (int j = 0; j <= i; ++j) {
-      int blocks = 0;
-      if (i < pk)
-        GPRX_CUDA_TRY(dot_nt(hs_s.p + (size_t)i * nn, hs_s.p + (size_t)j * nn, ld, n, hs_part.p, &blocks, stream));
-      else if (j < pk)
-        GPRX_CUDA_TRY(dot_nn(hs_s.p + (size_t)j * nn, Mf, ld, n, hs_part.p, &blocks, stream));
-      else
-        GPRX_CUDA_TRY(dot_nn(Mf, Mf, ld, n, hs_part.p, &blocks, stream));
-      GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, 1, 1, hs_res.p + FRO + i * p + j, stream));
-      GPRX_CUDA_TRY(dot_dev(U + (size_t)i * n, Q + (size_t)j * n, n, hs_res.p + VD + i * p + j, status.p, stream));
-    }
+  // VD(i, j) = u_iᵀ (M u_j), p × p column-major
+  GPRX_CUDA_TRY(dgemm(true, false, gemm_params(p, p, n, U, n, Q, n, hs_res.p + VD, p, 1.0, 0.0, status.p), stream));
+  if (fuse_trace) {
+    HessMats mats{};
+    for (int i = 0; i < pk; ++i) mats.m[i] = hs_s.p + (size_t)i * nn;
+    mats.m[pk] = Mf;
+    int blocks = 0;
+    GPRX_CUDA_TRY(trace_products(mats, p, ld, n, hs_part.p, &blocks, stream));
+    GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, HESS_TRACE_SLOTS, HESS_TRACE_SLOTS, hs_res.p + TRF, stream));
+  } else {
+    for (int i = 0; i < p; ++i)
+      for (int j = 0; j <= i; ++j) {
+        int blocks = 0;
+        if (i < pk)
+          GPRX_CUDA_TRY(dot_nt(hs_s.p + (size_t)i * nn, hs_s.p + (size_t)j * nn, ld, n, hs_part.p, &blocks, stream));
+        else if (j < pk)
+          GPRX_CUDA_TRY(dot_nn(hs_s.p + (size_t)j * nn, Mf, ld, n, hs_part.p, &blocks, stream));
+        else
+          GPRX_CUDA_TRY(dot_nn(Mf, Mf, ld, n, hs_part.p, &blocks, stream));
+        GPRX_CUDA_TRY(reduce_slots(hs_part.p, blocks, 1, 1, hs_res.p + FRO + i * p + j, stream));
+      }
+  }
   if (emu) GPRX_CUDA_TRY(cudaMemcpyAsync(emu_err_h.p, emu_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
   GPRX_CUDA_TRY(cudaMemcpyAsync(hs_res_h.p, hs_res.p, sizeof(double) * nres, cudaMemcpyDeviceToHost, stream));
   DevStatus ds;
@@ -405,13 +427,20 @@ gprx_status ExactState::hessian(const double* params, double* out, double* nlml_
   const double* r = hs_res_h.p;
   const double s2 = noise();
   std::vector<double> h((size_t)p * p, 0.0);
+  // packed slots of the fused kernels: second-order (a ≤ b) row by row over
+  // HESS_FUSE_K columns, trace products (j ≤ i) row by row
+  auto sec = [&](int i, int j) {
+    if (!fuse_second) return r[SEC + i * HESS_MAX_PARAMS + (j - i)];
+    return r[FUS + i * HESS_FUSE_K - i * (i - 1) / 2 + (j - i)];
+  };
+  auto fro = [&](int i, int j) { return fuse_trace ? r[TRF + i * (i + 1) / 2 + j] : r[FRO + i * p + j]; };
   for (int i = 0; i < pk; ++i)
-    for (int j = i; j < pk; ++j) h[(size_t)i * p + j] = h[(size_t)j * p + i] = -0.5 * r[SEC + i * HESS_MAX_PARAMS + (j - i)];
+    for (int j = i; j < pk; ++j) h[(size_t)i * p + j] = h[(size_t)j * p + i] = -0.5 * sec(i, j);
   h[(size_t)pk * p + pk] = -0.5 * s2 * (r[AA] - r[TR]);
   for (int i = 0; i < p; ++i)
     for (int j = 0; j <= i; ++j) {
       const double sc = (i == pk ? s2 : 1.0) * (j == pk ? s2 : 1.0);
-      const double add = sc * (-0.5 * r[FRO + i * p + j] + r[VD + i * p + j]);
+      const double add = sc * (-0.5 * fro(i, j) + r[VD + i + j * p]);
       h[(size_t)i * p + j] += add;
       if (i != j) h[(size_t)j * p + i] += add;
     }

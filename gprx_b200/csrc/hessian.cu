@@ -183,6 +183,190 @@ __global__ void __launch_bounds__(HESS_THREADS) hess_second_kernel(KTree t, Hess
   }
 }
 
+// All rows at once.  With T_t the value of term t at the pair and, for
+// parameter a of leaf l_a, ∂v_l/∂θ_a = v_l f_a (f = u for rbf, u_f for
+// rbf_ard, 1 for constant, a / b for periodic), the pair's second derivative
+// is Σ_{t ∋ l_a, l_b} T_t (f_a f_b + [l_a = l_b] ∂f_b/∂θ_a), with ∂f_b/∂θ_a =
+// −2 f_b for the length-scale-type parameters, 0 across ARD dimensions and for
+// a constant, and 4 (φ² (s² − c²) − s c φ)/ℓ² for a periodic leaf's period
+// twice.
+template <int ARD_D>
+__global__ void __launch_bounds__(HESS_THREADS) hess_all_kernel(KTree t, HessMap hm, const double* x, long long ldx,
+                                                                int n, const double* kinv, long long ld,
+                                                                const double* alpha, double* partials) {
+  constexpr int K = HESS_FUSE_K, NS = HESS_FUSE_SLOTS;
+  __shared__ double xi[GPRX_MAX_DIM * HT];
+  __shared__ double xj[GPRX_MAX_DIM * HT];
+  __shared__ double red[HESS_THREADS / 32][NS];
+  const int np = hm.n_par;
+  double acc[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) acc[q] = 0.0;
+  const int nt = (n + HT - 1) / HT;
+  const long long ntiles = (long long)nt * (nt + 1) / 2;
+  for (long long idx = blockIdx.x; idx < ntiles; idx += gridDim.x) {
+    int ti, tj;
+    hess_lower_tile(idx, ti, tj);
+    const int i0 = ti * HT, j0 = tj * HT;
+    __syncthreads();
+    for (int e = threadIdx.x; e < t.d * HT; e += blockDim.x) {
+      const int r = e % HT, f = e / HT;
+      xi[f * HT + r] = (i0 + r < n) ? x[(i0 + r) + (long long)f * ldx] : 0.0;
+      xj[f * HT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * ldx] : 0.0;
+    }
+    __syncthreads();
+    const int r = threadIdx.x % HT;
+    const int pa = i0 + r;
+    for (int c = threadIdx.x / HT; c < HT; c += HESS_THREADS / HT) {
+      const int pb = j0 + c;
+      if (pa >= n || pb >= n || pa < pb) continue;
+      const double w = fma(alpha[pa], alpha[pb], -kinv[pa + (long long)pb * ld]);
+      const double cw = pa == pb ? w : 2.0 * w;
+      PairGeom g;
+      double v[KT_MAX_LEAVES];
+      pair_setup<ARD_D>(t, xi + r, xj + c, g, v);
+      // term values
+      double tv[KT_MAX_TERMS];
+#pragma unroll
+      for (int tt = 0; tt < KT_MAX_TERMS; ++tt) {
+        double pr = tt < t.n_terms ? 1.0 : 0.0;
+#pragma unroll
+        for (int l = 0; l < KT_MAX_LEAVES; ++l)
+          if (tt < t.n_terms && l < t.n_leaves && ((t.term_mask[tt] >> l) & 1u)) pr *= v[l];
+        tv[tt] = pr;
+      }
+      // per-parameter factors f_a and the periodic period's own term e_a
+      double fa[K], ea[K];
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+        fa[a] = 0.0;
+        ea[a] = 0.0;
+        if (a < np) {
+          const KLeaf& lf = t.leaf[hm.leaf_of[a]];
+          const int loc = hm.local_of[a];
+          switch (lf.kind) {
+            case GPRX_LEAF_CONSTANT:
+              fa[a] = 1.0;
+              break;
+            case GPRX_LEAF_RBF:
+              fa[a] = 2.0 * lf.c0 * g.r2;
+              break;
+            case GPRX_LEAF_RBF_ARD:
+              fa[a] = g.dx[loc] * g.dx[loc] * t.inv_ell2[loc];
+              break;
+            case GPRX_LEAF_PERIODIC: {
+              const double phi = lf.c0 * sqrt(fmax(g.r2, 0.0));
+              double sn, cs;
+              sincos(phi, &sn, &cs);
+              fa[a] = loc == 0 ? 4.0 * sn * sn * lf.c1 : 4.0 * sn * cs * phi * lf.c1;
+              ea[a] = 4.0 * lf.c1 * (phi * phi * (sn * sn - cs * cs) - sn * cs * phi);
+              break;
+            }
+          }
+        }
+      }
+      int q = 0;
+#pragma unroll
+      for (int a = 0; a < K; ++a) {
+#pragma unroll
+        for (int b = a; b < K; ++b, ++q) {
+          if (b >= np) continue;
+          const unsigned m = hm.terms_of[a] & hm.terms_of[b];
+          double sum = 0.0;
+#pragma unroll
+          for (int tt = 0; tt < KT_MAX_TERMS; ++tt)
+            if ((m >> tt) & 1u) sum += tv[tt];
+          double dd = fa[a] * fa[b];
+          if (hm.leaf_of[a] == hm.leaf_of[b]) {
+            const int kind = t.leaf[hm.leaf_of[a]].kind;
+            if (kind == GPRX_LEAF_RBF || kind == GPRX_LEAF_RBF_ARD) {
+              if (a == b) dd -= 2.0 * fa[a];
+            } else if (kind == GPRX_LEAF_PERIODIC) {
+              dd += (hm.local_of[a] == 1 && hm.local_of[b] == 1) ? ea[b] : -2.0 * fa[b];
+            }
+          }
+          acc[q] = fma(cw, sum * dd, acc[q]);
+        }
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const double vs = warp_sum(acc[q]);
+    if (lane == 0) red[warp][q] = vs;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < NS; q += blockDim.x) {
+    double tot = 0.0;
+    for (int wq = 0; wq < HESS_THREADS / 32; ++wq) tot += red[wq][q];
+    partials[(long long)blockIdx.x * NS + q] = tot;
+  }
+}
+
+// tr(M_i M_j) for every j ≤ i < np in one pass: per 32×32 tile each thread
+// reads its element of every M_i and, through shared memory, the transposed
+// element of every M_j.
+__global__ void __launch_bounds__(256) trace_products_kernel(HessMats mats, int np, long long ld, int n,
+                                                             double* partials) {
+  constexpr int P = HESS_FUSE_P, NS = HESS_TRACE_SLOTS;
+  extern __shared__ double tsm[];  // P tiles of 32 × 33, then the reduction
+  double* red = tsm + P * 32 * 33;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int nt = (n + 31) / 32;
+  const long long ntiles = (long long)nt * nt;
+  double acc[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) acc[q] = 0.0;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int r0 = (int)(t % nt) * 32, c0 = (int)(t / nt) * 32;
+    __syncthreads();
+    // tile j: ys[a][b] = M_j(c0 + b, r0 + a)
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      if (j < np) {
+        for (int yy = ty; yy < 32; yy += 8) {
+          const int b = c0 + tx, a = r0 + yy;
+          tsm[j * 32 * 33 + yy * 33 + tx] = (a < n && b < n) ? mats.m[j][b + (long long)a * ld] : 0.0;
+        }
+      }
+    }
+    __syncthreads();
+    const int a = r0 + tx;
+    if (a < n) {
+      for (int yy = ty; yy < 32; yy += 8) {
+        const int b = c0 + yy;
+        if (b >= n) continue;
+        double xv[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) xv[i] = i < np ? mats.m[i][a + (long long)b * ld] : 0.0;
+        int q = 0;
+#pragma unroll
+        for (int i = 0; i < P; ++i) {
+#pragma unroll
+          for (int j = 0; j <= i; ++j, ++q) {
+            if (i < np) acc[q] = fma(xv[i], tsm[j * 32 * 33 + tx * 33 + yy], acc[q]);
+          }
+        }
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    const double vs = warp_sum(acc[q]);
+    if (lane == 0) red[warp * NS + q] = vs;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < NS; q += blockDim.x) {
+    double tot = 0.0;
+    for (int wq = 0; wq < 8; ++wq) tot += red[wq * NS + q];
+    partials[(long long)blockIdx.x * NS + q] = tot;
+  }
+}
+
 // out (full n×n, ld) = ∂K/∂θ_i
 template <int ARD_D>
 __global__ void __launch_bounds__(HESS_THREADS) fill_deriv_kernel(KTree t, HessMap hm, int i, const double* x,
@@ -322,6 +506,43 @@ cudaError_t hess_second(const HostKernel& k, const HessMap& hm, int i, const dou
     default: GPRX_HS(32); break;
   }
 #undef GPRX_HS
+  return cudaGetLastError();
+}
+
+cudaError_t hess_second_all(const HostKernel& k, const HessMap& hm, const double* x, long long ldx, int n,
+                            const double* kinv, long long ld, const double* alpha, double* partials, int* blocks_out,
+                            cudaStream_t s) {
+  if (hm.n_par > HESS_FUSE_K) return cudaErrorInvalidValue;
+  const int nt = (n + HT - 1) / HT;
+  const int grid = hess_grid((long long)nt * (nt + 1) / 2);
+  *blocks_out = grid;
+#define GPRX_HA(D) \
+  GPRX_LAUNCH(hess_all_kernel<D>, grid, HESS_THREADS, 0, s, k.tree, hm, x, ldx, n, kinv, ld, alpha, partials)
+  switch (k.ard_d) {
+    case 0: GPRX_HA(0); break;
+    case 4: GPRX_HA(4); break;
+    case 8: GPRX_HA(8); break;
+    case 16: GPRX_HA(16); break;
+    default: GPRX_HA(32); break;
+  }
+#undef GPRX_HA
+  return cudaGetLastError();
+}
+
+cudaError_t trace_products(const HessMats& mats, int np, long long ld, int n, double* partials, int* blocks_out,
+                           cudaStream_t s) {
+  if (np > HESS_FUSE_P) return cudaErrorInvalidValue;
+  const long long nt = (n + 31) / 32;
+  const int grid = (int)std::max<long long>(1, std::min<long long>(nt * nt, HESS_MAX_BLOCKS));
+  *blocks_out = grid;
+  const size_t smem = sizeof(double) * ((size_t)HESS_FUSE_P * 32 * 33 + 8 * HESS_TRACE_SLOTS);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(trace_products_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  GPRX_LAUNCH(trace_products_kernel, grid, 256, smem, s, mats, np, ld, n, partials);
   return cudaGetLastError();
 }
 

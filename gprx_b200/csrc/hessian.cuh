@@ -17,6 +17,16 @@ struct HessMap {
   int n_par;
   int leaf_of[HESS_MAX_PARAMS];
   int local_of[HESS_MAX_PARAMS];
+  unsigned terms_of[HESS_MAX_PARAMS];  // bit t: term t holds the parameter's leaf
+};
+
+// All rows of the second-order part in one launch when the kernel has at
+// most HESS_FUSE_K parameters; the trace products of at most HESS_FUSE_P
+// matrices in one pass.
+constexpr int HESS_FUSE_K = 10;
+constexpr int HESS_FUSE_P = 11;
+struct HessMats {
+  const double* m[HESS_FUSE_P];
 };
 
 // Partial sums (HESS_MAX_PARAMS per block, blocks in *blocks_out) of
@@ -25,6 +35,19 @@ struct HessMap {
 cudaError_t hess_second(const HostKernel& k, const HessMap& hm, int i, const double* x, long long ldx, int n,
                         const double* kinv, long long ld, const double* alpha, double* partials, int* blocks_out,
                         cudaStream_t s);
+// Partial sums (HESS_FUSE_K·(HESS_FUSE_K+1)/2 per block, packed upper
+// triangle row by row) of the same contraction for every i ≤ j < n_par in one
+// launch; n_par ≤ HESS_FUSE_K.
+constexpr int HESS_FUSE_SLOTS = HESS_FUSE_K * (HESS_FUSE_K + 1) / 2;
+cudaError_t hess_second_all(const HostKernel& k, const HessMap& hm, const double* x, long long ldx, int n,
+                            const double* kinv, long long ld, const double* alpha, double* partials, int* blocks_out,
+                            cudaStream_t s);
+// Partial sums (HESS_FUSE_P·(HESS_FUSE_P+1)/2 per block, packed lower
+// triangle row by row) of tr(M_i M_j) = Σ_ab M_i(a,b) M_j(b,a) for every
+// j ≤ i < np, np ≤ HESS_FUSE_P, in one pass over the matrices.
+constexpr int HESS_TRACE_SLOTS = HESS_FUSE_P * (HESS_FUSE_P + 1) / 2;
+cudaError_t trace_products(const HessMats& mats, int np, long long ld, int n, double* partials, int* blocks_out,
+                           cudaStream_t s);
 // out (n×n, both triangles, ld) = ∂K/∂θ_i.
 cudaError_t fill_deriv(const HostKernel& k, const HessMap& hm, int i, const double* x, long long ldx, int n,
                        double* out, long long ld, cudaStream_t s);

@@ -816,12 +816,13 @@ int orc_exact_hessian(const int32_t* nodes, int n_nodes, const double* params, i
     trsm_lower(f.l.data(), n, n, mt.data(), n, n);
     sm[i] = std::move(mt);
   }
+  // upper triangle (i ≤ j), mirrored
   for (int i = 0; i < np; ++i)
-    for (int j = 0; j < np; ++j) {
+    for (int j = i; j < np; ++j) {
       double fro = 0.0, vd = 0.0;
       for (size_t e = 0; e < (size_t)n * n; ++e) fro += sm[i][e] * sm[j][e];
       for (int64_t a = 0; a < n; ++a) vd += vv[i][a] * vv[j][a];
-      hess[(size_t)i * np + j] = -0.5 * sec[(size_t)i * np + j] - 0.5 * fro + vd;
+      hess[(size_t)i * np + j] = hess[(size_t)j * np + i] = -0.5 * sec[(size_t)i * np + j] - 0.5 * fro + vd;
     }
   return 0;
 }

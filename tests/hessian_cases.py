@@ -54,5 +54,6 @@ def ard_case(n, d=3, seed=5):
     # C × ARD + Rbf × C (a periodic leaf on a distance in d > 1 is not
     # positive definite in general, so it stays in the 1-d case)
     nodes = [[1, 2], [2, 2], [12, 0], [11, d], [2, 2], [10, 0], [12, 0]]
-    params = [LN(1.2)] + [LN(v) for v in (0.9, 1.4, 2.2)[:d]] + [LN(2.5), LN(0.3), LN(0.05)]
-    return ("ard%d" % n, nodes, params, x, y)
+    ls = [(0.9, 1.4, 2.2)[f % 3] * (1.0 + 0.5 * (f // 3)) for f in range(d)]
+    params = [LN(1.2)] + [LN(v) for v in ls] + [LN(2.5), LN(0.3), LN(0.05)]
+    return ("ard%d" % n if d == 3 else "ard%d_d%d" % (n, d), nodes, params, x, y)

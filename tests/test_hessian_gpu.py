@@ -1,7 +1,7 @@
 """gprx_exact_hessian against the oracle's analytic Hessian (itself pinned on
 finite differences of the golden-pinned gradient): the reference's own cases
 (src/gpr/tests.rs:1394-1493), a periodic product and seeded ARD cases up to
-n = 1100.  FP64: |a − e| ≤ 1e-9 · max(max|e|, 1) per entry; the mixed form
+n = 1100, with up to 15 kernel parameters.  FP64: |a − e| ≤ 1e-9 · max(max|e|, 1) per entry; the mixed form
 (emulated products from n = 1024): 1e-6 on the same scale.  A second call
 gives the same bits (src/gpr/tests.rs:1440-1442), and the model is left at
 the evaluated θ like a gradient evaluation.
@@ -18,7 +18,9 @@ from hessian_cases import ard_case, col, periodic_case, reference_cases
 
 pytestmark = pytest.mark.gpu
 
-CASES = reference_cases() + [periodic_case(), ard_case(65), ard_case(300)]
+# ard*_d12 has 15 kernel parameters: the per-row second-order launches and the
+# pairwise trace products (the others take the single-launch forms)
+CASES = reference_cases() + [periodic_case(), ard_case(65), ard_case(300), ard_case(97, d=12)]
 
 
 def fitted(nodes, params, x, y, precision=gx.Precision.Fp64):

@@ -11,7 +11,7 @@ import pytest
 import oracle_lib as O
 from hessian_cases import ard_case, col, periodic_case, reference_cases
 
-CASES = reference_cases() + [periodic_case(), ard_case(12)]
+CASES = reference_cases() + [periodic_case(), ard_case(12), ard_case(20, d=5)]
 
 
 def fd_hessian(nodes, params, x, y, h=1e-5):
