@@ -370,19 +370,21 @@ gprx_status gprx_exact_set_params(gprx_exact* h, const double* params, uint64_t 
   CHECK_HANDLE(h);
   ExactState& s = h->s;
   if (!params || p != (uint64_t)s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
-  if (s.online) return set_error(GPRX_INVALID_CONFIG, "an online model keeps its θ");
+  // an online model goes through an LLT view (OnlineGpr::set_params, src/gpr/online.rs:659)
   std::vector<double> prev(p);
   s.get_params(prev.data());
-  gprx_status st = s.write_params(params);
-  if (st != GPRX_OK) return st;
-  st = s.factor_current();
-  if (st != GPRX_OK) {
-    gprx_error_info saved = last_error();
-    s.write_params(prev.data());
-    s.factor_current();
-    last_error() = saved;
-  }
-  return st;
+  return s.with_llt_view([&]() -> gprx_status {
+    gprx_status st = s.write_params(params);
+    if (st != GPRX_OK) return st;
+    st = s.factor_current();
+    if (st != GPRX_OK) {
+      gprx_error_info saved = last_error();
+      s.write_params(prev.data());
+      s.factor_current();
+      last_error() = saved;
+    }
+    return st;
+  });
 }
 
 gprx_status gprx_exact_factor(gprx_exact* h) {
@@ -395,14 +397,14 @@ gprx_status gprx_exact_eval(gprx_exact* h, const double* params, uint64_t p, dou
   CHECK_HANDLE(h);
   if (!params || !nlml) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (p != (uint64_t)h->s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
-  return h->s.eval(params, nlml, grad);
+  return h->s.with_llt_view([&] { return h->s.eval(params, nlml, grad); });
 }
 
 gprx_status gprx_exact_hessian(gprx_exact* h, const double* params, uint64_t p, double* out) {
   CHECK_HANDLE(h);
   if (!params || !out) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (p != (uint64_t)h->s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
-  return h->s.hessian(params, out);
+  return h->s.with_llt_view([&] { return h->s.hessian(params, out); });
 }
 
 gprx_status gprx_exact_value_gradient_hessian(gprx_exact* h, const double* params, uint64_t p, double* nlml,
@@ -410,7 +412,7 @@ gprx_status gprx_exact_value_gradient_hessian(gprx_exact* h, const double* param
   CHECK_HANDLE(h);
   if (!params || !nlml || !grad || !hess) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (p != (uint64_t)h->s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
-  return h->s.hessian(params, hess, nlml, grad);
+  return h->s.with_llt_view([&] { return h->s.hessian(params, hess, nlml, grad); });
 }
 
 gprx_status gprx_exact_nlml(gprx_exact* h, double* nlml) {

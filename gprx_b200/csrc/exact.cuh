@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cmath>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -109,6 +110,12 @@ struct ExactState {
 
   // online (LDLT)
   gprx_status online_begin();
+  // Runs op (θ writes, evaluations, Hessians) on an online model through a
+  // plain LLT: afterwards A is the LDLT at the model's θ again, and a failed
+  // op leaves the LDLT, α and the jitter as they were
+  // (with_llt_view, src/gpr/online.rs:1151-1185).
+  DevBuf<double> ldlt_keep, alpha_keep;
+  gprx_status with_llt_view(const std::function<gprx_status()>& op);
   gprx_status online_insert(const double* xnew, double ynew, uint64_t* id);
   gprx_status online_delete(uint64_t id);
   gprx_status online_alpha();

@@ -165,6 +165,44 @@ gprx_status ExactState::online_begin() {
   return GPRX_OK;
 }
 
+gprx_status ExactState::with_llt_view(const std::function<gprx_status()>& op) {
+  if (!online) return op();
+  // keep the LDLT: a failed operation leaves the online model as it was
+  const size_t keep = (size_t)ld * n;
+  if (ldlt_keep.ensure(std::max<size_t>(keep, 1)) != cudaSuccess || alpha_keep.ensure(std::max(n, 1)) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "device allocation of the online factor copy failed");
+  GPRX_CUDA_TRY(cudaMemcpyAsync(ldlt_keep.p, A.p, sizeof(double) * keep, cudaMemcpyDeviceToDevice, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(alpha_keep.p, alpha.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+  const bool alpha_was_ok = alpha_ok;
+  const double jitter_was = jitter;
+  std::vector<double> theta_was(num_params());
+  get_params(theta_was.data());
+  online = false;
+  factor_ok = false;
+  linv_ok = false;
+  alpha_ok = false;
+  gprx_status st = op();
+  if (st == GPRX_OK && (!factor_ok || !alpha_ok)) st = factor_current();
+  if (st == GPRX_OK) {
+    llt_to_ldlt_kernel<<<n, 256, 0, stream>>>(A.p, ld, n);
+    count_launch();
+    GPRX_CUDA_TRY(cudaGetLastError());
+  } else {
+    gprx_error_info saved = last_error();
+    write_params(theta_was.data());
+    GPRX_CUDA_TRY(cudaMemcpyAsync(A.p, ldlt_keep.p, sizeof(double) * keep, cudaMemcpyDeviceToDevice, stream));
+    GPRX_CUDA_TRY(cudaMemcpyAsync(alpha.p, alpha_keep.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+    alpha_ok = alpha_was_ok;
+    jitter = jitter_was;
+    last_error() = saved;
+  }
+  online = true;
+  factor_ok = false;
+  linv_ok = false;
+  GPRX_CUDA_TRY(cudaStreamSynchronize(stream));
+  return st;
+}
+
 gprx_status ExactState::grow(int needed) {
   if (needed <= cap) return GPRX_OK;
   int new_cap = std::max(needed, std::max(cap, 1) * 2);

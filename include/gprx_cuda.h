@@ -186,7 +186,12 @@ uint64_t gprx_exact_num_params(const gprx_exact* h);
 /* log θ of the kernel then log σn² (Gpr::get_params). */
 gprx_status gprx_exact_get_params(gprx_exact* h, double* out, uint64_t p);
 /* Writes θ and factors A = K + σn² I (+ jitter retries) at it; on failure
- * the previous θ and its factor are restored (src/gpr/exact_fit.rs:196-206). */
+ * the previous θ and its factor are restored (src/gpr/exact_fit.rs:196-206).
+ * On an online model this, gprx_exact_eval, gprx_exact_hessian and
+ * gprx_exact_value_gradient_hessian run through an LLT of the current points
+ * and leave the model online at the new θ; a failure leaves its LDLT, α and θ
+ * unchanged (OnlineGpr::set_params / value_and_gradient_into / hessian_into,
+ * src/gpr/online.rs:659-697, with_llt_view :1151-1185). */
 gprx_status gprx_exact_set_params(gprx_exact* h, const double* params, uint64_t p);
 /* Factors at the stored θ (Gpr<Fixed>::factor → factor_written_k_with_policy,
  * src/gpr/factor.rs:515-542). */
