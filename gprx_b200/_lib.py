@@ -123,6 +123,7 @@ _SIGS = {
     "gprx_exact_factor": (C.c_int32, [C.c_void_p]),
     "gprx_exact_eval": (C.c_int32, [C.c_void_p, D, C.c_uint64, D, D]),
     "gprx_exact_hessian": (C.c_int32, [C.c_void_p, D, C.c_uint64, D]),
+    "gprx_exact_data": (C.c_int32, [C.c_void_p, D, D]),
     "gprx_exact_nlml": (C.c_int32, [C.c_void_p, D]),
     "gprx_exact_factor_jitter": (C.c_int32, [C.c_void_p, D]),
     "gprx_exact_predict": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),

@@ -487,12 +487,13 @@ class Gpr:
         opt = self._options()
         check(L.lib().gprx_exact_create(L.ptr(x), n_rows, n_cols, L.ptr(y), nodes, nn, L.ptr(theta), theta.size,
                                         C.byref(opt), C.byref(h)))
-        return FittedGpr(h, n_cols, self.kernel.copy())
+        return FittedGpr(h, n_cols, self.kernel.copy(), self)
 
     def factor(self, x, n_rows, n_cols, y):
         """Factor at the given θ (Gpr<Fixed>::factor)."""
         f = self._create(x, n_rows, n_cols, y)
         check(L.lib().gprx_exact_factor(f._h))
+        f.optimizer = Fixed()
         return f
 
     def fit(self, x, n_rows, n_cols, y):
@@ -514,11 +515,69 @@ class Gpr:
 class FittedGpr:
     """A factored exact GPR (src/gpr/fitted.rs)."""
 
-    def __init__(self, handle, d, kernel):
+    def __init__(self, handle, d, kernel, trainer=None):
         self._h = handle
         self.d = d
         self.kernel = kernel
         self.report = None
+        self._trainer = trainer
+        self.optimizer = trainer.optimizer if trainer is not None else Fixed()
+
+    def x(self):
+        """Training features, column-major n × d (FittedGpr::x, src/gpr/fitted.rs:1091)."""
+        n = self.n()
+        x = np.zeros(n * self.d)
+        y = np.zeros(n)
+        check(L.lib().gprx_exact_data(self._h, L.ptr(x), L.ptr(y)))
+        return x
+
+    def y(self):
+        """Training targets (FittedGpr::y, src/gpr/fitted.rs:324)."""
+        n = self.n()
+        x = np.zeros(n * self.d)
+        y = np.zeros(n)
+        check(L.lib().gprx_exact_data(self._h, L.ptr(x), L.ptr(y)))
+        return y
+
+    def likelihood(self):
+        """The Gaussian likelihood at the current σn² (src/gpr/fitted.rs:308)."""
+        return GaussianLikelihood(math.exp(self.get_params()[-1]))
+
+    def to_kernel(self):
+        """The kernel at the current θ (FittedGpr::kernel, src/gpr/fitted.rs:836)."""
+        k = self.kernel.copy()
+        k.set_params(list(self.get_params()[:-1]))
+        return k
+
+    def with_optimizer(self, optimizer):
+        """Replaces the optimizer used by a later refit (src/gpr/fitted.rs:328)."""
+        self.optimizer = optimizer
+        return self
+
+    def refit(self):
+        """Re-runs the stored optimizer on the stored data from the current θ;
+        with Fixed, refactors at the current θ (src/gpr/fitted.rs:1146-1166)."""
+        if isinstance(self.optimizer, Fixed):
+            check(L.lib().gprx_exact_factor(self._h))
+            return
+        rep = L.FitReport()
+        opt = self.optimizer._c()
+        if isinstance(self.optimizer, TrustRegion):
+            check(L.lib().gprx_exact_fit_trust_region(self._h, C.byref(opt), C.byref(rep)))
+        else:
+            check(L.lib().gprx_exact_fit(self._h, C.byref(opt), C.byref(rep)))
+        self.report = rep
+
+    def into_trainer(self):
+        """Drops the factor and the data; returns a trainer with the current
+        kernel, likelihood, optimizer and options (src/gpr/fitted.rs:291-306)."""
+        t = self._trainer
+        g = Gpr(self.to_kernel(), self.likelihood(), self.optimizer,
+                t.precision if t is not None else Precision.Fp64, t.device if t is not None else 0)
+        if t is not None:
+            g.jitter = t.jitter
+        self.__del__()
+        return g
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -685,7 +744,8 @@ class FittedGpr:
     def into_online(self):
         """FittedGpr::into_online (src/gpr/fitted.rs:757-765)."""
         check(L.lib().gprx_online_begin(self._h))
-        on = OnlineGpr(self._h, self.d, self.kernel)
+        on = OnlineGpr(self._h, self.d, self.kernel, self._trainer)
+        on.optimizer = self.optimizer
         self._h = None
         return on
 

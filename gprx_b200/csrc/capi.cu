@@ -366,6 +366,17 @@ gprx_status gprx_exact_get_params(gprx_exact* h, double* out, uint64_t p) {
   return GPRX_OK;
 }
 
+gprx_status gprx_exact_data(gprx_exact* h, double* x_out, double* y_out) {
+  CHECK_HANDLE(h);
+  ExactState& s = h->s;
+  if (!x_out || !y_out) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  GPRX_CUDA_TRY(cudaMemcpy2DAsync(x_out, sizeof(double) * s.n, s.x.p, sizeof(double) * s.cap, sizeof(double) * s.n, s.d,
+                                  cudaMemcpyDeviceToHost, s.stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(y_out, s.y.p, sizeof(double) * s.n, cudaMemcpyDeviceToHost, s.stream));
+  GPRX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+  return GPRX_OK;
+}
+
 gprx_status gprx_exact_set_params(gprx_exact* h, const double* params, uint64_t p) {
   CHECK_HANDLE(h);
   ExactState& s = h->s;

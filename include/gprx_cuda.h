@@ -185,6 +185,10 @@ gprx_status gprx_exact_set_data(gprx_exact* h, const double* x, const double* y)
 uint64_t gprx_exact_num_params(const gprx_exact* h);
 /* log θ of the kernel then log σn² (Gpr::get_params). */
 gprx_status gprx_exact_get_params(gprx_exact* h, double* out, uint64_t p);
+/* The training points in buffer order: x (n×d, column-major, n rows) and y
+ * (n), host memory (FittedGpr::x / y, src/gpr/fitted.rs:1091,324; an online
+ * model's current points, in the order of gprx_online_point_ids). */
+gprx_status gprx_exact_data(gprx_exact* h, double* x_out, double* y_out);
 /* Writes θ and factors A = K + σn² I (+ jitter retries) at it; on failure
  * the previous θ and its factor are restored (src/gpr/exact_fit.rs:196-206).
  * On an online model this, gprx_exact_eval, gprx_exact_hessian and
