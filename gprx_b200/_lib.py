@@ -147,6 +147,8 @@ _SIGS = {
     "gprx_sgpr_eval": (C.c_int32, [C.c_void_p, D, C.c_uint64, D, D]),
     "gprx_sgpr_nlml": (C.c_int32, [C.c_void_p, D]),
     "gprx_sgpr_predict": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
+    "gprx_sgpr_predict_covariance": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
+    "gprx_sgpr_sample": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, C.c_uint64, C.c_uint64, D]),
     "gprx_sgpr_fit": (C.c_int32, [C.c_void_p, C.POINTER(LbfgsOptions), C.POINTER(FitReport)]),
     "gprx_sgpr_insert": (C.c_int32, [C.c_void_p, D, C.c_double, U64]),
     "gprx_sgpr_delete": (C.c_int32, [C.c_void_p, C.c_uint64]),

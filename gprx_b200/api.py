@@ -889,6 +889,33 @@ class FittedSgpr:
                                         L.ptr(var)))
         return Prediction(mean, var, options.variance_kind)
 
+    def predict_covariance(self, xs, n_rows, n_cols):
+        """Mean and query covariance of the VFE posterior (src/sgpr/fitted.rs:795-850)."""
+        return self.predict_covariance_with(xs, n_rows, n_cols, PredictOptions())
+
+    def predict_covariance_with(self, xs, n_rows, n_cols, options):
+        if n_cols != self.d:
+            raise ShapeMismatch("query has %d features, model has %d" % (n_cols, self.d))
+        xs = L.f64(xs)
+        mean = np.zeros(n_rows)
+        cov = np.zeros(n_rows * n_rows)
+        check(L.lib().gprx_sgpr_predict_covariance(self._h, L.ptr(xs), n_rows, int(options.variance_kind),
+                                                   L.ptr(mean), L.ptr(cov)))
+        return PredictiveCovariance(mean, cov.reshape(n_rows, n_rows, order="F"), options.variance_kind)
+
+    def sample(self, xs, n_rows, n_cols, n_draws, seed):
+        """n_draws posterior draws, column-major n_rows × n_draws (src/sgpr/fitted.rs:855-900)."""
+        return self.sample_with(xs, n_rows, n_cols, PredictOptions(), n_draws, seed)
+
+    def sample_with(self, xs, n_rows, n_cols, options, n_draws, seed):
+        if n_cols != self.d:
+            raise ShapeMismatch("query has %d features, model has %d" % (n_cols, self.d))
+        xs = L.f64(xs)
+        out = np.zeros(n_rows * n_draws)
+        check(L.lib().gprx_sgpr_sample(self._h, L.ptr(xs), n_rows, int(options.variance_kind), int(n_draws),
+                                       int(seed), L.ptr(out)))
+        return out
+
     def stream_ptr(self):
         s = C.c_void_p()
         check(L.lib().gprx_sgpr_stream(self._h, C.byref(s)))

@@ -123,7 +123,7 @@ gprx_status ExactState::enqueue_factor(double j) {
 }
 
 // JitterPolicy retry offsets after the first attempt (src/policy.rs:306-397).
-static std::vector<double> retry_list(const gprx_options& o) {
+std::vector<double> retry_list(const gprx_options& o) {
   std::vector<double> out;
   if (o.jitter_kind == GPRX_JITTER_FIXED) {
     if (o.jitter_initial > 0.0) out.push_back(o.jitter_initial);
@@ -138,6 +138,13 @@ static std::vector<double> retry_list(const gprx_options& o) {
     j = g;
   }
   return out;
+}
+
+std::vector<double> jitter_attempts(const gprx_options& o) {
+  std::vector<double> js{0.0};
+  auto r = retry_list(o);
+  js.insert(js.end(), r.begin(), r.end());
+  return js;
 }
 
 gprx_status ExactState::factor_with_retries(int stage) {
@@ -650,25 +657,36 @@ gprx_status ExactState::sample(const double* xs, uint64_t q, int kind, uint64_t 
   std::vector<double> mean(q);
   gprx_status st = covariance_dev(xs, q, kind, mean.data());
   if (st != GPRX_OK || n_draws == 0) return st;
-  const int qi = (int)q, nd = (int)n_draws;
+  return draw_posterior(covbuf.p, (int)q, mean.data(), n_draws, seed, jitter_attempts(opt), covl, covlinv, zbuf, status.p,
+                        stream, [&] { return reset_status(); }, [&](DevStatus* ds) { return read_status(ds); }, out);
+}
+
+// LLT of the covariance with the model's jitter retries (src/linalg/chol.rs:20-43,83-103),
+// q unit normals per draw from the seeded generator (src/rng.rs:83-87), out(:, k) = μ + L z_k
+// (src/prediction.rs:206-243).
+gprx_status draw_posterior(const double* cov, int qi, const double* mean_host, uint64_t n_draws, uint64_t seed,
+                           const std::vector<double>& js, DevBuf<double>& covl, DevBuf<double>& covlinv,
+                           DevBuf<double>& zbuf, DevStatus* st_dev, cudaStream_t stream,
+                           const std::function<gprx_status()>& reset,
+                           const std::function<gprx_status(DevStatus*)>& read, double* out) {
+  if (n_draws == 0) return GPRX_OK;
+  const size_t q = (size_t)qi;
+  const int nd = (int)n_draws;
   const size_t nblk = (size_t)ceil_div(qi, NB);
-  if (covl.ensure((size_t)q * q) != cudaSuccess || covlinv.ensure(nblk * NB * NB) != cudaSuccess ||
-      zbuf.ensure((size_t)q * n_draws * 2 + q) != cudaSuccess)
+  if (covl.ensure(q * q) != cudaSuccess || covlinv.ensure(nblk * NB * NB) != cudaSuccess ||
+      zbuf.ensure(q * n_draws * 2 + q) != cudaSuccess)
     return set_error(GPRX_OUT_OF_MEMORY, "draw buffers");
-  // LLT of the covariance with the model's jitter retries (src/linalg/chol.rs:20-43,83-103)
-  std::vector<double> js{0.0};
-  auto r = retry_list(opt);
-  js.insert(js.end(), r.begin(), r.end());
+  gprx_status st;
   bool ok = false;
   double last = 0.0;
   for (double j : js) {
     last = j;
-    if ((st = reset_status()) != GPRX_OK) return st;
-    GPRX_CUDA_TRY(cudaMemcpyAsync(covl.p, covbuf.p, sizeof(double) * q * q, cudaMemcpyDeviceToDevice, stream));
+    if ((st = reset()) != GPRX_OK) return st;
+    GPRX_CUDA_TRY(cudaMemcpyAsync(covl.p, cov, sizeof(double) * q * q, cudaMemcpyDeviceToDevice, stream));
     if (j != 0.0) GPRX_LAUNCH(add_diag_q_kernel, ceil_div(qi, 256), 256, 0, stream, covl.p, qi, j);
-    GPRX_CUDA_TRY(potrf_blocked(covl.p, qi, qi, covlinv.p, status.p, stream, nullptr));
+    GPRX_CUDA_TRY(potrf_blocked(covl.p, qi, qi, covlinv.p, st_dev, stream, nullptr));
     DevStatus ds;
-    if ((st = read_status(&ds)) != GPRX_OK) return st;
+    if ((st = read(&ds)) != GPRX_OK) return st;
     if (ds.code == GPRX_OK) {
       ok = true;
       break;
@@ -676,25 +694,24 @@ gprx_status ExactState::sample(const double* xs, uint64_t q, int kind, uint64_t 
     if (ds.code != GPRX_CHOLESKY_FAILED) return status_to_error(ds, j, q, GPRX_STAGE_PREDICT);
   }
   if (!ok) return set_cholesky_error(last, q, GPRX_STAGE_PREDICT);
-  // z: q unit normals per draw from the seeded generator (src/rng.rs:83-87)
-  std::vector<double> z((size_t)q * n_draws);
+  std::vector<double> z(q * n_draws);
   gprx_rng rng;
   gprx_rng_seed(&rng, seed);
   gprx_rng_fill_normal(&rng, z.data(), z.size());
   double* zd = zbuf.p;
-  double* od = zbuf.p + (size_t)q * n_draws;
-  double* md = od + (size_t)q * n_draws;
+  double* od = zbuf.p + q * n_draws;
+  double* md = od + q * n_draws;
   GPRX_CUDA_TRY(cudaMemcpyAsync(zd, z.data(), sizeof(double) * z.size(), cudaMemcpyHostToDevice, stream));
-  GPRX_CUDA_TRY(cudaMemcpyAsync(md, mean.data(), sizeof(double) * q, cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(md, mean_host, sizeof(double) * q, cudaMemcpyHostToDevice, stream));
   GPRX_LAUNCH(zero_upper_kernel, blocks_for((long long)qi * qi), 256, 0, stream, covl.p, qi);
-  GemmParams p = gemm_params(qi, nd, qi, covl.p, qi, zd, qi, od, qi, 1.0, 0.0, status.p);
+  GemmParams p = gemm_params(qi, nd, qi, covl.p, qi, zd, qi, od, qi, 1.0, 0.0, st_dev);
   p.mode = GEMM_K_TO_ROW;
   GPRX_CUDA_TRY(dgemm(false, false, p, stream));
   GPRX_LAUNCH(add_mean_kernel, blocks_for((long long)qi * nd), 256, 0, stream, od, md, qi, (long long)qi * nd);
   GPRX_CUDA_TRY(cudaMemcpyAsync(out, od, sizeof(double) * q * n_draws, cudaMemcpyDeviceToHost, stream));
   DevStatus ds;
-  if ((st = read_status(&ds)) != GPRX_OK) return st;
-  if (ds.code != GPRX_OK) return status_to_error(ds, jitter, q, GPRX_STAGE_PREDICT);
+  if ((st = read(&ds)) != GPRX_OK) return st;
+  if (ds.code != GPRX_OK) return status_to_error(ds, 0.0, q, GPRX_STAGE_PREDICT);
   return GPRX_OK;
 }
 

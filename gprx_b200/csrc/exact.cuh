@@ -16,6 +16,21 @@ struct gprx_exact;
 
 namespace gprx {
 
+// JitterPolicy retry offsets after the first attempt (src/policy.rs:306-397),
+// and the whole list of attempts starting with no jitter.
+std::vector<double> retry_list(const gprx_options& o);
+std::vector<double> jitter_attempts(const gprx_options& o);
+
+// out (q × n_draws, column k = draw k, host) = μ + L z_k: L the LLT of the
+// q×q device covariance `cov` under the jitter attempts js, z_k standard
+// normals from the seeded generator.  reset / read clear and read the
+// caller's device status word st_dev.
+gprx_status draw_posterior(const double* cov, int q, const double* mean_host, uint64_t n_draws, uint64_t seed,
+                           const std::vector<double>& js, DevBuf<double>& covl, DevBuf<double>& covlinv,
+                           DevBuf<double>& zbuf, DevStatus* st_dev, cudaStream_t stream,
+                           const std::function<gprx_status()>& reset,
+                           const std::function<gprx_status(DevStatus*)>& read, double* out);
+
 struct ExactState {
   int device = 0;
   cudaStream_t stream = nullptr;

@@ -21,6 +21,7 @@
 
 #include "dense_f64.cuh"
 #include "emu_gemm.cuh"
+#include "exact.cuh"
 #include "kernels.cuh"
 #include "lbfgs.h"
 #include "runtime.cuh"
@@ -262,7 +263,7 @@ struct SgprState {
   int m = 0, d = 0;
   long long ldm = 0;
   DevBuf<double> x, y, z, Lmm, linv_mm, Amat, Bl, linv_B, w, ay, G, H, Wm, Xb, Xt, splitbuf, partials, res, vtmp,
-      qbuf, qbuf2, qx, Btrial;
+      qbuf, qbuf2, qx, Btrial, covbuf, covl, covlinv, zbuf;
   DevBuf<int> slot_param;
   DevBuf<DevStatus> status;
   // mixed precision: the two m×m Gram products over n (B = A Aᵀ and H = G Aᵀ)
@@ -330,6 +331,9 @@ struct SgprState {
   gprx_status gradient(double* grad);
   gprx_status eval(const double* params, double* nlml_out, double* grad);
   gprx_status predict(const double* xs, uint64_t q, int kind, double* mean, double* var);
+  gprx_status covariance_dev(const double* xs, uint64_t q, int kind, double* mean_host);
+  gprx_status predict_covariance(const double* xs, uint64_t q, int kind, double* mean, double* cov);
+  gprx_status sample(const double* xs, uint64_t q, int kind, uint64_t n_draws, uint64_t seed, double* out);
   gprx_status solve_w();
   gprx_status insert(const double* xnew, double ynew, uint64_t* id);
   gprx_status remove(uint64_t id);
@@ -477,22 +481,6 @@ gprx_status SgprState::write_params(const double* params) {
   return GPRX_OK;
 }
 
-static std::vector<double> retry_list_sparse(const gprx_options& o) {
-  std::vector<double> out;
-  if (o.jitter_kind == GPRX_JITTER_FIXED) {
-    if (o.jitter_initial > 0.0) out.push_back(o.jitter_initial);
-    return out;
-  }
-  double j = o.jitter_initial;
-  for (int r = 0; r < o.jitter_max_retries; ++r) {
-    if (!(j <= o.jitter_max)) break;
-    out.push_back(j);
-    double g = j * o.jitter_multiplier;
-    if (!std::isfinite(g)) break;
-    j = g;
-  }
-  return out;
-}
 
 // B = Σ_slices A_s A_sᵀ (+ σ² I on the diagonal), lower or full, by split-K.
 static cudaError_t syrk_splitk(const double* A, long long lda, int m, long long n, const double* B, long long ldb,
@@ -579,7 +567,7 @@ gprx_status SgprState::assemble() {
   if (n > INT32_MAX) return set_error(GPRX_CAPACITY, "n too large for one assembly");
   const int nn = (int)n;
   std::vector<double> js{0.0};
-  auto r = retry_list_sparse(opt);
+  auto r = retry_list(opt);
   js.insert(js.end(), r.begin(), r.end());
   bool ok = false;
   gprx_status st;
@@ -820,6 +808,86 @@ gprx_status SgprState::predict(const double* xs, uint64_t q, int kind, double* m
   return GPRX_OK;
 }
 
+// covariance: lower triangle K** − A*ᵀA* + σn² S*ᵀS* mirrored off the
+// diagonal, the predictive variance on it
+__global__ void sgpr_cov_finish_kernel(double* C, int q, const double* var) {
+  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (e >= (long long)q * q) return;
+  const int i = (int)(e % q), j = (int)(e / q);
+  if (i == j) C[e] = var[i];
+  else if (i < j) C[e] = C[j + (long long)i * q];
+}
+
+// The VFE query covariance on the device (predict_vfe_covariance,
+// src/sgpr/factor/predict.rs:263-345; SparseCore::finish_covariance,
+// src/sparse/core.rs:641-667) into covbuf (q×q, both triangles).
+gprx_status SgprState::covariance_dev(const double* xs, uint64_t q, int kind, double* mean_host) {
+  if (kind != GPRX_VARIANCE_LATENT && kind != GPRX_VARIANCE_OBSERVATION)
+    return set_error(GPRX_INVALID_ARGUMENT, "variance kind");
+  if (q > (uint64_t)INT32_MAX) return set_error(GPRX_CAPACITY, "too many query points");
+  if (!all_finite(xs, q * d)) return set_error(GPRX_NONFINITE_INPUT, "non-finite query");
+  gprx_status st;
+  if (!assembled && (st = assemble()) != GPRX_OK) return st;
+  const int qi = (int)q;
+  if (qbuf.ensure((size_t)ldm * q) || qbuf2.ensure((size_t)ldm * q) || qx.ensure((size_t)q * (d + 4)) ||
+      covbuf.ensure((size_t)q * q))
+    return set_error(GPRX_OUT_OF_MEMORY, "covariance buffers");
+  double* xq = qx.p;
+  double* mdev = qx.p + (size_t)q * d;
+  double* vdev = mdev + q;
+  double* an = vdev + q;
+  double* bn = an + q;
+  if ((st = reset_status()) != GPRX_OK) return st;
+  GPRX_CUDA_TRY(cudaMemcpyAsync(xq, xs, sizeof(double) * q * d, cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(fill_cross(kern, z.p, m, m, xq, qi, qi, qbuf.p, ldm, status.p, stream));
+  GPRX_CUDA_TRY(trsm_lower(Lmm.p, ldm, m, linv_mm.p, qbuf.p, ldm, qi, status.p, stream));
+  GPRX_CUDA_TRY(gemv_t(qbuf.p, ldm, m, qi, false, w.p, mdev, status.p, stream));
+  GPRX_CUDA_TRY(col_sumsq(qbuf.p, ldm, m, qi, nullptr, an, status.p, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(qbuf2.p, qbuf.p, sizeof(double) * ldm * q, cudaMemcpyDeviceToDevice, stream));
+  GPRX_CUDA_TRY(trsm_lower(Bl.p, ldm, m, linv_B.p, qbuf2.p, ldm, qi, status.p, stream));
+  GPRX_CUDA_TRY(col_sumsq(qbuf2.p, ldm, m, qi, nullptr, bn, status.p, stream));
+  sgpr_finish_var_kernel<<<ceil_div(qi, 256), 256, 0, stream>>>(an, bn, qi, kern.diag_value(), noise(), kind, vdev,
+                                                                   status.p);
+  count_launch();
+  GPRX_CUDA_TRY(fill_lower(kern, xq, qi, qi, covbuf.p, qi, 0.0, status.p, stream));
+  GemmParams pa = gemm_params(qi, qi, m, qbuf.p, ldm, qbuf.p, ldm, covbuf.p, qi, -1.0, 1.0, status.p);
+  pa.mode = GEMM_LOWER_TILES;
+  GPRX_CUDA_TRY(dgemm(true, false, pa, stream));
+  GemmParams pb = gemm_params(qi, qi, m, qbuf2.p, ldm, qbuf2.p, ldm, covbuf.p, qi, noise(), 1.0, status.p);
+  pb.mode = GEMM_LOWER_TILES;
+  GPRX_CUDA_TRY(dgemm(true, false, pb, stream));
+  sgpr_cov_finish_kernel<<<(int)(((long long)qi * qi + 255) / 256), 256, 0, stream>>>(covbuf.p, qi, vdev);
+  count_launch();
+  GPRX_CUDA_TRY(cudaGetLastError());
+  GPRX_CUDA_TRY(cudaMemcpyAsync(mean_host, mdev, sizeof(double) * q, cudaMemcpyDeviceToHost, stream));
+  return sync_check(GPRX_STAGE_PREDICT);
+}
+
+gprx_status SgprState::predict_covariance(const double* xs, uint64_t q, int kind, double* mean, double* cov) {
+  if (!xs || !mean || !cov) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (q == 0) return GPRX_OK;
+  gprx_status st = covariance_dev(xs, q, kind, mean);
+  if (st != GPRX_OK) return st;
+  GPRX_CUDA_TRY(cudaMemcpyAsync(cov, covbuf.p, sizeof(double) * q * q, cudaMemcpyDeviceToHost, stream));
+  GPRX_CUDA_TRY(cudaStreamSynchronize(stream));
+  return GPRX_OK;
+}
+
+// FittedSgpr::sample_with (src/sgpr/fitted.rs:855-900): the exact model's
+// draw from the VFE covariance, with this model's jitter retries.
+gprx_status SgprState::sample(const double* xs, uint64_t q, int kind, uint64_t n_draws, uint64_t seed,
+                              double* out) {
+  if (!xs || (n_draws > 0 && !out)) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
+  if (q == 0) return GPRX_OK;
+  if (n_draws > (uint64_t)INT32_MAX) return set_error(GPRX_CAPACITY, "too many draws");
+  std::vector<double> mean(q);
+  gprx_status st = covariance_dev(xs, q, kind, mean.data());
+  if (st != GPRX_OK || n_draws == 0) return st;
+  return draw_posterior(covbuf.p, (int)q, mean.data(), n_draws, seed, jitter_attempts(opt), covl, covlinv, zbuf,
+                        status.p, stream, [&] { return reset_status(); },
+                        [&](DevStatus* ds) { return read_status(ds); }, out);
+}
+
 gprx_status SgprState::insert(const double* xnew, double ynew, uint64_t* id) {
   if (!xnew || !id) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (!all_finite(xnew, d) || !std::isfinite(ynew)) return set_error(GPRX_NONFINITE_INPUT, "non-finite point");
@@ -1021,7 +1089,7 @@ gprx_status SgprState::set_inducing(const double* zh, uint64_t mm) {
 gprx_status SgprState::factor_kmm_and_a(EmuWork& ew, bool& emu) {
   const int nn = (int)n;
   std::vector<double> js{0.0};
-  auto r = retry_list_sparse(opt);
+  auto r = retry_list(opt);
   js.insert(js.end(), r.begin(), r.end());
   bool ok = false;
   gprx_status st;
@@ -1313,6 +1381,18 @@ gprx_status gprx_sgpr_shard_gradient(gprx_sgpr* h, const double* exchange2, doub
 gprx_status gprx_sgpr_predict(gprx_sgpr* h, const double* xs, uint64_t q, int32_t kind, double* mean, double* var) {
   CHECK_SGPR(h);
   return h->s.predict(xs, q, kind, mean, var);
+}
+
+gprx_status gprx_sgpr_predict_covariance(gprx_sgpr* h, const double* xs, uint64_t q, int32_t kind, double* mean,
+                                         double* cov) {
+  CHECK_SGPR(h);
+  return h->s.predict_covariance(xs, q, kind, mean, cov);
+}
+
+gprx_status gprx_sgpr_sample(gprx_sgpr* h, const double* xs, uint64_t q, int32_t kind, uint64_t n_draws,
+                             uint64_t seed, double* out) {
+  CHECK_SGPR(h);
+  return h->s.sample(xs, q, kind, n_draws, seed, out);
 }
 
 gprx_status gprx_sgpr_fit(gprx_sgpr* h, const gprx_lbfgs_options* opt, gprx_fit_report* report) {

@@ -336,6 +336,17 @@ gprx_status gprx_sgpr_nlml(gprx_sgpr* h, double* nlml);
 /* vfe_predict_into / vfe_latent (src/sgpr/factor/predict.rs:102-262). */
 gprx_status gprx_sgpr_predict(gprx_sgpr* h, const double* xs, uint64_t q, int32_t variance_kind,
                               double* mean, double* var);
+/* Mean and the q×q query covariance of the VFE posterior, column-major:
+ * off the diagonal K** − A*ᵀA* + σn² S*ᵀS* (A* = L_mm⁻¹ K_m*, S* = L_B⁻¹ A*),
+ * on it the predictive variance of gprx_sgpr_predict
+ * (FittedSgpr::predict_covariance_with, src/sgpr/fitted.rs:818-850;
+ * src/sgpr/factor/predict.rs:263-345, src/sparse/core.rs:641-667). */
+gprx_status gprx_sgpr_predict_covariance(gprx_sgpr* h, const double* xs, uint64_t q, int32_t variance_kind,
+                                         double* mean, double* cov);
+/* Posterior draws from that covariance, as gprx_exact_sample (the model's
+ * jitter retries; FittedSgpr::sample_with, src/sgpr/fitted.rs:855-900). */
+gprx_status gprx_sgpr_sample(gprx_sgpr* h, const double* xs, uint64_t q, int32_t variance_kind, uint64_t n_draws,
+                             uint64_t seed, double* out);
 gprx_status gprx_sgpr_fit(gprx_sgpr* h, const gprx_lbfgs_options* opt, gprx_fit_report* report);
 /* OnlineSgpr::insert → append_point (src/sgpr/online/mod.rs:1695-1810). */
 gprx_status gprx_sgpr_insert(gprx_sgpr* h, const double* x_new, double y_new, uint64_t* id);

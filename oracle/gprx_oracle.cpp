@@ -873,25 +873,11 @@ int orc_exact_covariance(const int32_t* nodes, int n_nodes, const double* params
   return exact_covariance(t, noise, f, x, n, d, xs, q, kind, mean, cov);
 }
 
-// Posterior draws (PredictiveCovariance::draw, src/prediction.rs:206-243):
-// LLT of the covariance retried with the jitter list (src/linalg/chol.rs:20-43),
-// then column k = μ + L z_k, z_k the next q unit normals (src/rng.rs:72-87),
-// L z summed column by column as mul_lower_vec (src/linalg/dense.rs:409-422).
-int orc_exact_sample(const int32_t* nodes, int n_nodes, const double* params, int n_params, const double* x,
-                     int64_t n, int d, const double* y, int jitter_kind, double jitter_initial, double jitter_mult,
-                     int jitter_retries, double jitter_max, const double* xs, int64_t q, int kind, int64_t n_draws,
-                     uint64_t seed, double* out) {
-  Tree t;
-  int nk = n_params - 1;
-  if (!build_tree(t, nodes, n_nodes, params, nk)) return 3;
-  double noise = std::exp(params[nk]);
-  auto jl = retry_jitters(jitter_kind, jitter_initial, jitter_mult, jitter_retries, jitter_max);
-  Factor f;
-  double last_j = 0.0;
-  int st = factor_exact(t, x, n, d, y, noise, jl, f, &last_j);
-  if (st != 0) return st;
-  std::vector<double> mean(q), cov((size_t)q * q);
-  exact_covariance(t, noise, f, x, n, d, xs, q, kind, mean.data(), cov.data());
+// μ + L z_k for n_draws seeded standard-normal vectors, L the LLT of cov
+// with the jitter retries (FittedGpr::sample_with, src/prediction.rs:206-243;
+// Box–Muller on the open-unit draws of the seeded Xoshiro256++, src/rng.rs:83-87).
+static int draw_samples(const std::vector<double>& cov, const std::vector<double>& mean, int64_t q,
+                        const std::vector<double>& jl, int64_t n_draws, uint64_t seed, double* out) {
   if (n_draws == 0) return 0;
   std::vector<double> js{0.0};
   js.insert(js.end(), jl.begin(), jl.end());
@@ -927,6 +913,28 @@ int orc_exact_sample(const int32_t* nodes, int n_nodes, const double* params, in
     for (int64_t i = 0; i < q; ++i) out[k * q + i] = mean[i] + lz[i];
   }
   return 0;
+}
+
+// Posterior draws (PredictiveCovariance::draw, src/prediction.rs:206-243):
+// LLT of the covariance retried with the jitter list (src/linalg/chol.rs:20-43),
+// then column k = μ + L z_k, z_k the next q unit normals (src/rng.rs:72-87),
+// L z summed column by column as mul_lower_vec (src/linalg/dense.rs:409-422).
+int orc_exact_sample(const int32_t* nodes, int n_nodes, const double* params, int n_params, const double* x,
+                     int64_t n, int d, const double* y, int jitter_kind, double jitter_initial, double jitter_mult,
+                     int jitter_retries, double jitter_max, const double* xs, int64_t q, int kind, int64_t n_draws,
+                     uint64_t seed, double* out) {
+  Tree t;
+  int nk = n_params - 1;
+  if (!build_tree(t, nodes, n_nodes, params, nk)) return 3;
+  double noise = std::exp(params[nk]);
+  auto jl = retry_jitters(jitter_kind, jitter_initial, jitter_mult, jitter_retries, jitter_max);
+  Factor f;
+  double last_j = 0.0;
+  int st = factor_exact(t, x, n, d, y, noise, jl, f, &last_j);
+  if (st != 0) return st;
+  std::vector<double> mean(q), cov((size_t)q * q);
+  exact_covariance(t, noise, f, x, n, d, xs, q, kind, mean.data(), cov.data());
+  return draw_samples(cov, mean, q, jl, n_draws, seed, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1355,6 +1363,49 @@ void orc_sgpr_predict(void* p, const double* xs, int64_t q, int kind, double* me
     mean[c] = mu;
     var[c] = kind == 1 ? lat + h->noise : lat;
   }
+}
+
+// Query covariance of the VFE posterior (predict_vfe_covariance,
+// src/sgpr/factor/predict.rs:263-345; SparseCore::finish_covariance,
+// src/sparse/core.rs:641-667): off the diagonal K** − A*ᵀA* + σn² S*ᵀS*
+// with A* = L_mm⁻¹ K_m*, S* = L_B⁻¹ A*; on it the predictive variance.
+static void sgpr_covariance(OrcSgpr* h, const double* xs, int64_t q, int kind, double* mean, double* cov) {
+  int64_t m = h->m;
+  int d = h->d;
+  std::vector<double> var(q);
+  orc_sgpr_predict(h, xs, q, kind, mean, var.data());
+  Mat as((size_t)m * q);
+  for (int64_t c = 0; c < q; ++c)
+    for (int64_t i = 0; i < m; ++i) AT(as, m, i, c) = kval(h->t, h->z.data() + i, m, xs + c, q, d);
+  trsm_lower(h->lmm.data(), m, m, as.data(), q, m);
+  Mat bs = as;
+  trsm_lower(h->bl.data(), m, m, bs.data(), q, m);
+  for (int64_t c = 0; c < q; ++c)
+    for (int64_t r = 0; r < q; ++r) {
+      if (r == c) {
+        cov[r + c * q] = var[r];
+        continue;
+      }
+      double ad = 0.0, sd = 0.0;
+      for (int64_t k = 0; k < m; ++k) {
+        ad += AT(as, m, k, r) * AT(as, m, k, c);
+        sd += AT(bs, m, k, r) * AT(bs, m, k, c);
+      }
+      cov[r + c * q] = kval(h->t, xs + r, q, xs + c, q, d) - ad + h->noise * sd;
+    }
+}
+
+void orc_sgpr_covariance(void* p, const double* xs, int64_t q, int kind, double* mean, double* cov) {
+  sgpr_covariance((OrcSgpr*)p, xs, q, kind, mean, cov);
+}
+
+// FittedSgpr::sample_with (src/sgpr/fitted.rs:855-900): the exact model's
+// draw from the VFE covariance, with the model's jitter retries.
+int orc_sgpr_sample(void* p, const double* xs, int64_t q, int kind, int64_t n_draws, uint64_t seed, double* out) {
+  OrcSgpr* h = (OrcSgpr*)p;
+  std::vector<double> mean(q), cov((size_t)q * q);
+  sgpr_covariance(h, xs, q, kind, mean.data(), cov.data());
+  return draw_samples(cov, mean, q, retry_jitters(h->jk, h->ji, h->jm, h->jr, h->jx), n_draws, seed, out);
 }
 
 static void sgpr_set_points(OrcSgpr* h, std::vector<double>& nx, std::vector<double>& ny, int64_t n) {

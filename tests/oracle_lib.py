@@ -70,6 +70,8 @@ def lib():
     L.orc_sgpr_nlml.restype = C.c_double
     L.orc_sgpr_grad.argtypes = [C.c_void_p, D]
     L.orc_sgpr_predict.argtypes = [C.c_void_p, D, C.c_int64, C.c_int, D, D]
+    L.orc_sgpr_covariance.argtypes = [C.c_void_p, D, C.c_int64, C.c_int, D, D]
+    L.orc_sgpr_sample.argtypes = [C.c_void_p, D, C.c_int64, C.c_int, C.c_int64, C.c_uint64, D]
     L.orc_sgpr_insert.argtypes = [C.c_void_p, D, C.c_double, U64]
     L.orc_sgpr_delete.argtypes = [C.c_void_p, C.c_uint64]
     L.orc_sgpr_set_inducing.argtypes = [C.c_void_p, D, C.c_int64]
@@ -287,6 +289,19 @@ class Sgpr:
         var = np.zeros(q)
         lib().orc_sgpr_predict(self.h, _ptr(_f(xs)), q, kind, _ptr(mean), _ptr(var))
         return mean, var
+
+    def covariance(self, xs, q, kind):
+        mean = np.zeros(q)
+        cov = np.zeros(q * q)
+        lib().orc_sgpr_covariance(self.h, _ptr(_f(xs)), q, kind, _ptr(mean), _ptr(cov))
+        return mean, cov.reshape(q, q).T
+
+    def sample(self, xs, q, kind, n_draws, seed):
+        out = np.zeros(q * n_draws)
+        st = lib().orc_sgpr_sample(self.h, _ptr(_f(xs)), q, kind, n_draws, seed, _ptr(out))
+        if st != 0:
+            raise OracleError(st)
+        return out.reshape(n_draws, q)
 
     def insert(self, x, y):
         pid = C.c_uint64(0)
