@@ -146,6 +146,7 @@ _SIGS = {
     "gprx_sgpr_factor": (C.c_int32, [C.c_void_p]),
     "gprx_sgpr_eval": (C.c_int32, [C.c_void_p, D, C.c_uint64, D, D]),
     "gprx_sgpr_nlml": (C.c_int32, [C.c_void_p, D]),
+    "gprx_sgpr_set_params": (C.c_int32, [C.c_void_p, D, C.c_uint64]),
     "gprx_sgpr_predict": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
     "gprx_sgpr_predict_covariance": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
     "gprx_sgpr_sample": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, C.c_uint64, C.c_uint64, D]),

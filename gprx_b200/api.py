@@ -805,7 +805,7 @@ class Sgpr:
         h = C.c_void_p()
         check(L.lib().gprx_sgpr_create(L.ptr(x), n_rows, n_cols, L.ptr(y), L.ptr(z), m, nodes, nn, L.ptr(theta),
                                        theta.size, C.byref(o), C.byref(h)))
-        return FittedSgpr(h, n_cols)
+        return FittedSgpr(h, n_cols, self)
 
     def factor(self, x, n_rows, n_cols, y, z, m):
         f = self._create(x, n_rows, n_cols, y, z, m)
@@ -829,10 +829,47 @@ class Sgpr:
 class FittedSgpr:
     """An assembled VFE model (src/sgpr/fitted.rs)."""
 
-    def __init__(self, handle, d):
+    def __init__(self, handle, d, trainer=None):
         self._h = handle
         self.d = d
         self.report = None
+        self._trainer = trainer
+        self.optimizer = trainer.optimizer if trainer is not None else Fixed()
+
+    def set_params(self, params):
+        """Writes θ and reassembles (FittedSgpr::set_params)."""
+        p = L.f64(params)
+        check(L.lib().gprx_sgpr_set_params(self._h, L.ptr(p), p.size))
+
+    def likelihood(self):
+        """The Gaussian likelihood at the current σn²."""
+        return GaussianLikelihood(math.exp(self.get_params()[-1]))
+
+    def to_kernel(self):
+        """The kernel at the current θ."""
+        if self._trainer is None:
+            raise InvalidConfig("this model has no kernel description")
+        k = self._trainer.kernel.copy()
+        k.set_params(list(self.get_params()[:-1]))
+        return k
+
+    def with_optimizer(self, optimizer):
+        """Replaces the optimizer used by a later refit."""
+        self.optimizer = optimizer
+        return self
+
+    def refit(self):
+        """Re-runs the stored optimizer from the current θ on the stored data
+        (Fixed: reassembles at the current θ)."""
+        if isinstance(self.optimizer, Fixed):
+            check(L.lib().gprx_sgpr_factor(self._h))
+            return
+        if isinstance(self.optimizer, TrustRegion):
+            raise InvalidConfig("TrustRegion needs the Hessian, which this backend builds for exact models only")
+        rep = L.FitReport()
+        opt = self.optimizer._c()
+        check(L.lib().gprx_sgpr_fit(self._h, C.byref(opt), C.byref(rep)))
+        self.report = rep
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -960,7 +997,8 @@ class FittedSgpr:
 
     def into_online(self):
         """FittedSgpr::into_online: the same device state, now updatable."""
-        on = OnlineSgpr(self._h, self.d)
+        on = OnlineSgpr(self._h, self.d, self._trainer)
+        on.optimizer = self.optimizer
         self._h = None
         return on
 

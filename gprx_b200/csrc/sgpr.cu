@@ -1341,6 +1341,23 @@ gprx_status gprx_sgpr_factor(gprx_sgpr* h) {
   return h->s.assemble();
 }
 
+gprx_status gprx_sgpr_set_params(gprx_sgpr* h, const double* params, uint64_t p) {
+  CHECK_SGPR(h);
+  SgprState& s = h->s;
+  if (!params || p != (uint64_t)s.num_params()) return set_error(GPRX_SHAPE_MISMATCH, "parameter count");
+  std::vector<double> prev(p);
+  s.get_params(prev.data());
+  gprx_status st = s.write_params(params);
+  if (st == GPRX_OK) st = s.assemble();
+  if (st != GPRX_OK) {
+    gprx_error_info saved = last_error();
+    s.write_params(prev.data());
+    s.assemble();
+    last_error() = saved;
+  }
+  return st;
+}
+
 gprx_status gprx_sgpr_eval(gprx_sgpr* h, const double* params, uint64_t p, double* nlml, double* grad) {
   CHECK_SGPR(h);
   if (!params || !nlml) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");

@@ -328,6 +328,9 @@ uint64_t gprx_sgpr_num_params(const gprx_sgpr* h);
 gprx_status gprx_sgpr_get_params(gprx_sgpr* h, double* out, uint64_t p);
 /* assemble_vfe at the stored θ (src/sgpr/factor/vfe.rs:191-277). */
 gprx_status gprx_sgpr_factor(gprx_sgpr* h);
+/* Writes θ and reassembles at it; on failure the previous θ and its
+ * assembly are restored (FittedSgpr::set_params, src/sgpr/fitted.rs). */
+gprx_status gprx_sgpr_set_params(gprx_sgpr* h, const double* params, uint64_t p);
 /* FittedSgpr::value_and_gradient_into (src/sgpr/fitted.rs:306-326):
  * reassembly, vfe_neg_log_marginal_likelihood (vfe.rs:338-369) and
  * analytic_gradient (derivatives.rs:283-366).  `grad` may be NULL. */

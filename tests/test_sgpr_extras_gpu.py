@@ -40,3 +40,33 @@ def test_sgpr_covariance_and_draws_match_oracle(n, m, q, tree):
     draws = f.sample_with(xs, q, d, gx.PredictOptions(1), 3, 11)
     do = orc.sample(xs, q, 1, 3, 11)
     assert np.all(O.rel_err(draws, do.reshape(-1)) <= 1e-9)
+
+
+def test_sgpr_set_params_refit_and_accessors():
+    d, nodes, theta, spacing = TREES[1]
+    rs = np.random.RandomState(5)
+    n, m = 300, 33
+    zp = grid(m, d, 1.6 * spacing, rs)
+    hi = zp.max(axis=0) + 0.5 * spacing
+    x = (rs.uniform(0, 1, size=(n, d)) * hi).T.reshape(-1)
+    y = np.sin(6 * x[:n]) + 0.1 * rs.standard_normal(n)
+    z = zp.T.reshape(-1)
+    f = model(nodes, theta, 0.05, x, n, d, y, z, m)
+    moved = np.array(theta + [math.log(0.05)]) + 0.05
+    f.set_params(moved)
+    assert np.allclose(f.get_params(), moved, rtol=0, atol=1e-15)
+    orc = O.Sgpr(nodes, moved, x, n, d, y, z, m)
+    assert O.rel_err(f.neg_log_marginal_likelihood(), orc.nlml()) <= 1e-10
+    assert abs(f.likelihood().noise_variance - math.exp(moved[-1])) <= 1e-15
+    assert np.allclose(f.to_kernel().get_params(), moved[:-1], rtol=0, atol=0)
+    v0 = f.neg_log_marginal_likelihood()
+    f.refit()  # Fixed: reassembles at the current θ
+    assert f.neg_log_marginal_likelihood() == v0
+    f.with_optimizer(gx.Lbfgs().with_max_iterations(10)).refit()
+    assert f.neg_log_marginal_likelihood() <= v0 + 1e-12
+    bad = moved.copy()
+    bad[0] = float("nan")
+    before = f.get_params().copy()
+    with pytest.raises(gx.InvalidHyperparameter):
+        f.set_params(bad)
+    assert np.array_equal(f.get_params(), before)
