@@ -27,6 +27,7 @@ enum GemmMode : int {
   GEMM_SPLIT_K = 4,
   GEMM_K_TO_ROW = 8,   // k-loop stops at the tile's last global row + 1 (lower-triangular A)
   GEMM_K_FROM_COL = 16, // k-loop starts at the tile's first global column (lower-triangular B)
+  GEMM_K_TO_COL = 32,   // k-loop stops at the tile's last global column + 1 (op(B)(k, j) = 0 for k > j)
 };
 
 struct GemmParams {
@@ -159,6 +160,11 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, BK, WM, WN, STAGES, TA, TB>::T
   if (p.mode & GEMM_K_TO_ROW) {
     long long last_row = p.row0 + min(m0 + BM, p.M);  // exclusive
     long long ke = last_row - p.krow0;
+    if (ke < kend) kend = (int)max(ke, 0LL);
+  }
+  if (p.mode & GEMM_K_TO_COL) {
+    long long last_col = p.col0 + min(n0 + BN, p.N);  // exclusive
+    long long ke = last_col - p.krow0;
     if (ke < kend) kend = (int)max(ke, 0LL);
   }
 

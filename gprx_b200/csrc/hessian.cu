@@ -305,55 +305,40 @@ __global__ void __launch_bounds__(HESS_THREADS) hess_all_kernel(KTree t, HessMap
   }
 }
 
-// tr(M_i M_j) for every j ≤ i < np in one pass: per 32×32 tile each thread
-// reads its element of every M_i and, through shared memory, the transposed
-// element of every M_j.
-__global__ void __launch_bounds__(256) trace_products_kernel(HessMats mats, int np, long long ld, int n,
-                                                             double* partials) {
+// ⟨M_i, M_j⟩ for symmetric matrices held in their lower triangles: 64×64
+// lower tiles, each thread one row of a column pass (coalesced), every
+// matrix's element in registers and all products accumulated at once.
+__global__ void __launch_bounds__(256) sym_products_kernel(HessMats mats, int np, long long ld, int n,
+                                                           double* partials) {
   constexpr int P = HESS_FUSE_P, NS = HESS_TRACE_SLOTS;
-  extern __shared__ double tsm[];  // P tiles of 32 × 33, then the reduction
-  double* red = tsm + P * 32 * 33;
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int nt = (n + 31) / 32;
-  const long long ntiles = (long long)nt * nt;
+  __shared__ double red[8 * NS];
   double acc[NS];
 #pragma unroll
   for (int q = 0; q < NS; ++q) acc[q] = 0.0;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int r0 = (int)(t % nt) * 32, c0 = (int)(t / nt) * 32;
-    __syncthreads();
-    // tile j: ys[a][b] = M_j(c0 + b, r0 + a)
+  const int nt = (n + HT - 1) / HT;
+  const long long ntiles = (long long)nt * (nt + 1) / 2;
+  const int r = threadIdx.x % HT;
+  for (long long idx = blockIdx.x; idx < ntiles; idx += gridDim.x) {
+    int ti, tj;
+    hess_lower_tile(idx, ti, tj);
+    const int a = ti * HT + r;
+    for (int c = threadIdx.x / HT; c < HT; c += 256 / HT) {
+      const int b = tj * HT + c;
+      if (a >= n || b >= n || a < b) continue;
+      const double w = a == b ? 1.0 : 2.0;
+      double xv[P];
 #pragma unroll
-    for (int j = 0; j < P; ++j) {
-      if (j < np) {
-        for (int yy = ty; yy < 32; yy += 8) {
-          const int b = c0 + tx, a = r0 + yy;
-          tsm[j * 32 * 33 + yy * 33 + tx] = (a < n && b < n) ? mats.m[j][b + (long long)a * ld] : 0.0;
-        }
-      }
-    }
-    __syncthreads();
-    const int a = r0 + tx;
-    if (a < n) {
-      for (int yy = ty; yy < 32; yy += 8) {
-        const int b = c0 + yy;
-        if (b >= n) continue;
-        double xv[P];
+      for (int i = 0; i < P; ++i) xv[i] = i < np ? mats.m[i][a + (long long)b * ld] : 0.0;
+      int q = 0;
 #pragma unroll
-        for (int i = 0; i < P; ++i) xv[i] = i < np ? mats.m[i][a + (long long)b * ld] : 0.0;
-        int q = 0;
+      for (int i = 0; i < P; ++i) {
+        const double wx = w * xv[i];
 #pragma unroll
-        for (int i = 0; i < P; ++i) {
-#pragma unroll
-          for (int j = 0; j <= i; ++j, ++q) {
-            if (i < np) acc[q] = fma(xv[i], tsm[j * 32 * 33 + tx * 33 + yy], acc[q]);
-          }
-        }
+        for (int j = 0; j <= i; ++j, ++q) acc[q] = fma(wx, xv[j], acc[q]);
       }
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __syncthreads();
 #pragma unroll
   for (int q = 0; q < NS; ++q) {
     const double vs = warp_sum(acc[q]);
@@ -408,63 +393,6 @@ __global__ void __launch_bounds__(HESS_THREADS) fill_deriv_kernel(KTree t, HessM
       out[pa + (long long)pb * ld] = tot;
       out[pb + (long long)pa * ld] = tot;
     }
-  }
-}
-
-// Σ_{r < n, c < n} X(r,c) Y(r,c) over column-major n×n blocks with ld:
-// one partial per block.
-__global__ void __launch_bounds__(256) dot_nn_kernel(const double* X, const double* Y, long long ld, int n,
-                                                     double* partials) {
-  __shared__ double red[32];
-  double acc = 0.0;
-  const long long total = (long long)n * n;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long r = e % n, c = e / n;
-    acc = fma(X[r + c * ld], Y[r + c * ld], acc);
-  }
-  const double s = block_sum(acc, red);
-  if (threadIdx.x == 0) partials[blockIdx.x] = s;
-}
-
-// Σ_{a,b < n} X(a,b) Y(b,a): 32×32 tiles, Y's tile staged transposed in
-// shared memory so that both reads are coalesced.  One partial per block.
-__global__ void __launch_bounds__(256) dot_nt_kernel(const double* X, const double* Y, long long ld, int n,
-                                                     double* partials) {
-  __shared__ double ys[32][33];
-  __shared__ double red[32];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  const int nt = (n + 31) / 32;
-  const long long ntiles = (long long)nt * nt;
-  double acc = 0.0;
-  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int r0 = (int)(t % nt) * 32, c0 = (int)(t / nt) * 32;
-    __syncthreads();
-    // ys[a][b] = Y(c0 + b, r0 + a)
-    for (int yy = ty; yy < 32; yy += 8) {
-      const int b = c0 + tx, a = r0 + yy;
-      ys[yy][tx] = (a < n && b < n) ? Y[b + (long long)a * ld] : 0.0;
-    }
-    __syncthreads();
-    const int a = r0 + tx;
-    if (a < n)
-      for (int yy = ty; yy < 32; yy += 8) {
-        const int b = c0 + yy;
-        if (b < n) acc = fma(X[a + (long long)b * ld], ys[tx][yy], acc);
-      }
-  }
-  const double s = block_sum(acc, red);
-  if (threadIdx.x == 0) partials[blockIdx.x] = s;
-}
-
-// M(a, b) = M(b, a) = L(max(a,b), min(a,b)): the full symmetric matrix from
-// a lower triangle.
-__global__ void symmetrize_kernel(const double* Lw, long long ldl, int n, double* M, long long ldm) {
-  const long long total = (long long)n * n;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int a = (int)(e % n), b = (int)(e / n);
-    M[a + (long long)b * ldm] = a >= b ? Lw[a + (long long)b * ldl] : Lw[b + (long long)a * ldl];
   }
 }
 
@@ -529,20 +457,13 @@ cudaError_t hess_second_all(const HostKernel& k, const HessMap& hm, const double
   return cudaGetLastError();
 }
 
-cudaError_t trace_products(const HessMats& mats, int np, long long ld, int n, double* partials, int* blocks_out,
-                           cudaStream_t s) {
+cudaError_t sym_products(const HessMats& mats, int np, long long ld, int n, double* partials, int* blocks_out,
+                         cudaStream_t s) {
   if (np > HESS_FUSE_P) return cudaErrorInvalidValue;
-  const long long nt = (n + 31) / 32;
-  const int grid = (int)std::max<long long>(1, std::min<long long>(nt * nt, HESS_MAX_BLOCKS));
+  const int nt = (n + HT - 1) / HT;
+  const int grid = hess_grid((long long)nt * (nt + 1) / 2);
   *blocks_out = grid;
-  const size_t smem = sizeof(double) * ((size_t)HESS_FUSE_P * 32 * 33 + 8 * HESS_TRACE_SLOTS);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(trace_products_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  GPRX_LAUNCH(trace_products_kernel, grid, 256, smem, s, mats, np, ld, n, partials);
+  GPRX_LAUNCH(sym_products_kernel, grid, 256, 0, s, mats, np, ld, n, partials);
   return cudaGetLastError();
 }
 
@@ -559,29 +480,6 @@ cudaError_t fill_deriv(const HostKernel& k, const HessMap& hm, int i, const doub
     default: GPRX_FD(32); break;
   }
 #undef GPRX_FD
-  return cudaGetLastError();
-}
-
-cudaError_t dot_nn(const double* X, const double* Y, long long ld, int n, double* partials, int* blocks_out,
-                   cudaStream_t s) {
-  const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)n * n + 255) / 256, HESS_MAX_BLOCKS));
-  *blocks_out = grid;
-  GPRX_LAUNCH(dot_nn_kernel, grid, 256, 0, s, X, Y, ld, n, partials);
-  return cudaGetLastError();
-}
-
-cudaError_t dot_nt(const double* X, const double* Y, long long ld, int n, double* partials, int* blocks_out,
-                   cudaStream_t s) {
-  const long long nt = (n + 31) / 32;
-  const int grid = (int)std::max<long long>(1, std::min<long long>(nt * nt, HESS_MAX_BLOCKS));
-  *blocks_out = grid;
-  GPRX_LAUNCH(dot_nt_kernel, grid, 256, 0, s, X, Y, ld, n, partials);
-  return cudaGetLastError();
-}
-
-cudaError_t symmetrize(const double* Lw, long long ldl, int n, double* M, long long ldm, cudaStream_t s) {
-  const int grid = (int)std::max<long long>(1, std::min<long long>(((long long)n * n + 255) / 256, 148 * 8));
-  GPRX_LAUNCH(symmetrize_kernel, grid, 256, 0, s, Lw, ldl, n, M, ldm);
   return cudaGetLastError();
 }
 

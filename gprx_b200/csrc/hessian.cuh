@@ -21,7 +21,7 @@ struct HessMap {
 };
 
 // All rows of the second-order part in one launch when the kernel has at
-// most HESS_FUSE_K parameters; the trace products of at most HESS_FUSE_P
+// most HESS_FUSE_K parameters; the Frobenius products of at most HESS_FUSE_P
 // matrices in one pass.
 constexpr int HESS_FUSE_K = 10;
 constexpr int HESS_FUSE_P = 11;
@@ -42,24 +42,16 @@ constexpr int HESS_FUSE_SLOTS = HESS_FUSE_K * (HESS_FUSE_K + 1) / 2;
 cudaError_t hess_second_all(const HostKernel& k, const HessMap& hm, const double* x, long long ldx, int n,
                             const double* kinv, long long ld, const double* alpha, double* partials, int* blocks_out,
                             cudaStream_t s);
-// Partial sums (HESS_FUSE_P·(HESS_FUSE_P+1)/2 per block, packed lower
-// triangle row by row) of tr(M_i M_j) = Σ_ab M_i(a,b) M_j(b,a) for every
-// j ≤ i < np, np ≤ HESS_FUSE_P, in one pass over the matrices.
 constexpr int HESS_TRACE_SLOTS = HESS_FUSE_P * (HESS_FUSE_P + 1) / 2;
-cudaError_t trace_products(const HessMats& mats, int np, long long ld, int n, double* partials, int* blocks_out,
-                           cudaStream_t s);
+// Partial sums (HESS_TRACE_SLOTS per block, packed lower triangle row by
+// row) of ⟨M_i, M_j⟩_F = Σ_{a≥b} c_ab M_i(a,b) M_j(a,b) for symmetric M_i
+// stored in their lower triangles (c = 1 on the diagonal, 2 off it), every
+// j ≤ i < np, np ≤ HESS_FUSE_P.
+cudaError_t sym_products(const HessMats& mats, int np, long long ld, int n, double* partials, int* blocks_out,
+                         cudaStream_t s);
 // out (n×n, both triangles, ld) = ∂K/∂θ_i.
 cudaError_t fill_deriv(const HostKernel& k, const HessMap& hm, int i, const double* x, long long ldx, int n,
                        double* out, long long ld, cudaStream_t s);
-// Partial sums of Σ X ∘ Y over the n×n blocks (ld).
-cudaError_t dot_nn(const double* X, const double* Y, long long ld, int n, double* partials, int* blocks_out,
-                   cudaStream_t s);
-
-// Partial sums of Σ_{a,b} X(a,b) Y(b,a) = tr(X Y) over the n×n blocks (ld).
-cudaError_t dot_nt(const double* X, const double* Y, long long ld, int n, double* partials, int* blocks_out,
-                   cudaStream_t s);
-// M (n×n, ldm, both triangles) from the lower triangle of Lw (ldl).
-cudaError_t symmetrize(const double* Lw, long long ldl, int n, double* M, long long ldm, cudaStream_t s);
 // out[q] = Σ_b partials[b·stride + q], q < nq.
 cudaError_t reduce_slots(const double* partials, int blocks, int stride, int nq, double* out, cudaStream_t s);
 // out = trace of M (n×n, ld).
