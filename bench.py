@@ -15,9 +15,9 @@ The default line's value is the mixed form (FP64 products emulated on the
 int8 tensor cores); the plain FP64 form is timed beside it ("fp64") with the
 largest error of the mixed results against it.  The other workloads ride in
 the same line: "batched" (4096 ragged exact fits), "serving" (a Poisson
-request stream, p50/p99) and "sgpr" (VFE at n = 10⁶, m = 1024); each is also
-available alone through --workload.  "hessian" (alone only) times the NLML
-Hessian (gprx_exact_hessian) at the exact workload's θ in both forms.
+request stream, p50/p99), "sgpr" (VFE at n = 10⁶, m = 1024) and "hessian"
+(the NLML Hessian, gprx_exact_hessian, at the exact workload's θ in both
+forms); each is also available alone through --workload.
 
 N > 1 runs N independent replicas (one exact problem does not shard; launched
 by torchrun, one rank per GPU); `value` is the aggregate evals/s over ranks,
@@ -557,6 +557,44 @@ def serving_measure(torch, dev, rate, duration, precision, datasets, seed=5, wor
             "per_kind": per, "merged_predict_launches": stats["merged_launches"], "workers": workers}
 
 
+def hessian_measure(torch, dev, local, spec, x, y, theta, n, d, steps, warm, forms=("fp64", "mixed")):
+    """NLML Hessians (gprx_exact_hessian) at the exact workload's θ, timed
+    with CUDA events on the model's stream, per precision form."""
+    import gprx_b200 as gx
+    from gprx_b200 import _lib as L
+
+    per = {}
+    for f in forms:
+        prec = gx.Precision.Fp64 if f == "fp64" else gx.Precision.Mixed
+        model = gx.Gpr(spec, gx.GaussianLikelihood(NOISE), precision=prec, device=local) \
+            .with_optimizer(gx.Fixed()).factor(x, n, d, y)
+        stream = torch.cuda.ExternalStream(model.stream_ptr(), device=dev)
+        for i in range(warm):
+            model.hessian(theta)
+        torch.cuda.synchronize()
+        l0 = L.lib().gprx_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(steps):
+            h = model.hessian(theta)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        per[f] = {"ms_per_hessian": ms, "launches_per_hessian": (L.lib().gprx_launch_count() - l0) / steps,
+                  "h00": float(h[0, 0])}
+        del model
+        torch.cuda.empty_cache()
+    head = per["mixed"] if "mixed" in per else per["fp64"]
+    p = theta.size
+    return {"metric": "NLML Hessians/s n=%d p=%d" % (n, p), "value": 1e3 / head["ms_per_hessian"],
+            "unit": "hessians/s", "config": {"workload": "exact_gpr_nlml_hessian_n%d_d%d_const_rbfard" % (n, d),
+                                             "n": n, "d": d, "p": p},
+            "forms": per,
+            "work": "one evaluation with gradient; per kernel parameter S_i = X dK/dθ_i X^T with X = L^-1 "
+                    "(4 n^3 / 3 flop) and the second-order kernel walk over the n(n+1)/2 pairs (all parameters in "
+                    "one launch)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -670,44 +708,19 @@ def main():
     spec = gx.ConstantKernel(CONST) * gx.RbfArdKernel(list(np.exp(theta[1:1 + d])))
 
     if args.workload == "hessian":
-        # NLML Hessians (gprx_exact_hessian) at the exact workload's θ
         forms = ["fp64"] if args.precision == "fp64" else ["mixed"] if args.precision == "mixed" else ["fp64", "mixed"]
-        per = {}
-        for f in forms:
-            prec = gx.Precision.Fp64 if f == "fp64" else gx.Precision.Mixed
+        if args.profile_evals > 0:
+            prec = gx.Precision.Fp64 if forms[0] == "fp64" else gx.Precision.Mixed
             model = gx.Gpr(spec, gx.GaussianLikelihood(NOISE), precision=prec, device=local) \
                 .with_optimizer(gx.Fixed()).factor(x, n, d, y)
-            if args.profile_evals > 0:
-                for i in range(args.profile_evals):
-                    model.hessian(theta)
-                torch.cuda.synchronize()
-                return
-            stream = torch.cuda.ExternalStream(model.stream_ptr(), device=dev)
-            for i in range(warm):
+            for i in range(args.profile_evals):
                 model.hessian(theta)
             torch.cuda.synchronize()
-            l0 = L.lib().gprx_launch_count()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for i in range(args.steps):
-                h = model.hessian(theta)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / args.steps
-            per[f] = {"ms_per_hessian": ms, "launches_per_hessian": (L.lib().gprx_launch_count() - l0) / args.steps,
-                      "h00": float(h[0, 0])}
-            del model
-            torch.cuda.empty_cache()
-        head = per["mixed"] if "mixed" in per else per["fp64"]
-        p = theta.size
-        print(json.dumps({
-            "metric": "NLML Hessians/s n=%d p=%d" % (n, p), "value": 1e3 / head["ms_per_hessian"],
-            "unit": "hessians/s", "n_gpus": 1, "steps": args.steps, "warmup": warm, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "exact_gpr_nlml_hessian_n%d_d%d_const_rbfard" % (n, d), "n": n, "d": d, "p": p},
-            "forms": per,
-            "work": "one evaluation with gradient, p - 1 products A^-1 dK/dθ_i of 2 n^3 flops, "
-                    "p - 1 second-order kernel walks over the n(n+1)/2 pairs"}), flush=True)
+            return
+        out = hessian_measure(torch, dev, local, spec, x, y, theta, n, d, args.steps, warm, forms)
+        out.update({"n_gpus": 1, "steps": args.steps, "warmup": warm, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f64", "data": "synthetic"})
+        print(json.dumps(out), flush=True)
         return
 
     def barrier():
@@ -836,6 +849,8 @@ def main():
         line["serving"] = [serving_measure(torch, dev, 4.0, 12.0, prec, datasets) for prec in ("fp64", "mixed")]
         torch.cuda.empty_cache()
         line["sgpr"] = sgpr_measure(torch, dev, 3, 2, fp64_peak=fp64_peak)
+        torch.cuda.empty_cache()
+        line["hessian"] = hessian_measure(torch, dev, local, spec, x, y, theta, n, d, 3, 3)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
