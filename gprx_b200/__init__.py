@@ -30,6 +30,10 @@ from .api import (  # noqa: F401
     KernelSpec,
     Lbfgs,
     TrustRegion,
+    JitterPolicy,
+    KernelExp,
+    DistanceCachePolicy,
+    CholeskyBuffer,
     LoadedGpr,
     PersistFailed,
     UnsupportedPersistVersion,

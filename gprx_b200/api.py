@@ -436,7 +436,116 @@ def _check_points(x, n_rows, n_cols):
 # ---------------------------------------------------------------------------
 # exact GPR (src/gpr/)
 # ---------------------------------------------------------------------------
-class Gpr:
+class JitterPolicy:
+    """The Cholesky stabilizer (src/policy.rs:130-397): fixed(j) retries once
+    with j after an unregularized failure; adaptive(initial, multiplier,
+    max_retries, max_jitter) retries with a growing sequence."""
+
+    def __init__(self, kind, initial, multiplier, max_retries, max_jitter):
+        self.kind, self.initial, self.multiplier = int(kind), float(initial), float(multiplier)
+        self.max_retries, self.max_jitter = int(max_retries), float(max_jitter)
+
+    @staticmethod
+    def fixed(jitter):
+        if not (math.isfinite(jitter) and jitter >= 0.0):
+            raise InvalidConfig("jitter must be finite and non-negative, got %r" % jitter)
+        return JitterPolicy(0, jitter, 1.0, 0, jitter)
+
+    @staticmethod
+    def adaptive(initial, multiplier, max_retries, max_jitter):
+        if not (math.isfinite(initial) and initial > 0.0):
+            raise InvalidConfig("adaptive initial jitter must be finite and positive, got %r" % initial)
+        if not (math.isfinite(multiplier) and multiplier > 1.0):
+            raise InvalidConfig("adaptive jitter multiplier must be finite and greater than 1, got %r" % multiplier)
+        if int(max_retries) < 1:
+            raise InvalidConfig("adaptive jitter max_retries must be at least 1")
+        if not (math.isfinite(max_jitter) and max_jitter >= initial):
+            raise InvalidConfig("adaptive max_jitter must be finite and at least initial (%r), got %r"
+                                % (initial, max_jitter))
+        return JitterPolicy(1, initial, multiplier, max_retries, max_jitter)
+
+    def _tuple(self):
+        return (self.kind, self.initial, self.multiplier, self.max_retries, self.max_jitter)
+
+    def __eq__(self, other):
+        return isinstance(other, JitterPolicy) and self._tuple() == other._tuple()
+
+
+class KernelExp(enum.IntEnum):
+    """exp in the kernel walks (src/policy.rs:104-110).  The device computes
+    the FP64 exp; FastApprox (gprx's degree-7 polynomial) is not built."""
+    Accurate = 0
+    FastApprox = 1
+
+
+class DistanceCachePolicy(enum.IntEnum):
+    """Whether the host reference caches pairwise distances; the device path
+    recomputes them inside each fill, so this is recorded only."""
+    Uncached = 0
+    Cached = 1
+
+
+class CholeskyBuffer(enum.IntEnum):
+    """Whether the host reference keeps L beside W; the device path keeps a
+    dedicated inverse buffer, so this is recorded only."""
+    Reuse = 0
+    Retain = 1
+
+
+class _TrainerPolicies:
+    """The trainer's policy setters shared by Gpr and Sgpr (src/gpr/trainer.rs)."""
+
+    def with_jitter_policy(self, policy):
+        self.jitter = policy._tuple()
+        return self
+
+    def jitter_policy(self):
+        if self.jitter is None:
+            return JitterPolicy.fixed(0.0)
+        return JitterPolicy(*self.jitter)
+
+    def with_math(self, mode):
+        mode = KernelExp(mode)
+        if mode != KernelExp.Accurate:
+            raise InvalidConfig("KernelExp.FastApprox is not built on the device; the kernel walks use FP64 exp")
+        self._math = mode
+        return self
+
+    def math(self):
+        return getattr(self, "_math", KernelExp.Accurate)
+
+    def with_prefer_memory(self):
+        self._cache, self._buffer = DistanceCachePolicy.Uncached, CholeskyBuffer.Reuse
+        return self
+
+    def with_prefer_speed(self):
+        self._cache, self._buffer = DistanceCachePolicy.Cached, CholeskyBuffer.Retain
+        return self
+
+    def distance_cache_policy(self):
+        return getattr(self, "_cache", DistanceCachePolicy.Cached)
+
+    def cholesky_buffer(self):
+        return getattr(self, "_buffer", CholeskyBuffer.Retain)
+
+    def num_params(self):
+        return self.kernel.num_params() + 1
+
+    def get_params(self):
+        return np.array(self.kernel.get_params() + [self.likelihood.log_noise_variance])
+
+    def set_params(self, params):
+        params = list(params)
+        if len(params) != self.num_params():
+            raise ShapeMismatch("expected %d parameters, got %d" % (self.num_params(), len(params)))
+        self.kernel.set_params(params[:-1])
+        self.likelihood = GaussianLikelihood(math.exp(params[-1]))
+
+    def to_kernel(self):
+        return self.kernel.copy()
+
+
+class Gpr(_TrainerPolicies):
     """Exact GPR trainer (src/gpr/trainer.rs:533-613)."""
 
     def __init__(self, kernel, likelihood, optimizer=None, precision=Precision.Fp64, device=0):
@@ -774,7 +883,7 @@ class OnlineGpr(FittedGpr):
 # ---------------------------------------------------------------------------
 # VFE sparse GPR (src/sgpr/)
 # ---------------------------------------------------------------------------
-class Sgpr:
+class Sgpr(_TrainerPolicies):
     """VFE sparse GPR trainer (src/sgpr/model.rs:448-579).  The K_mm factor
     retries with JitterPolicy::adaptive(1e-8, 10, 5, 1e-3) by default."""
 
@@ -784,9 +893,17 @@ class Sgpr:
         self.optimizer = optimizer if optimizer is not None else Lbfgs()
         self.precision = Precision(precision)
         self.device = device
+        self.jitter = None  # None = JitterPolicy.adaptive(1e-8, 10, 5, 1e-3)
 
     def with_optimizer(self, opt):
-        return Sgpr(self.kernel, self.likelihood, opt, self.precision, self.device)
+        g = Sgpr(self.kernel, self.likelihood, opt, self.precision, self.device)
+        g.jitter = self.jitter
+        return g
+
+    def jitter_policy(self):
+        if self.jitter is None:
+            return JitterPolicy.adaptive(1e-8, 10.0, 5, 1e-3)
+        return JitterPolicy(*self.jitter)
 
     def _create(self, x, n_rows, n_cols, y, z, m):
         x = _check_points(x, n_rows, n_cols)
@@ -802,6 +919,8 @@ class Sgpr:
         L.lib().gprx_options_default_sparse(C.byref(o))
         o.precision = int(self.precision)
         o.device = int(self.device)
+        if self.jitter is not None:
+            o.jitter_kind, o.jitter_initial, o.jitter_multiplier, o.jitter_max_retries, o.jitter_max = self.jitter
         h = C.c_void_p()
         check(L.lib().gprx_sgpr_create(L.ptr(x), n_rows, n_cols, L.ptr(y), L.ptr(z), m, nodes, nn, L.ptr(theta),
                                        theta.size, C.byref(o), C.byref(h)))
