@@ -70,3 +70,25 @@ def test_sgpr_set_params_refit_and_accessors():
     with pytest.raises(gx.InvalidHyperparameter):
         f.set_params(bad)
     assert np.array_equal(f.get_params(), before)
+
+
+def test_sgpr_jitter_policy_reaches_the_device():
+    # a K_mm with duplicated inducing inputs fails without jitter: the fixed
+    # policy retries once with its j, as the oracle does with the same policy
+    d, nodes, theta, spacing = TREES[0]
+    rs = np.random.RandomState(9)
+    n, m = 120, 9
+    zp = grid(m - 1, d, 1.6 * spacing, rs)
+    zp = np.vstack([zp, zp[:1]])
+    hi = zp.max(axis=0) + 0.5 * spacing
+    x = (rs.uniform(0, 1, size=(n, d)) * hi).T.reshape(-1)
+    y = np.sin(6 * x[:n]) + 0.1 * rs.standard_normal(n)
+    z = zp.T.reshape(-1)
+    params = np.array(theta + [math.log(0.05)])
+    pol = gx.JitterPolicy.fixed(1e-6)
+    from test_sgpr_gpu import spec
+    f = gx.Sgpr(spec(nodes, theta), gx.GaussianLikelihood(0.05)).with_jitter_policy(pol).with_optimizer(
+        gx.Fixed()).factor(x, n, d, y, z, m)
+    orc = O.Sgpr(nodes, params, x, n, d, y, z, m, jitter=(0, 1e-6, 1.0, 0, 1e-6))
+    assert f.kmm_jitter() == orc.kmm_jitter == 1e-6
+    assert O.rel_err(f.neg_log_marginal_likelihood(), orc.nlml()) <= 1e-9
