@@ -133,7 +133,7 @@ def measured_peaks():
 
 def fp64_peak_tflops(torch, dev):
     """cuBLAS DGEMM throughput on this GPU (the FP64 denominator; measured
-    here because the driver's peak file has no FP64 figure)."""
+    here because MEASURED_PEAKS.json has no FP64 figure)."""
     n = 8192
     a = torch.randn(n, n, dtype=torch.float64, device=dev)
     b = torch.randn(n, n, dtype=torch.float64, device=dev)

@@ -1,6 +1,6 @@
 // probe.cu — device microbenchmarks of the FP64 building blocks (timed with
 // CUDA events on a private stream).  They measure the roofline denominators
-// that the driver's peak file does not carry (FP64 GEMM on this part) and
+// that MEASURED_PEAKS.json does not carry (FP64 GEMM on this part) and
 // the blocked factor in isolation.
 
 #include <cmath>

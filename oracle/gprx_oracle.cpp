@@ -1,7 +1,7 @@
 // gprx_oracle.cpp — TEST INFRASTRUCTURE ONLY.
 //
 // A plain FP64 CPU restatement of gprx 0.2.0's exact-GPR and VFE-SGPR
-// objective-and-prediction path.  It is the parity checker for the CUDA
+// objective-and-prediction path.  It is the parity reference for the CUDA
 // backend (tests, __graft_entry__.smoke) and the timed CPU baseline of
 // bench.py (kind "port"); nothing in the product links or calls it.
 //

@@ -1,6 +1,6 @@
 """ctypes wrapper of the CPU oracle (oracle/gprx_oracle.cpp).
 
-Test infrastructure: the checker the CUDA backend is compared against.  Only
+Test infrastructure: the reference results the CUDA backend is compared against.  Only
 tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
 """
 

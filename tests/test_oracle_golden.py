@@ -1,6 +1,6 @@
 """Pins the CPU oracle against the reference's own goldens (CPU only).
 
-The oracle (oracle/gprx_oracle.cpp) is the parity checker for the CUDA
+The oracle (oracle/gprx_oracle.cpp) is the parity reference for the CUDA
 backend; these tests are what make it trustworthy.  Tolerances are the
 reference's: 1e-8 for the sklearn / libgp / GPyTorch goldens
 (tests/goldens.rs:15, tests/online_libgp.rs, tests/sparse_gpytorch.rs),

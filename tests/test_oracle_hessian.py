@@ -1,4 +1,4 @@
-"""CPU checks of the oracle's analytic NLML Hessian (the checker of
+"""CPU checks of the oracle's analytic NLML Hessian (the parity reference of
 gprx_exact_hessian), pinned the way the reference pins its own
 (src/gpr/tests.rs:1394-1493): every entry against central differences
 (h = 1e-5) of the oracle's gradient, which the committed goldens pin, within

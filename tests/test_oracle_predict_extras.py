@@ -1,5 +1,5 @@
 """CPU checks of the oracle's leave-one-out, query covariance and posterior
-draws (the checkers of gprx_exact_loo / _predict_covariance / _sample),
+draws (the parity references of gprx_exact_loo / _predict_covariance / _sample),
 pinned on identities the reference's own tests use (src/gpr/tests.rs:1727-1870:
 LOO at n = 1 is the prior, LOO matches a refit without the point, the
 observation variance is the latent one plus the noise) and on the draw

@@ -1,5 +1,5 @@
 """CPU checks of the oracle's VFE query covariance and posterior draws (the
-checkers of gprx_sgpr_predict_covariance / gprx_sgpr_sample): the diagonal
+parity references of gprx_sgpr_predict_covariance / gprx_sgpr_sample): the diagonal
 is the predictive variance, the matrix is symmetric, and with the inducing
 inputs at the training points the VFE posterior is the exact one, so the
 covariance and the seeded draws equal the exact model's (1e-8)."""
