@@ -4,9 +4,11 @@
 //   H_ij = −½ ⟨W, ∂²A/∂θ_i∂θ_j⟩ − ½ ⟨S_i, S_j⟩_F + v_iᵀ v_j,
 //   W = ααᵀ − A⁻¹,  S_i = L⁻¹ A_i L⁻ᵀ,  v_i = L⁻¹ A_i α,  A_i = ∂A/∂θ_i.
 //
-// This file computes the first term's contraction (one launch per row i of
-// the Hessian, all j ≥ i accumulated in registers) and fills A_i as a full
-// symmetric matrix for the GEMMs of S_i.  Leaf second derivatives, in the log
+// This file computes the first term's contraction (every entry in one launch
+// up to HESS_FUSE_K kernel parameters, else one launch per row i with all
+// j ≥ i accumulated in registers), fills A_i as a full symmetric matrix for
+// the products that form S_i, and takes the Frobenius products ⟨S_i, S_j⟩ of
+// the lower-stored S_i in one pass.  Leaf second derivatives, in the log
 // parameters (u = r²/ℓ², u_f = Δ_f²/ℓ_f², φ = π r / p, s = sin φ, c = cos φ):
 //   constant  k = c                     ∂ = c,  ∂² = c
 //   rbf       k = e^{−u/2}              ∂ = k u,  ∂² = k (u² − 2u)
