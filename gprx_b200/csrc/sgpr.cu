@@ -71,6 +71,36 @@ __global__ void sumsq_kernel(const double* A, long long ld, int m, long long n, 
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
+// Σ_c (kdiag − ‖A[:, c]‖²) over the n columns of the m×n matrix A: each term
+// is point c's Nyström residual k(x_c, x_c) − k_cᵀ K_mm⁻¹ k_c ≥ 0, so the sum
+// keeps its digits where Σ k_ii − ‖A‖²_F (vfe.rs:338-369) cancels.  One warp
+// per column; one partial per block.
+__global__ void trace_residual_kernel(const double* A, long long ld, int m, long long n, double kdiag,
+                                      double* partial, const DevStatus* st) {
+  __shared__ double red[32];
+  if (dev_failed(st)) return;
+  const int lane = threadIdx.x & 31;
+  const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  double acc = 0.0;
+  for (long long c = warp; c < n; c += nw) {
+    const double* a = A + c * ld;
+    double ss = 0.0;
+    for (int i = lane; i < m; i += 32) ss = fma(a[i], a[i], ss);
+    ss = warp_sum(ss);
+    if (lane == 0) acc += kdiag - ss;
+  }
+  double s = block_sum(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// Σ y² in extended precision (the host's long double).
+static double sumsq_host(const std::vector<double>& v) {
+  long double s = 0.0L;
+  for (double e : v) s += (long double)e * e;
+  return (double)s;
+}
+
 __global__ void sum_partials_kernel(const double* partial, int count, double* out, const DevStatus* st) {
   __shared__ double red[32];
   if (dev_failed(st)) return;
@@ -284,7 +314,8 @@ struct SgprState {
   HostPinned<DevStatus> status_h;
   FactorCtx fctx;
   // host scalars of the assembly
-  double kdiag_sum = 0.0, afro = 0.0, y2 = 0.0, kmm_jitter = 0.0, pivot_ratio = 1.0;
+  // trace_sum = Σ_c (k(x_c, x_c) − ‖a_c‖²), the numerator of the VFE trace term
+  double trace_sum = 0.0, y2 = 0.0, kmm_jitter = 0.0, pivot_ratio = 1.0;
   bool assembled = false;
   std::vector<double> y_host;     // slot order
   std::vector<long long> order;   // registry index → slot
@@ -433,8 +464,7 @@ gprx_status SgprState::create(const double* xh, uint64_t nn, uint64_t dd, const 
   GPRX_CUDA_TRY(cudaMemcpyAsync(slot_param.p, sp.data(), sizeof(int) * 64, cudaMemcpyHostToDevice, stream));
   GPRX_CUDA_TRY(cudaStreamSynchronize(stream));
   y_host.assign(yh, yh + n);
-  y2 = 0.0;
-  for (double v : y_host) y2 += v * v;
+  y2 = sumsq_host(y_host);
   for (long long i = 0; i < n; ++i) {
     order.push_back(i);
     ids.push_back(next_id++);
@@ -608,9 +638,9 @@ gprx_status SgprState::assemble() {
     GPRX_CUDA_TRY(syrk_splitk(Amat.p, ldm, m, nn, Amat.p, ldm, true, noise(), splitbuf, Bl.p, ldm, status.p, stream));
   }
   GPRX_CUDA_TRY(potrf_blocked(Bl.p, ldm, m, linv_B.p, status.p, stream, &fctx));
-  // ‖A‖²_F and A y
-  int blocks = grid_for((long long)m * nn, 1024);
-  sumsq_kernel<<<blocks, 256, 0, stream>>>(Amat.p, ldm, m, nn, partials.p, status.p);
+  // Σ_c (k_cc − ‖a_c‖²) and A y
+  int blocks = grid_for((long long)nn * 32, 1024);
+  trace_residual_kernel<<<blocks, 256, 0, stream>>>(Amat.p, ldm, m, nn, kern.diag_value(), partials.p, status.p);
   sum_partials_kernel<<<1, 1024, 0, stream>>>(partials.p, blocks, res.p + 11, status.p);
   count_launch(2);
   {
@@ -629,8 +659,7 @@ gprx_status SgprState::assemble() {
   if ((st = sync_check(GPRX_STAGE_FIT)) != GPRX_OK) return st;
   if (emu && *emu_err_h.p) return set_error(GPRX_TIMEOUT, "an emulated product's bounded wait ran out");
   pivot_ratio = res_h.p[0];
-  afro = res_h.p[1];
-  kdiag_sum = (double)n * kern.diag_value();
+  trace_sum = res_h.p[1];
   assembled = true;
   sharded = false;
   st = solve_w();
@@ -657,7 +686,7 @@ gprx_status SgprState::nlml(double* out) {
   const double noise_v = noise();
   const double logdet = ((double)n - (double)m) * std::log(noise_v) + res_h.p[0];
   const double quad = (y2 - res_h.p[1]) / noise_v;
-  const double trace = (kdiag_sum - afro) / (2.0 * noise_v);
+  const double trace = trace_sum / (2.0 * noise_v);
   *out = 0.5 * ((double)n * std::log(2.0 * M_PI) + logdet + quad) + trace;
   return GPRX_OK;
 }
@@ -734,7 +763,7 @@ gprx_status SgprState::gradient(double* grad) {
   // directional_noise (derivatives.rs:186-202) with ∂σ² = σ²
   const double trb = res_h.p[2], ww = res_h.p[3], ayw = res_h.p[4];
   const double quad = (y2 - ayw) / noise_v;
-  const double trace = (kdiag_sum - afro) / (2.0 * noise_v);
+  const double trace = trace_sum / (2.0 * noise_v);
   const double dn = noise_v;
   const double d_logdet_b = dn * trb;
   const double d_q = -dn * ww;
@@ -925,8 +954,7 @@ gprx_status SgprState::insert(const double* xnew, double ynew, uint64_t* id) {
   GPRX_CUDA_TRY(tri_inv_blocks(Bl.p, ldm, m, false, linv_B.p, status.p, stream));
   GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p + 12, sizeof(double), cudaMemcpyDeviceToHost, stream));
   if ((st = sync_check(GPRX_STAGE_ONLINE_INSERT)) != GPRX_OK) return st;
-  afro += res_h.p[0];
-  kdiag_sum += kern.diag_value();
+  trace_sum += kern.diag_value() - res_h.p[0];
   last_in_place = 1;
   return solve_w();
 }
@@ -958,8 +986,7 @@ gprx_status SgprState::remove(uint64_t id) {
     if (ds.code == GPRX_CHOLESKY_FAILED) ok = false;
     else if (ds.code != GPRX_OK) return status_to_error(ds, 0.0, m, GPRX_STAGE_ONLINE_DELETE);
     if (ok) {
-      afro -= res_h.p[0];
-      kdiag_sum -= kern.diag_value();
+      trace_sum -= kern.diag_value() - res_h.p[0];
       axpy_kernel<<<ceil_div(m, 256), 256, 0, stream>>>(ay.p, col, -ydel, m);
       count_launch();
       std::swap(Bl.p, Btrial.p);
@@ -985,8 +1012,7 @@ gprx_status SgprState::remove(uint64_t id) {
   n -= 1;
   if (!ok) {
     last_in_place = 0;
-    y2 = 0.0;
-    for (double v : y_host) y2 += v * v;
+    y2 = sumsq_host(y_host);
     return assemble();
   }
   last_in_place = 1;
@@ -1080,8 +1106,9 @@ gprx_status SgprState::set_inducing(const double* zh, uint64_t mm) {
 // ---------------------------------------------------------------------------
 // sharded evaluation (one shard = the points this handle holds; Z, K_mm and
 // L are replicated).  Exchange buffer 1 (m² + m + 3): B_s = A_s A_sᵀ (lower,
-// ld m, upper zero), A_s y_s, ‖A_s‖²_F, Σ y_s², n_s.  Exchange buffer 2
-// (m² + p): H_s = G_s A_sᵀ (ld m) and the θ-gradient of the cross term
+// ld m, upper zero), A_s y_s, Σ_c (k_cc − ‖a_c‖²) over the shard's points,
+// Σ y_s², n_s.  Exchange buffer 2 (m² + p): H_s = G_s A_sᵀ (ld m) and the
+// θ-gradient of the cross term
 // ⟨L⁻ᵀ G_s, ∂K(Z, X_s)⟩.  Both are sums over n, so their sum over the shards
 // is the unsharded value (assemble_vfe, src/sgpr/factor/vfe.rs:191-277;
 // analytic_gradient, src/sgpr/factor/derivatives.rs:283-366).
@@ -1137,8 +1164,8 @@ gprx_status SgprState::shard_assemble(const double* params, double* e1) {
   } else {
     GPRX_CUDA_TRY(syrk_splitk(Amat.p, ldm, m, nn, Amat.p, ldm, true, 0.0, splitbuf, e1, m, status.p, stream));
   }
-  int blocks = grid_for((long long)m * nn, 1024);
-  sumsq_kernel<<<blocks, 256, 0, stream>>>(Amat.p, ldm, m, nn, partials.p, status.p);
+  int blocks = grid_for((long long)nn * 32, 1024);
+  trace_residual_kernel<<<blocks, 256, 0, stream>>>(Amat.p, ldm, m, nn, kern.diag_value(), partials.p, status.p);
   sum_partials_kernel<<<1, 1024, 0, stream>>>(partials.p, blocks, e1 + mm2 + m, status.p);
   count_launch(2);
   {
@@ -1181,10 +1208,9 @@ gprx_status SgprState::shard_nlml(const double* e1, double* nlml_out, double* e2
   GPRX_CUDA_TRY(cudaMemcpyAsync(ay.p, e1 + mm2, sizeof(double) * m, cudaMemcpyDeviceToDevice, stream));
   GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p + 20, e1 + mm2 + m, sizeof(double) * 3, cudaMemcpyDeviceToHost, stream));
   if ((st = solve_w()) != GPRX_OK) return st;  // synchronises the stream
-  afro = res_h.p[20];
+  trace_sum = res_h.p[20];
   const double y2_total = res_h.p[21];
   n_total = res_h.p[22];
-  kdiag_sum = n_total * kern.diag_value();
   GPRX_CUDA_TRY(logdet_diag(Bl.p, ldm, m, false, res.p + 0, status.p, stream));
   GPRX_CUDA_TRY(dot_dev(ay.p, w.p, m, res.p + 1, status.p, stream));
   GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p, res.p, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
@@ -1192,7 +1218,7 @@ gprx_status SgprState::shard_nlml(const double* e1, double* nlml_out, double* e2
   shard_y2 = y2_total;
   const double logdet = (n_total - (double)m) * std::log(noise_v) + res_h.p[0];
   const double quad = (y2_total - res_h.p[1]) / noise_v;
-  const double trace = (kdiag_sum - afro) / (2.0 * noise_v);
+  const double trace = trace_sum / (2.0 * noise_v);
   *nlml_out = 0.5 * (n_total * std::log(2.0 * M_PI) + logdet + quad) + trace;
   shard_ready = true;
   assembled = true;  // L, L_B and w are the global posterior's
@@ -1279,7 +1305,7 @@ gprx_status SgprState::shard_gradient(const double* e2, double* grad) {
   for (int i = 0; i < nk; ++i) grad[i] = res_h.p[20 + i] + res_h.p[21 + nk + i] + wdiag * n_total * dg[i];
   const double trb = res_h.p[2], ww = res_h.p[3], ayw = res_h.p[4];
   const double quad = (shard_y2 - ayw) / noise_v;
-  const double trace = (kdiag_sum - afro) / (2.0 * noise_v);
+  const double trace = trace_sum / (2.0 * noise_v);
   const double dn = noise_v;
   const double d_logdet_b = dn * trb;
   const double d_q = -dn * ww;

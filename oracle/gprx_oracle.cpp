@@ -318,17 +318,44 @@ void llt_solve(const double* l, int64_t n, int64_t ld, double* b) {
   }
 }
 
-// Overwrites each column of B (n×q) with L⁻¹ B (faer solve_lower_triangular_in_place).
+// Overwrites each column of B (n×q) with L⁻¹ B (faer solve_lower_triangular_in_place),
+// column-oriented: x_t = b_t / L_tt, then b_i −= L_it x_t down column t of L
+// (contiguous in memory).
 void trsm_lower(const double* l, int64_t n, int64_t ld, double* b, int64_t q, int64_t ldb) {
 #pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < q; ++c) {
     double* col = b + c * ldb;
-    for (int64_t i = 0; i < n; ++i) {
-      double s = col[i];
-      for (int64_t t = 0; t < i; ++t) s -= AT(l, ld, i, t) * col[t];
-      col[i] = s / AT(l, ld, i, i);
+    for (int64_t t = 0; t < n; ++t) {
+      const double xt = col[t] / AT(l, ld, t, t);
+      col[t] = xt;
+      const double* lt = &AT(l, ld, 0, t);
+      for (int64_t i = t + 1; i < n; ++i) col[i] -= lt[i] * xt;
     }
   }
+}
+
+// C (m×m, ldc) = A Bᵀ over the n columns of the column-major m×n matrices A and
+// B (lower triangle only when `lower`), in chunks of columns packed row-wise
+// for packed_update; sums over n accumulate chunk by chunk.
+void gemm_abt_cols(const double* a, const double* b, int64_t m, int64_t n, double* c, int64_t ldc, bool lower) {
+  const int64_t KC = 1024;
+  for (int64_t j = 0; j < m; ++j)
+    for (int64_t i = 0; i < m; ++i) AT(c, ldc, i, j) = 0.0;
+  std::vector<double> pa((size_t)m * KC), pb;
+  if (a != b) pb.resize((size_t)m * KC);
+  for (int64_t c0 = 0; c0 < n; c0 += KC) {
+    int kt = (int)std::min<int64_t>(KC, n - c0);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < m; ++i)
+      for (int t = 0; t < kt; ++t) {
+        pa[(size_t)i * kt + t] = AT(a, m, i, c0 + t);
+        if (a != b) pb[(size_t)i * kt + t] = AT(b, m, i, c0 + t);
+      }
+    // packed_update subtracts: accumulate −A Bᵀ and flip the sign at the end
+    packed_update(c, ldc, pa.data(), (int)m, a != b ? pb.data() : pa.data(), (int)m, kt, 0, 0, lower);
+  }
+  for (int64_t j = 0; j < m; ++j)
+    for (int64_t i = lower ? j : 0; i < m; ++i) AT(c, ldc, i, j) = -AT(c, ldc, i, j);
 }
 
 // Overwrites each column of B (n×q) with L⁻ᵀ B.
@@ -661,29 +688,23 @@ int orc_exact_eval(const int32_t* nodes, int n_nodes, const double* params, int 
   llt_inverse(f.l.data(), n, n, kinv.data(), n);
   // W = ααᵀ − K⁻¹ (form_w_lower, src/workspace.rs:351-360); lower-triangle
   // Frobenius with weight 1 on the diagonal and 2 off it (src/linalg/dense.rs:20-34).
+  // Each column's sum is formed on its own, then the columns are folded in
+  // column order (par_lower_fold, src/kernel/dist.rs:187-233), so the result
+  // does not depend on the thread count.
   int np = n_params;
-  int nthreads = orc_num_threads();
-  std::vector<double> acc((size_t)nthreads * np, 0.0);
-#pragma omp parallel
-  {
-#ifdef _OPENMP
-    int tid = omp_get_thread_num();
-#else
-    int tid = 0;
-#endif
-    double* g = &acc[(size_t)tid * np];
-#pragma omp for schedule(dynamic, 16)
-    for (int64_t j = 0; j < n; ++j) {
-      for (int64_t i = j; i < n; ++i) {
-        double w = f.alpha[i] * f.alpha[j] - AT(kinv, n, i, j);
-        double scale = (i == j) ? w : 2.0 * w;
-        node_grad(t, 0, x + i, n, x + j, n, d, scale, g);
-      }
+  std::vector<double> cols((size_t)n * np, 0.0);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t j = 0; j < n; ++j) {
+    double* g = &cols[(size_t)j * np];
+    for (int64_t i = j; i < n; ++i) {
+      double w = f.alpha[i] * f.alpha[j] - AT(kinv, n, i, j);
+      double scale = (i == j) ? w : 2.0 * w;
+      node_grad(t, 0, x + i, n, x + j, n, d, scale, g);
     }
   }
   std::vector<double> g(np, 0.0);
-  for (int th = 0; th < nthreads; ++th)
-    for (int p = 0; p < np; ++p) g[p] += acc[(size_t)th * np + p];
+  for (int64_t j = 0; j < n; ++j)
+    for (int p = 0; p < np; ++p) g[p] += cols[(size_t)j * np + p];
   for (int p = 0; p < nk; ++p) grad[p] = -0.5 * g[p];
   // noise: −½ σn² Σ W_ii (src/gpr/exact_fit.rs:676-682)
   double wdiag = 0.0;
@@ -1138,9 +1159,25 @@ struct OrcSgpr {
   // assembled state
   Mat lmm, a, bl;  // L (m×m), A (m×n), L_B (m×m)
   std::vector<double> w, ay;
-  double kdiag_sum = 0.0, afro = 0.0, kmm_jitter = 0.0, pivot_ratio = 1.0;
+  // Σ_c (k(x_c, x_c) − ‖a_c‖²), the trace term's numerator summed per point
+  // (each term is the point's Nyström residual, ≥ 0); the reference computes
+  // it as Σ k_ii − ‖A‖²_F (vfe.rs:338-369), the same sum in another
+  // association, which loses digits to cancellation at large n.
+  double trace_sum = 0.0, kmm_jitter = 0.0, pivot_ratio = 1.0;
   int last_in_place = 0;
 };
+
+static double sumsq_ld(const double* v, int64_t n) {
+  long double s = 0.0L;
+  for (int64_t i = 0; i < n; ++i) s += (long double)v[i] * v[i];
+  return (double)s;
+}
+
+static double dot_ld(const double* a, const double* b, int64_t n) {
+  long double s = 0.0L;
+  for (int64_t i = 0; i < n; ++i) s += (long double)a[i] * b[i];
+  return (double)s;
+}
 
 static double min_pivot_ratio(const Mat& l, int64_t m) {
   // min_pivot_ratio (src/sgpr/factor/updates.rs:414-427)
@@ -1182,21 +1219,35 @@ static int sgpr_assemble(OrcSgpr* h) {
   trsm_lower(h->lmm.data(), m, m, h->a.data(), n, m);
   // B = A Aᵀ + σ² I (gram_aat_plus_noise, src/linalg/dense.rs:231-239)
   h->bl.assign((size_t)m * m, 0.0);
-#pragma omp parallel for schedule(dynamic, 4)
-  for (int64_t j = 0; j < m; ++j)
-    for (int64_t i = j; i < m; ++i) {
-      double s = 0.0;
-      for (int64_t c = 0; c < n; ++c) s += AT(h->a, m, i, c) * AT(h->a, m, j, c);
-      AT(h->bl, m, i, j) = s + (i == j ? h->noise : 0.0);
-    }
+  gemm_abt_cols(h->a.data(), h->a.data(), m, n, h->bl.data(), m, true);
+  for (int64_t i = 0; i < m; ++i) AT(h->bl, m, i, i) += h->noise;
   if (!potrf(h->bl.data(), m, m)) return 1;
-  h->kdiag_sum = 0.0;
-  for (int64_t c = 0; c < n; ++c) h->kdiag_sum += kval(h->t, h->x.data() + c, n, h->x.data() + c, n, d);
-  h->afro = 0.0;
-  for (size_t q = 0; q < h->a.size(); ++q) h->afro += h->a[q] * h->a[q];
+  // Σ_c (k_cc − ‖a_c‖²) and A y, the long sums over n in long double
+  long double tr = 0.0L;
+  std::vector<long double> ay(m, 0.0L);
+#pragma omp parallel
+  {
+    long double tr_t = 0.0L;
+    std::vector<long double> ay_t(m, 0.0L);
+#pragma omp for schedule(static)
+    for (int64_t c = 0; c < n; ++c) {
+      const double* ac = &AT(h->a, m, 0, c);
+      long double ss = 0.0L;
+      for (int64_t i = 0; i < m; ++i) {
+        ss += (long double)ac[i] * ac[i];
+        ay_t[i] += (long double)ac[i] * h->y[c];
+      }
+      tr_t += (long double)kval(h->t, h->x.data() + c, n, h->x.data() + c, n, d) - ss;
+    }
+#pragma omp critical
+    {
+      tr += tr_t;
+      for (int64_t i = 0; i < m; ++i) ay[i] += ay_t[i];
+    }
+  }
+  h->trace_sum = (double)tr;
   h->ay.assign(m, 0.0);
-  for (int64_t c = 0; c < n; ++c)
-    for (int64_t i = 0; i < m; ++i) h->ay[i] += AT(h->a, m, i, c) * h->y[c];
+  for (int64_t i = 0; i < m; ++i) h->ay[i] = (double)ay[i];
   h->w = h->ay;
   llt_solve(h->bl.data(), m, m, h->w.data());
   return 0;
@@ -1235,12 +1286,10 @@ double orc_sgpr_nlml(void* p) {
   for (int64_t i = 0; i < m; ++i) ldb += std::log(AT(h->bl, m, i, i));
   ldb *= 2.0;
   double logdet = ((double)n - (double)m) * std::log(h->noise) + ldb;
-  double y2 = 0.0;
-  for (int64_t c = 0; c < n; ++c) y2 += h->y[c] * h->y[c];
-  double ayw = 0.0;
-  for (int64_t i = 0; i < m; ++i) ayw += h->ay[i] * h->w[i];
+  double y2 = sumsq_ld(h->y.data(), n);
+  double ayw = dot_ld(h->ay.data(), h->w.data(), m);
   double quad = (y2 - ayw) / h->noise;
-  double trace = (h->kdiag_sum - h->afro) / (2.0 * h->noise);
+  double trace = h->trace_sum / (2.0 * h->noise);
   return 0.5 * ((double)n * std::log(2.0 * M_PI) + logdet + quad) + trace;
 }
 
@@ -1255,23 +1304,15 @@ void orc_sgpr_grad(void* p, double* grad) {
   trsm_lower(h->bl.data(), m, m, g.data(), n, m);
   trsm_lower_t(h->bl.data(), m, m, g.data(), n, m);
   std::vector<double> r(n);
-  for (int64_t c = 0; c < n; ++c) {
-    double s = h->y[c];
-    for (int64_t i = 0; i < m; ++i) s -= AT(h->a, m, i, c) * h->w[i];
-    r[c] = s;
-  }
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < n; ++c) r[c] = h->y[c] - dot_ld(&AT(h->a, m, 0, c), h->w.data(), m);
   double inv = 1.0 / noise;
+#pragma omp parallel for schedule(static)
   for (int64_t c = 0; c < n; ++c)
     for (int64_t i = 0; i < m; ++i) AT(g, m, i, c) -= (h->w[i] * r[c] + AT(h->a, m, i, c)) * inv;
   // H = G Aᵀ (m×m)
   Mat hh((size_t)m * m, 0.0);
-#pragma omp parallel for schedule(static)
-  for (int64_t j = 0; j < m; ++j)
-    for (int64_t i = 0; i < m; ++i) {
-      double s = 0.0;
-      for (int64_t c = 0; c < n; ++c) s += AT(g, m, i, c) * AT(h->a, m, j, c);
-      AT(hh, m, i, j) = s;
-    }
+  gemm_abt_cols(g.data(), h->a.data(), m, n, hh.data(), m, false);
   // w_mn = L⁻ᵀ G
   trsm_lower_t(h->lmm.data(), m, m, g.data(), n, m);
   // X = tril½(H); X ← L⁻ᵀ X; Xt = Xᵀ; Xt ← L⁻ᵀ Xt; w_mm = −½(Xt + Xtᵀ)
@@ -1295,35 +1336,31 @@ void orc_sgpr_grad(void* p, double* grad) {
       double s = (i == j ? 1.0 : 2.0) * AT(wmm, m, i, j);
       node_grad(h->t, 0, h->z.data() + i, m, h->z.data() + j, m, d, s, gk.data());
     }
-  // ⟨w_mn, ∂K(Z, X)⟩ over the full rectangle (add_cross_contraction_mn)
-  int nthreads = orc_num_threads();
-  std::vector<double> acc((size_t)nthreads * nk, 0.0);
+  // ⟨w_mn, ∂K(Z, X)⟩ over the full rectangle (add_cross_contraction_mn) and
+  // w_diag Σ ∂k(x_c, x_c) (add_diag_contraction): one column of sums per
+  // point, the columns summed in long double
+  std::vector<long double> gl(nk, 0.0L);
 #pragma omp parallel
   {
-#ifdef _OPENMP
-    int tid = omp_get_thread_num();
-#else
-    int tid = 0;
-#endif
+    std::vector<long double> gt(nk, 0.0L);
+    std::vector<double> gc(nk);
 #pragma omp for schedule(static)
-    for (int64_t c = 0; c < n; ++c)
+    for (int64_t c = 0; c < n; ++c) {
+      std::fill(gc.begin(), gc.end(), 0.0);
       for (int64_t i = 0; i < m; ++i)
-        node_grad(h->t, 0, h->z.data() + i, m, h->x.data() + c, n, d, AT(g, m, i, c),
-                  &acc[(size_t)tid * nk]);
+        node_grad(h->t, 0, h->z.data() + i, m, h->x.data() + c, n, d, AT(g, m, i, c), gc.data());
+      node_grad(h->t, 0, h->x.data() + c, n, h->x.data() + c, n, d, wdiag, gc.data());
+      for (int q = 0; q < nk; ++q) gt[q] += gc[q];
+    }
+#pragma omp critical
+    for (int q = 0; q < nk; ++q) gl[q] += gt[q];
   }
-  for (int th = 0; th < nthreads; ++th)
-    for (int q = 0; q < nk; ++q) gk[q] += acc[(size_t)th * nk + q];
-  // w_diag Σ ∂k(x_i, x_i) (add_diag_contraction)
-  for (int64_t c = 0; c < n; ++c)
-    node_grad(h->t, 0, h->x.data() + c, n, h->x.data() + c, n, d, wdiag, gk.data());
-  for (int q = 0; q < nk; ++q) grad[q] = gk[q];
+  for (int q = 0; q < nk; ++q) grad[q] = (double)((long double)gk[q] + gl[q]);
   // directional_noise (derivatives.rs:186-202) with d_noise = σ²
-  double y2 = 0.0;
-  for (int64_t c = 0; c < n; ++c) y2 += h->y[c] * h->y[c];
-  double ayw = 0.0;
-  for (int64_t i = 0; i < m; ++i) ayw += h->ay[i] * h->w[i];
+  double y2 = sumsq_ld(h->y.data(), n);
+  double ayw = dot_ld(h->ay.data(), h->w.data(), m);
   double quad = (y2 - ayw) / noise;
-  double trace = (h->kdiag_sum - h->afro) / (2.0 * noise);
+  double trace = h->trace_sum / (2.0 * noise);
   // trace_solve(L_B, σ² I) = σ² tr(B⁻¹)
   Mat binv((size_t)m * m, 0.0);
   llt_inverse(h->bl.data(), m, m, binv.data(), m);
@@ -1331,8 +1368,7 @@ void orc_sgpr_grad(void* p, double* grad) {
   for (int64_t i = 0; i < m; ++i) trb += AT(binv, m, i, i);
   double dn = noise;
   double d_logdet_b = dn * trb;
-  double ww = 0.0;
-  for (int64_t i = 0; i < m; ++i) ww += h->w[i] * h->w[i];
+  double ww = sumsq_ld(h->w.data(), m);
   double d_q = -dn * ww;
   double d_quad = -d_q / noise - quad * dn / noise;
   double d_trace = -trace * dn / noise;
@@ -1437,8 +1473,7 @@ int orc_sgpr_insert(void* p, const double* xnew, double ynew, uint64_t* id) {
   for (int64_t i = 0; i < m; ++i) v[i] = kval(h->t, h->z.data() + i, m, xnew, 1, d);
   trsm_lower(h->lmm.data(), m, m, v.data(), 1, m);
   double kd = kval(h->t, xnew, 1, xnew, 1, d);
-  for (int64_t i = 0; i < m; ++i) h->afro += v[i] * v[i];
-  h->kdiag_sum += kd;
+  h->trace_sum += (double)((long double)kd - (long double)sumsq_ld(v.data(), m));
   for (int64_t i = 0; i < m; ++i) h->ay[i] += v[i] * ynew;
   Mat na((size_t)m * (n + 1));
   std::copy(h->a.begin(), h->a.end(), na.begin());
@@ -1477,8 +1512,7 @@ int orc_sgpr_delete(void* p, uint64_t id) {
   for (int64_t i = 0; i < m; ++i) v[i] = AT(h->a, m, i, idx);
   const double* xp_base = h->x.data() + idx;
   double kd = kval(h->t, xp_base, n, xp_base, n, d);
-  double coln = 0.0;
-  for (int64_t i = 0; i < m; ++i) coln += v[i] * v[i];
+  double coln = sumsq_ld(v.data(), m);
   std::vector<double> nx((size_t)(n - 1) * d);
   for (int f = 0; f < d; ++f) {
     int64_t o = 0;
@@ -1508,8 +1542,7 @@ int orc_sgpr_delete(void* p, uint64_t id) {
   double yi = h->y[idx];
   h->ids.erase(h->ids.begin() + idx);
   if (ok) {
-    h->kdiag_sum -= kd;
-    h->afro -= coln;
+    h->trace_sum -= (double)((long double)kd - (long double)coln);
     for (int64_t i = 0; i < m; ++i) h->ay[i] -= v[i] * yi;
     Mat na((size_t)m * (n - 1));
     int64_t o = 0;

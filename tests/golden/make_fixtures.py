@@ -12,7 +12,7 @@ Two sources:
    reference's `compare/generate.py`: `GaussianProcessRegressor(optimizer=None)`),
    which also pin the noise gradient through a WhiteKernel term.
 
-Usage:  python tests/golden/make_fixtures.py [REFERENCE_CHECKOUT]
+Usage:  python tests/golden/make_fixtures.py REFERENCE_CHECKOUT
 Nothing at test time reads the reference; only these committed JSON files.
 """
 
@@ -222,7 +222,9 @@ def dump(name, obj):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py <gprx checkout>")
+    ref = sys.argv[1]
     gold = os.path.join(ref, "compare", "goldens")
     dump("exact_goldens.json", exact_cases(gold))
     dump("sklearn_goldens.json", sklearn_cases())

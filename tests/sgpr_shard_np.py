@@ -5,7 +5,8 @@ be checked without a GPU).
 
 It restates, for an RbfArd kernel, the same decomposition the CUDA shard
 phases use (sgpr.cu): exchange 1 carries this shard's B_s = A_s A_sᵀ,
-A_s y_s, ‖A_s‖²_F, Σ y_s² and n_s; exchange 2 carries H_s = G_s A_sᵀ and the
+A_s y_s, Σ_c (k_cc − ‖a_c‖²) over the shard's points (RbfArd: k_cc = 1),
+Σ y_s² and n_s; exchange 2 carries H_s = G_s A_sᵀ and the
 cross-term gradient ⟨L⁻ᵀ G_s, ∂K(Z, X_s)⟩, with
 G_s = B⁻¹A_s − (w r_sᵀ + A_s)/σ², r_s = y_s − A_sᵀ w (the VFE adjoint of
 src/sgpr/factor/derivatives.rs:102-144, 283-366).
@@ -49,7 +50,7 @@ class NumpyShard:
         e = ex1.numpy()
         e[:m * m] = np.tril(self.A @ self.A.T).reshape(-1, order="F")
         e[m * m:m * m + m] = self.A @ self.y
-        e[m * m + m] = (self.A ** 2).sum()
+        e[m * m + m] = (1.0 - (self.A ** 2).sum(axis=0)).sum()
         e[m * m + m + 1] = (self.y ** 2).sum()
         e[m * m + m + 2] = self.x.shape[0]
 
@@ -60,12 +61,12 @@ class NumpyShard:
         B = np.tril(low) + np.tril(low, -1).T + self.s2 * np.eye(m)
         self.B = B
         self.ay = e[m * m:m * m + m].copy()
-        self.afro, self.y2, self.nt = e[m * m + m], e[m * m + m + 1], e[m * m + m + 2]
+        self.tsum, self.y2, self.nt = e[m * m + m], e[m * m + m + 1], e[m * m + m + 2]
         LB = np.linalg.cholesky(B)
         self.w = np.linalg.solve(B, self.ay)
         logdet = (self.nt - m) * math.log(self.s2) + 2.0 * np.log(np.diag(LB)).sum()
         quad = (self.y2 - self.ay @ self.w) / self.s2
-        trace = (self.nt * 1.0 - self.afro) / (2.0 * self.s2)
+        trace = self.tsum / (2.0 * self.s2)
         nl = 0.5 * (self.nt * math.log(2 * math.pi) + logdet + quad) + trace
         if ex2 is not None:
             r = self.y - self.A.T @ self.w
@@ -95,7 +96,7 @@ class NumpyShard:
         trb = np.trace(np.linalg.inv(self.B))
         ww = self.w @ self.w
         quad = (self.y2 - self.ay @ self.w) / s2
-        trace = (self.nt - self.afro) / (2.0 * s2)
+        trace = self.tsum / (2.0 * s2)
         d_quad = s2 * ww / s2 - quad
         g[d] = 0.5 * ((self.nt - m) + s2 * trb + d_quad) - trace
         return g

@@ -106,8 +106,8 @@ def test_online_model_loo_and_covariance():
     for kind in (0, 1):
         p = on.loo_predict_with(gx.PredictOptions(kind))
         mo, vo = O.exact_loo(NODES, PARAMS, col(xa), n, 2, ya, kind)
-        assert np.all(O.rel_err(p.mean, mo) <= 1e-9) and np.all(O.rel_err(p.variance, vo) <= 1e-9)
+        assert np.all(O.rel_err(p.mean, mo) <= TOL) and np.all(O.rel_err(p.variance, vo) <= TOL)
     xs = np.random.RandomState(1).uniform(0, 4, size=(12, 2))
     c = on.predict_covariance(col(xs), 12, 2)
     mo, co = O.exact_covariance(NODES, PARAMS, col(xa), n, 2, ya, col(xs), 12, 1)
-    assert np.all(O.rel_err(c.mean, mo) <= 1e-9) and np.all(O.rel_err(c.covariance, co) <= 1e-9)
+    assert np.all(O.rel_err(c.mean, mo) <= TOL) and np.all(O.rel_err(c.covariance, co) <= TOL)

@@ -91,4 +91,4 @@ def test_sgpr_jitter_policy_reaches_the_device():
         gx.Fixed()).factor(x, n, d, y, z, m)
     orc = O.Sgpr(nodes, params, x, n, d, y, z, m, jitter=(0, 1e-6, 1.0, 0, 1e-6))
     assert f.kmm_jitter() == orc.kmm_jitter == 1e-6
-    assert O.rel_err(f.neg_log_marginal_likelihood(), orc.nlml()) <= 1e-9
+    assert O.rel_err(f.neg_log_marginal_likelihood(), orc.nlml()) <= 1e-10

@@ -1,8 +1,9 @@
 """GPU parity of the VFE sparse GPR path through the C ABI.
 
 Goldens: GPyTorch SGPR (tests/sparse_gpytorch.rs, tests/online_sgpr_gpytorch.rs)
-at 1e-8; everything else against the CPU oracle at 1e-10 (NLML, moments) and
-1e-9 (gradient), measured as |a − e| / max(|e|, 1).
+at 1e-8; everything else against the CPU oracle at 1e-10 (NLML, gradient,
+moments), measured as |a − e| / max(|e|, 1), from n = 80 to n = 10⁵ with
+m = 1024.
 """
 
 import itertools
@@ -102,7 +103,7 @@ def test_sgpr_eval_matches_oracle(n, m, tree):
     assert f.kmm_jitter() == orc.kmm_jitter
     nl, g = f.value_and_gradient(params)
     assert O.rel_err(nl, orc.nlml()) <= TOL, (nl, orc.nlml())
-    assert np.all(O.rel_err(g, orc.grad()) <= 1e-9), (g, orc.grad())
+    assert np.all(O.rel_err(g, orc.grad()) <= TOL), (g, orc.grad())
     q = 23
     xs = (rs.uniform(0, 1, size=(q, d)) * hi).T.reshape(-1)
     for kind in (0, 1):
@@ -110,6 +111,32 @@ def test_sgpr_eval_matches_oracle(n, m, tree):
         p = f.predict_with(xs, q, d, gx.PredictOptions(kind))
         assert np.all(O.rel_err(p.mean, mo) <= TOL)
         assert np.all(O.rel_err(p.variance, vo) <= TOL)
+
+
+@pytest.mark.parametrize("n,tree", [(20000, 1), (20000, 3), (40000, 1), (40000, 3), (100000, 1)])
+def test_sgpr_eval_large_n_matches_oracle(n, tree):
+    # m = 1024 inducing inputs and n up to 10⁵: the sums over n (the trace
+    # term's Nyström residuals, ‖y‖², A y, the cross contraction) keep 1e-10
+    m = 1024
+    d, nodes, theta, spacing = TREES[tree]
+    rs = np.random.RandomState(n + 7 * tree)
+    zp = grid(m, d, 1.6 * spacing, rs)
+    hi = zp.max(axis=0) + 0.5 * spacing
+    x = (rs.uniform(0, 1, size=(n, d)) * hi).T.reshape(-1)
+    y = np.sin(6 * x[:n]) + 0.1 * rs.standard_normal(n)
+    z = zp.T.reshape(-1)
+    params = np.array(theta + [math.log(0.05)])
+    orc = O.Sgpr(nodes, params, x, n, d, y, z, m)
+    f = model(nodes, theta, 0.05, x, n, d, y, z, m)
+    assert f.kmm_jitter() == orc.kmm_jitter
+    nl, g = f.value_and_gradient(params)
+    assert O.rel_err(nl, orc.nlml()) <= TOL, (nl, orc.nlml())
+    assert np.all(O.rel_err(g, orc.grad()) <= TOL), (g, orc.grad())
+    q = 23
+    xs = (rs.uniform(0, 1, size=(q, d)) * hi).T.reshape(-1)
+    mo, vo = orc.predict(xs, q, 1)
+    p = f.predict(xs, q, d)
+    assert np.all(O.rel_err(p.mean, mo) <= TOL) and np.all(O.rel_err(p.variance, vo) <= TOL)
 
 
 @pytest.mark.parametrize("case", load("online_sgpr_goldens.json"), ids=lambda c: c["name"])
@@ -176,11 +203,11 @@ def test_online_sgpr_sequence_matches_oracle():
             orc.delete(pid)
         assert on.last_step_in_place() == bool(orc.last_in_place)
         assert np.array_equal(on.point_ids(), np.array(ids, dtype=np.uint64))
-        assert O.rel_err(on.neg_log_marginal_likelihood(), orc.nlml()) <= 1e-9
+        assert O.rel_err(on.neg_log_marginal_likelihood(), orc.nlml()) <= TOL
         pm = on.predict(xs, 7, d)
         mo, vo = orc.predict(xs, 7, 1)
-        assert np.all(O.rel_err(pm.mean, mo) <= 1e-9)
-        assert np.all(O.rel_err(pm.variance, vo) <= 1e-9)
+        assert np.all(O.rel_err(pm.mean, mo) <= TOL)
+        assert np.all(O.rel_err(pm.variance, vo) <= TOL)
 
 
 def test_sgpr_fit_decreases_nlml_and_matches_oracle_at_optimum():
@@ -196,7 +223,7 @@ def test_sgpr_fit_decreases_nlml_and_matches_oracle_at_optimum():
     nl = f.neg_log_marginal_likelihood()
     assert nl < start
     orc = O.Sgpr([[11, 2]], p, x, n, d, y, z, m)
-    assert O.rel_err(nl, orc.nlml()) <= 1e-9
+    assert O.rel_err(nl, orc.nlml()) <= TOL
     g0 = O.Sgpr([[11, 2]], s.kernel.get_params() + [math.log(0.5)], x, n, d, y, z, m).grad()
     assert np.linalg.norm(orc.grad()) < 1e-2 * np.linalg.norm(g0)
 
