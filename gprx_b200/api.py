@@ -1354,6 +1354,74 @@ class GprBatch:
                         np.array([r.converged for r in reps], dtype=bool), st)
 
 
+def partition_by_cost(sizes, parts):
+    """Splits problem indices 0..len(sizes)-1 into `parts` shards balanced by
+    Σ n_i³ (an evaluation's work per problem is O(n_i³)): longest processing
+    time first — problems by decreasing n³ (ties by index), each to the shard
+    with the least work so far (ties to the lower shard).  Returns one sorted
+    index array per shard; every problem is in exactly one shard."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    parts = int(parts)
+    if parts < 1:
+        raise InvalidConfig("at least one shard")
+    cost = sizes.astype(np.float64) ** 3
+    order = sorted(range(sizes.size), key=lambda i: (-cost[i], i))
+    load = [0.0] * parts
+    out = [[] for _ in range(parts)]
+    for i in order:
+        k = min(range(parts), key=lambda j: (load[j], j))
+        out[k].append(i)
+        load[k] += cost[i]
+    return [np.array(sorted(o), dtype=np.int64) for o in out]
+
+
+def sharded_batch_fit(kernel, xs, ys, d, params0, rank, world, all_gather_object, optimizer=None, device=0,
+                      jitter=None, batch_factory=None):
+    """GprBatch.fit over problems split across processes (one GPU each).
+
+    Every process passes the same problem list; partition_by_cost gives
+    process `rank` its shard, which it fits on `device` in one GprBatch
+    (batch_factory(kernel, xs, ys, d, jitter, device) builds it; GprBatch by
+    default).  all_gather_object(out_list, obj) gathers one object per process
+    (torch.distributed.all_gather_object); it is the only exchange, once at
+    the end.  Returns the BatchFit of all problems in their original order,
+    the same on every process."""
+    n = len(xs)
+    if len(ys) != n or n == 0:
+        raise ShapeMismatch("xs and ys must be non-empty lists of the same length")
+    p0 = np.asarray(params0, dtype=np.float64)
+    if p0.ndim != 2 or p0.shape[0] != n:
+        raise ShapeMismatch("params0 must hold one row per problem")
+    sizes = [np.asarray(y).size for y in ys]
+    shard = partition_by_cost(sizes, world)[int(rank)]
+    mine = None
+    if shard.size:
+        make = batch_factory if batch_factory is not None else (
+            lambda k, x, y, dd, j, dev: GprBatch(k, x, y, dd, jitter=j, device=dev))
+        b = make(kernel, [xs[i] for i in shard], [ys[i] for i in shard], d, jitter, device)
+        r = b.fit(p0[shard], optimizer)
+        mine = (shard, r.params, r.nlml, r.iterations, r.evaluations, r.grad_norm, r.converged, r.status)
+    got = [None] * int(world)
+    all_gather_object(got, mine)
+    p = p0.shape[1]
+    params = np.zeros((n, p))
+    nlml = np.zeros(n)
+    iters = np.zeros(n, dtype=np.int64)
+    evals = np.zeros(n, dtype=np.int64)
+    gnorm = np.zeros(n)
+    conv = np.zeros(n, dtype=bool)
+    status = np.full(n, -1, dtype=np.int32)
+    for part in got:
+        if part is None:
+            continue
+        idx = part[0]
+        params[idx], nlml[idx], iters[idx], evals[idx] = part[1], part[2], part[3], part[4]
+        gnorm[idx], conv[idx], status[idx] = part[5], part[6], part[7]
+    if np.any(status < 0):
+        raise InvalidConfig("a problem came back from no shard (ranks passed different problem lists?)")
+    return BatchFit(params, nlml, iters, evals, gnorm, conv, status)
+
+
 # ---------------------------------------------------------------------------
 # serving: a request loop over resident exact models
 # ---------------------------------------------------------------------------
