@@ -989,6 +989,7 @@ struct NoAllocHeader {
   BatchHeader hdr;
   int order[1];
   int status[1];
+  int input_bad[1];
   double log_theta[BATCH_MAX_VARS];
   double nlml[1];
   double grad[BATCH_MAX_VARS];
@@ -1006,16 +1007,33 @@ struct NoAllocTheta {
   double v[BATCH_MAX_VARS];
 };
 
+constexpr int NOALLOC_PREP_THREADS = 256;
+
 // Writes the header of this call (everything the evaluation reads that must
-// start fresh: the queue counter, the problem, θ, the status).
-__global__ void noalloc_prep_kernel(double* scratch, BatchProblem prob, NoAllocTheta th, int p) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// start fresh: the queue counter, the problem, θ, the status) and checks the
+// caller's x and y for non-finite values, which the host cannot see here
+// (TrainInput::validate, src/data.rs).
+__global__ void __launch_bounds__(NOALLOC_PREP_THREADS) noalloc_prep_kernel(double* scratch, BatchProblem prob,
+                                                                            NoAllocTheta th, int p, int d) {
+  __shared__ int bad;
   NoAllocHeader* h = reinterpret_cast<NoAllocHeader*>(scratch);
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  const long long nx = (long long)prob.n * d;
+  int mine = 0;
+  for (long long i = threadIdx.x; i < nx + prob.n; i += blockDim.x) {
+    double v = i < nx ? prob.x[i] : prob.y[i - nx];
+    if (!isfinite(v)) mine = 1;
+  }
+  if (mine) atomicOr(&bad, 1);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   h->prob = prob;
   h->hdr.queue = 0;
   h->hdr.active = 0;
   h->order[0] = 0;
   h->status[0] = GPRX_NOT_CONVERGED;  // overwritten by the evaluation
+  h->input_bad[0] = bad;
   h->nlml[0] = 0.0;
   for (int i = 0; i < BATCH_MAX_VARS; ++i) {
     h->log_theta[i] = i < p ? th.v[i] : 0.0;
@@ -1026,11 +1044,12 @@ __global__ void noalloc_prep_kernel(double* scratch, BatchProblem prob, NoAllocT
 __global__ void noalloc_finish_kernel(const double* scratch, int p, double* nlml, double* grad, int32_t* status) {
   const NoAllocHeader* h = reinterpret_cast<const NoAllocHeader*>(scratch);
   const int i = threadIdx.x;
+  const int st = h->input_bad[0] ? (int)GPRX_NONFINITE_INPUT : h->status[0];
   if (i == 0) {
-    *status = h->status[0];
-    *nlml = h->status[0] == GPRX_OK ? h->nlml[0] : 0.0;
+    *status = st;
+    *nlml = st == GPRX_OK ? h->nlml[0] : 0.0;
   }
-  if (grad && i < p) grad[i] = h->status[0] == GPRX_OK ? h->grad[i] : 0.0;
+  if (grad && i < p) grad[i] = st == GPRX_OK ? h->grad[i] : 0.0;
 }
 
 // Device address of g_noalloc_scratch on the current device, looked up once
@@ -1058,12 +1077,42 @@ static gprx_status noalloc_scratch_ptr(int dev, double** out) {
   return GPRX_OK;
 }
 
+// Makes `dev` the current device for the life of the guard.
+struct NoAllocDeviceGuard {
+  int prev = -1;
+  cudaError_t set(int dev) {
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return e;
+    return prev == dev ? cudaSuccess : cudaSetDevice(dev);
+  }
+  ~NoAllocDeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
 static gprx_status exact_eval_noalloc(const double* x, const double* y, uint64_t n, uint64_t d,
                                       const gprx_kernel_node* nodes, int32_t n_nodes, const double* params,
                                       uint64_t p, const gprx_options* opts, double* nlml, double* grad,
                                       int32_t* status, void* stream) {
+  // The scratch and the launch belong to the device that owns the stream
+  // (the current device for the NULL stream); options.device must name it.
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0;
+  if (s) {
+    GPRX_CUDA_TRY(cudaStreamGetDevice(s, &dev));
+  } else {
+    GPRX_CUDA_TRY(cudaGetDevice(&dev));
+  }
+  if (opts && opts->device != dev)
+    return set_error(GPRX_INVALID_CONFIG, "options.device must be the device that owns the stream");
+  NoAllocDeviceGuard guard;
+  GPRX_CUDA_TRY(guard.set(dev));
+  double* scratch = nullptr;
+  gprx_status st = noalloc_scratch_ptr(dev, &scratch);
+  if (st != GPRX_OK) return st;
+  if (n == 0) return GPRX_OK;  // set-up only: nothing is enqueued
   if (!x || !y || !nodes || !params || !nlml || !status) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
-  if (n == 0) return set_error(GPRX_EMPTY_INPUT, "no training points");
   if (d == 0) return set_error(GPRX_EMPTY_INPUT, "no features (d = 0)");
   if (n > (uint64_t)NOALLOC_MAX_N)
     return set_error(GPRX_CAPACITY, "gprx_exact_eval_noalloc takes at most 512 points (its fixed scratch size); "
@@ -1077,12 +1126,8 @@ static gprx_status exact_eval_noalloc(const double* x, const double* y, uint64_t
     return set_error(GPRX_INVALID_CONFIG, "at most 8 jitter retries");
   HostKernel kern;
   std::string why;
-  gprx_status st = kern.init(nodes, n_nodes, params, (int)p - 1, (int)d, &why);
+  st = kern.init(nodes, n_nodes, params, (int)p - 1, (int)d, &why);
   if (st != GPRX_OK) return set_error(st, why);
-  int dev = 0;
-  GPRX_CUDA_TRY(cudaGetDevice(&dev));
-  double* scratch = nullptr;
-  if ((st = noalloc_scratch_ptr(dev, &scratch)) != GPRX_OK) return st;
   NoAllocHeader* h = reinterpret_cast<NoAllocHeader*>(scratch);  // a device address
   BatchProblem prob{x, y, (int)n, 0};
   NoAllocTheta th{};
@@ -1104,9 +1149,8 @@ static gprx_status exact_eval_noalloc(const double* x, const double* y, uint64_t
   a.jit = jitter_list(o);
   a.tmpl = kern.tree;
   for (int i = 0; i < 64; ++i) a.slot_param[i] = i < (int)kern.slot_param.size() ? kern.slot_param[i] : -1;
-  cudaStream_t s = (cudaStream_t)stream;
   const size_t smem = batch_smem();
-  noalloc_prep_kernel<<<1, 32, 0, s>>>(scratch, prob, th, (int)p);
+  noalloc_prep_kernel<<<1, NOALLOC_PREP_THREADS, 0, s>>>(scratch, prob, th, (int)p, (int)d);
   switch (kern.ard_d) {
     case 0: batch_eval_kernel<0><<<1, BT, smem, s>>>(a); break;
     case 4: batch_eval_kernel<4><<<1, BT, smem, s>>>(a); break;

@@ -4,8 +4,8 @@
  *
  * The reference (gprx 0.2.0, a Rust crate) has no FFI layer: its seams are
  * Rust traits.  Each entry point below names the reference function whose
- * work it takes over; a Rust `cuda` backend calls it from that seam (the
- * binding is shown in INTEGRATION.md).
+ * work it takes over; a Rust `cuda` backend calls it from that seam through
+ * an `extern "C"` block that mirrors these declarations.
  *
  * Conventions
  *  - Every call returns a gprx_status.  No exception, abort or panic crosses
@@ -525,15 +525,25 @@ gprx_status gprx_server_stats(gprx_server* s, gprx_server_stats_t* out);
  *    are DEVICE pointers owned by the caller; params (log θ, p values) and the
  *    kernel tree are host memory read during the call.
  *  - n ≤ 512 and p ≤ 16; larger requests return GPRX_CAPACITY / INVALID_CONFIG.
- *  - The work is enqueued on `stream` (a cudaStream_t; NULL = default stream)
- *    and the call returns without waiting: *status (a gprx_status) and the
+ *  - The work is enqueued on `stream` (a cudaStream_t; NULL = the current
+ *    device's default stream) and runs on the device that owns the stream.
+ *    The call returns without waiting: *status (a gprx_status) and the
  *    results are valid once the stream reaches them.  On a failed evaluation
- *    *status says why and nlml / grad are written as 0.
+ *    *status says why and nlml / grad are written as 0; a NaN or infinity in
+ *    x or y gives GPRX_NONFINITE_INPUT.
+ *  - Of `options` (NULL = gprx_options_default) the jitter fields and
+ *    `device` are read; `device` must be the stream's device, else the call
+ *    returns GPRX_INVALID_CONFIG without enqueuing work.
  *  - The scratch is one fixed 5.3 MB array in device memory per GPU, shared by
  *    every call: calls whose work overlaps on the GPU (other streams, other
- *    threads) race and must be ordered by the caller.  The first call on a
- *    device looks up that array's address and sets the kernel's shared-memory
- *    limit; make that first call before any stream capture.
+ *    threads) race and must be ordered by the caller.  Each call starts from
+ *    a fresh header, so the previous call's leftovers (another n, a failed
+ *    factor) do not reach its result.
+ *  - Set-up: the first call on a device looks up the array's device address
+ *    and sets the kernel's shared-memory limit.  A call with n = 0 does only
+ *    that (x, y, the kernel tree and the outputs are not read, nothing is
+ *    enqueued) and returns GPRX_OK; make it, or any first call, before a
+ *    stream capture begins.
  *  - Same result as gprx_batch_eval / gprx_exact_eval of the same problem
  *    (one CTA evaluates it in a fixed order). */
 gprx_status gprx_exact_eval_noalloc(const double* x, const double* y, uint64_t n, uint64_t d,
