@@ -10,19 +10,26 @@ namespace gprx {
 constexpr int NB_DIAG = 128;
 
 // ---------------------------------------------------------------------------
-// Diagonal block (nb ≤ 128): LLT and the block's inverse in shared memory.
-// The block is padded to a multiple of 32 with an identity tail.
-//   per 32-column sub-panel p:
-//     warp 0 factors the 32×32 diagonal sub-block in registers (lane = row,
-//     pivots broadcast by shuffles) and inverts it (lane = column);
-//     all warps (DMMA m16n8k4): P = A_below · L_pp⁻ᵀ, then A22 −= P Pᵀ.
-//   inverse, column blocks right to left from X L = I (DMMA):
-//     X_ij = −(Σ_{k=j+1..i} X_ik L_kj) X_jj, in place.
+// Diagonal block (nb ≤ 128): LLT and the block's inverse in shared memory,
+// one CTA of FD_THREADS threads.  The block is padded to a multiple of 16
+// with an identity tail.
+//   factor, per 16-column panel p (right-looking, with look-ahead inside the
+//   CTA):
+//     warp 0 factors the 16×16 leaf in registers (lane = row, pivots by
+//     shuffles) and keeps the reciprocal pivots; meanwhile warps 1..7 apply
+//     the previous panel's trailing update (DMMA m16n8k4, K = 16) to the rest
+//     of the block;
+//     all warps: the panel below the leaf by column-oriented substitution
+//     (lane = row, L entries broadcast from shared memory);
+//     warp 0: the next leaf's own update, then its factor.
+//   inverse (off the chain): every warp inverts one 16×16 leaf, then
+//   recursive doubling 16 → 32 → 64 → 128 on DMMA:
+//     X21 = −X22 (L21 X11), in place.
 // ---------------------------------------------------------------------------
 constexpr int FD_THREADS = 256;
-constexpr int SB = 32;          // sub-panel width
+constexpr int LF = 16;               // leaf / panel width
 constexpr int FLS = NB_DIAG + 4;     // ld of the block (≡ 4 mod 16: conflict-free fragments)
-constexpr int XLD = SB + 4;     // ld of a 32×32 scratch block
+constexpr int TMP_DOUBLES = 64 * 68; // the doubling step's T (ld h + 4 ≡ 4 mod 16)
 
 // C(16×8) += A(16×K) · B(K×8) with A(i,k) = a[i·ai + k·ak], B(k,j) = b[k·bk + j·bj].
 __device__ __forceinline__ void mma_tile_smem(double (&c)[4], const double* a, int ai, int ak, const double* b, int bk,
@@ -37,12 +44,11 @@ __device__ __forceinline__ void mma_tile_smem(double (&c)[4], const double* a, i
   }
 }
 
-// 16×16 leaf, one warp: lanes r and r+16 both hold row r of the block at
+// 16×16 leaf LLT, one warp: lanes r and r+16 both hold row r of the block at
 // (off, off) of s in registers; pivots are broadcast by shuffles.  Writes L
-// back to s and L⁻¹ (column-major, ld XLD) to xo.  Returns the failing column
-// or −1.  Kept out of line so one compact copy serves every call (the fully
-// unrolled 32-wide form overflowed the instruction cache).
-static __device__ __noinline__ int leaf16_factor_inv(double* s, int off, double* xo) {
+// back to s and 1/L_jj to rinv[off + j].  Returns the failing column or −1
+// (uniform over the warp).  Out of line: one compact copy for every panel.
+static __device__ __noinline__ int leaf16_factor(double* s, int off, double* rinv) {
   const int lane = threadIdx.x & 31, r = lane & 15;
   double d[16];
 #pragma unroll
@@ -73,105 +79,28 @@ static __device__ __noinline__ int leaf16_factor_inv(double* s, int off, double*
 #pragma unroll
     for (int c = 0; c < 16; ++c)
       if (c <= r) s[(off + r) + (off + c) * FLS] = d[c];
-  }
-  double x[16];
-#pragma unroll
-  for (int q = 0; q < 16; ++q) {
-    double acc = (q == r) ? 1.0 : 0.0;
-#pragma unroll
-    for (int t = 0; t < 16; ++t)
-      if (t < q) acc = fma(-__shfl_sync(0xffffffffu, d[t], q), x[t], acc);
-    x[q] = acc * __shfl_sync(0xffffffffu, my_inv, q);
-  }
-  if (lane < 16) {
-#pragma unroll
-    for (int q = 0; q < 16; ++q) xo[q + r * XLD] = x[q];
+    rinv[off + r] = my_inv;
   }
   __syncwarp();
   return -1;
 }
 
-// Factor + invert the 32×32 sub-block at (c0, c0) of s with one warp, as two
-// 16×16 leaves: L21 = A21 X11ᵀ, A22 −= L21 L21ᵀ, then X21 = −X22 (L21 X11),
-// the products on DMMA.  L goes back to s, L⁻¹ to xd (ld XLD, zero above the
-// diagonal).  Returns the failing column or −1 (uniform over the warp).
-__device__ __forceinline__ int warp_factor_inv32(double* s, int c0, double* xd) {
-  const int lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
-  int f = leaf16_factor_inv(s, c0, xd);
-  if (f >= 0) return f;
-  // L21 = A21 · X11ᵀ  (B(k, j) = X11(j, k))
-  double c[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
-#pragma unroll
-  for (int tn = 0; tn < 2; ++tn) mma_tile_smem(c[tn], s + (c0 + 16) + c0 * FLS, 1, FLS, xd + 8 * tn, XLD, 1, 16);
-  __syncwarp();
-#pragma unroll
-  for (int tn = 0; tn < 2; ++tn) {
-    int row = c0 + 16 + g, col = c0 + 8 * tn + 2 * t4;
-    s[row + col * FLS] = c[tn][0];
-    s[row + (col + 1) * FLS] = c[tn][1];
-    s[(row + 8) + col * FLS] = c[tn][2];
-    s[(row + 8) + (col + 1) * FLS] = c[tn][3];
-  }
-  __syncwarp();
-  // A22 −= L21 L21ᵀ (lower part)
-#pragma unroll
-  for (int tn = 0; tn < 2; ++tn) {
-    double u[4] = {0, 0, 0, 0};
-    mma_tile_smem(u, s + (c0 + 16) + c0 * FLS, 1, FLS, s + (c0 + 16 + 8 * tn) + c0 * FLS, FLS, 1, 16);
-    int i = g, j = 8 * tn + 2 * t4;  // within the 16×16 block
-    double* b = s + (c0 + 16) + (c0 + 16) * FLS;
-    if (i >= j) b[i + j * FLS] -= u[0];
-    if (i >= j + 1) b[i + (j + 1) * FLS] -= u[1];
-    if (i + 8 >= j) b[(i + 8) + j * FLS] -= u[2];
-    if (i + 8 >= j + 1) b[(i + 8) + (j + 1) * FLS] -= u[3];
-  }
-  __syncwarp();
-  f = leaf16_factor_inv(s, c0 + 16, xd + 16 + 16 * XLD);
-  if (f >= 0) return 16 + f;
-  // T = L21 · X11 into the (zero) upper-right quarter of xd, then
-  // X21 = −X22 · T, and the quarter back to zero
-  double* T = xd + 16 * XLD;  // rows 0..15, columns 16..31
-#pragma unroll
-  for (int tn = 0; tn < 2; ++tn) {
-    double u[4] = {0, 0, 0, 0};
-    mma_tile_smem(u, s + (c0 + 16) + c0 * FLS, 1, FLS, xd + 8 * tn * XLD, 1, XLD, 16);
-    int i = g, j = 8 * tn + 2 * t4;
-    T[i + j * XLD] = u[0];
-    T[i + (j + 1) * XLD] = u[1];
-    T[(i + 8) + j * XLD] = u[2];
-    T[(i + 8) + (j + 1) * XLD] = u[3];
-  }
-  __syncwarp();
-#pragma unroll
-  for (int tn = 0; tn < 2; ++tn) {
-    double u[4] = {0, 0, 0, 0};
-    mma_tile_smem(u, xd + 16 + 16 * XLD, 1, XLD, T + 8 * tn * XLD, 1, XLD, 16);
-    int i = g, j = 8 * tn + 2 * t4;
-    double* X21 = xd + 16;
-    X21[i + j * XLD] = -u[0];
-    X21[i + (j + 1) * XLD] = -u[1];
-    X21[(i + 8) + j * XLD] = -u[2];
-    X21[(i + 8) + (j + 1) * XLD] = -u[3];
-  }
-  __syncwarp();
-  for (int e = lane; e < 256; e += 32) T[(e % 16) + (e / 16) * XLD] = 0.0;
-  __syncwarp();
-  return -1;
-}
-
-// A22 −= P Pᵀ on the 16×8 tiles of rows [rlo, npad) × columns [clo, chi) that
-// are not strictly above the diagonal; tiles dealt to warps w0.. in steps of nws.
-__device__ __forceinline__ void diag_syrk_tiles(double* s, int c0, int rlo, int clo, int chi, int npad, int w0,
-                                                int nws) {
+// Lower 16×8 tiles of A[i][j] −= Σ_{t<16} A[i][k0+t] A[j][k0+t] over rows and
+// columns [r0, npad); `which` = 0: every tile but those of the 16×16 block at
+// (r0, r0), dealt to warps w0.. in steps of nws; 1: only that block's tiles
+// (the calling warp does both).
+__device__ __forceinline__ void syrk16_tiles(double* s, int k0, int r0, int npad, int which, int w0, int nws) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t4 = lane & 3;
-  const int tm_n = (npad - rlo) / 16, tn_n = (chi - clo) / 8;
-  for (int tile = warp - w0; tile < tm_n * tn_n; tile += nws) {
-    int tm = tile % tm_n, tn = tile / tm_n;
-    int rbeg = rlo + 16 * tm, cbeg = clo + 8 * tn;
+  const int tm_n = (npad - r0) / 16, tn_n = (npad - r0) / 8;
+  const int first = which ? 0 : warp - w0, count = which ? 2 : tm_n * tn_n, step = which ? 1 : nws;
+  for (int tile = first; tile < count; tile += step) {
+    const int tm = which ? 0 : tile % tm_n, tn = which ? tile : tile / tm_n;
+    if (!which && tm == 0 && tn < 2) continue;
+    const int rbeg = r0 + 16 * tm, cbeg = r0 + 8 * tn;
     if (rbeg + 15 < cbeg) continue;
     double c[4] = {0, 0, 0, 0};
-    mma_tile_smem(c, s + rbeg + c0 * FLS, 1, FLS, s + cbeg + c0 * FLS, FLS, 1, SB);
-    int row = rbeg + g, col = cbeg + 2 * t4;
+    mma_tile_smem(c, s + rbeg + k0 * FLS, 1, FLS, s + cbeg + k0 * FLS, FLS, 1, LF);
+    const int row = rbeg + g, col = cbeg + 2 * t4;
     if (row >= col) s[row + col * FLS] -= c[0];
     if (row >= col + 1) s[row + (col + 1) * FLS] -= c[1];
     if (row + 8 >= col) s[(row + 8) + col * FLS] -= c[2];
@@ -187,12 +116,12 @@ __device__ __forceinline__ void diag_syrk_tiles(double* s, int c0, int rlo, int 
 static __device__ int diag_block_factor_inv(double* A, long long lda, long long k0, int nb, double* linv, double* smem,
                                      int* fail_sh) {
   int& fail = *fail_sh;
-  double* s = smem;                       // NB_DIAG × FLS
-  double* xd = s + NB_DIAG * FLS;              // 4 × (32 × XLD) sub-block inverses
-  double* tmp = xd + 4 * SB * XLD;        // 3 × (32 × XLD)
+  double* s = smem;                     // NB_DIAG × FLS
+  double* tmp = s + NB_DIAG * FLS;      // TMP_DOUBLES
+  double* rinv = tmp + TMP_DOUBLES;     // NB_DIAG reciprocal pivots
   const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, nw = nt >> 5;
   const int lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-  const int npad = (nb + SB - 1) / SB * SB;
+  const int npad = (nb + LF - 1) / LF * LF;
   if (tid == 0) fail = -1;
   __syncthreads();
   // block load: every lower entry in flight at once (16-byte cp.async pairs
@@ -221,88 +150,126 @@ static __device__ int diag_block_factor_inv(double* A, long long lda, long long 
       else if (i >= nb || j >= nb) s[i + j * FLS] = (i == j) ? 1.0 : 0.0;
     }
   __syncthreads();
-  const int np = npad / SB;
-  // one call site of the warp factor (a second inlined copy ran several times
-  // slower)
+  const int np = npad / LF;
   for (int p = 0; p < np; ++p) {
-    const int c0 = p * SB;
+    const int c0 = p * LF;
     if (warp == 0) {
-      int f = warp_factor_inv32(s, c0, xd + p * SB * XLD);
+      // leaf p (its own update by the previous panel was done by this warp)
+      const int f = leaf16_factor(s, c0, rinv);
       if (f >= 0 && lane == 0) fail = c0 + f;
+    } else if (p > 0) {
+      // the previous panel's update of the rest of the trailing block
+      syrk16_tiles(s, c0 - LF, c0, npad, 0, 1, nw - 1);
     }
     __syncthreads();
     if (fail >= 0) break;
-    const int r0 = c0 + SB, cnt = npad - r0;
-    if (cnt <= 0) break;
-    // P = A_below · X_ppᵀ: tiles (cnt/16) × 4, held in registers until all read
-    const double* X = xd + p * SB * XLD;
-    const int tiles = (cnt / 16) * 4;
-    double pc[3][4];  // ≤ 24 tiles over 8 warps
+    const int r0 = c0 + LF;
+    if (r0 >= npad) break;
+    // panel: rows below the leaf solve X L_ppᵀ = A (32 rows per warp)
+    for (int grp = warp; grp * 32 < npad - r0; grp += nw) {
+      const int row = r0 + grp * 32 + lane;
+      const bool act = row < npad;
+      double a[LF];
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      int tile = warp + q * nw;
+      for (int c = 0; c < LF; ++c) a[c] = act ? s[row + (c0 + c) * FLS] : 0.0;
 #pragma unroll
-      for (int r = 0; r < 4; ++r) pc[q][r] = 0.0;
-      if (tile < tiles) {
-        int tm = tile % (cnt / 16), tn = tile / (cnt / 16);
-        mma_tile_smem(pc[q], s + (r0 + 16 * tm) + c0 * FLS, 1, FLS, X + 8 * tn, XLD, 1, SB);
+      for (int t = 0; t < LF; ++t) {
+        const double x = a[t] * rinv[c0 + t];
+        a[t] = x;
+#pragma unroll
+        for (int j = t + 1; j < LF; ++j) a[j] = fma(-x, s[(c0 + j) + (c0 + t) * FLS], a[j]);
+      }
+      if (act) {
+#pragma unroll
+        for (int c = 0; c < LF; ++c) s[row + (c0 + c) * FLS] = a[c];
       }
     }
     __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      int tile = warp + q * nw;
-      if (tile < tiles) {
-        int tm = tile % (cnt / 16), tn = tile / (cnt / 16);
-        int row = r0 + 16 * tm + g, col = c0 + 8 * tn + 2 * t4;
-        s[row + col * FLS] = pc[q][0];
-        s[row + (col + 1) * FLS] = pc[q][1];
-        s[(row + 8) + col * FLS] = pc[q][2];
-        s[(row + 8) + (col + 1) * FLS] = pc[q][3];
-      }
+    // the next leaf's own update (warp 0, which factors it next)
+    if (warp == 0) {
+      syrk16_tiles(s, c0, r0, npad, 1, 0, 1);
+      __syncwarp();
     }
-    __syncthreads();
-    // trailing update of the rest of the block (all warps)
-    diag_syrk_tiles(s, c0, r0, r0, npad, npad, 0, nw);
-    __syncthreads();
   }
   if (fail >= 0) return fail;
   // L back to global
   for (int j = warp; j < nb; j += nw)
     for (int i = j + lane; i < nb; i += 32) A[(k0 + i) + (k0 + j) * lda] = s[i + j * FLS];
-  // block inverse in place, column blocks right to left
-  for (int jb = np - 1; jb >= 0; --jb) {
-    const int j0 = jb * SB;
-    const int nout = np - 1 - jb;
-    // T_ib = Σ_{k=(jb+1)·32}^{(ib+1)·32−1} X(i, k) L(k, j): tiles (ib, 2 m-tiles, 4 n-tiles)
-    for (int tile = warp; tile < nout * 8; tile += nw) {
-      int ib = jb + 1 + tile / 8, tm = (tile % 8) / 4, tn = tile % 4;
+  __syncthreads();
+  // leaf inverses: lane q computes column q of L_pp⁻¹ by column-oriented
+  // substitution, written over L_pp (its off-diagonal blocks stay L)
+  for (int p = warp; p < np; p += nw) {
+    const int off = p * LF, q = lane & 15;
+    double acc[LF];
+#pragma unroll
+    for (int i = 0; i < LF; ++i) acc[i] = (i == q) ? 1.0 : 0.0;
+#pragma unroll
+    for (int t = 0; t < LF; ++t) {
+      const double x = acc[t] * rinv[off + t];
+      acc[t] = x;
+#pragma unroll
+      for (int j = t + 1; j < LF; ++j) acc[j] = fma(-s[(off + j) + (off + t) * FLS], x, acc[j]);
+    }
+    __syncwarp();
+    if (lane < 16) {
+#pragma unroll
+      for (int i = 0; i < LF; ++i)
+        if (i >= q) s[(off + i) + (off + q) * FLS] = acc[i];
+    }
+  }
+  __syncthreads();
+  // recursive doubling: for sibling blocks (a, b) of h columns,
+  // T = L21 X11 (X11 lower: k from the column), X21 = −X22 T (k up to the row)
+  for (int h = LF; h < npad; h *= 2) {
+    const int TL = h + 4;
+    const int pairs = (npad + 2 * h - 1) / (2 * h);
+    int ntile = 0;
+    for (int k = 0; k < pairs; ++k) {
+      const int b = 2 * k * h + h;
+      if (b < npad) ntile += (min(h, npad - b) / 16) * (h / 8);
+    }
+    for (int tile = warp; tile < ntile; tile += nw) {
+      int rest = tile, k = 0, h2 = 0;
+      for (;; ++k) {
+        const int b = 2 * k * h + h;
+        h2 = min(h, npad - b);
+        const int cnt = (h2 / 16) * (h / 8);
+        if (rest < cnt) break;
+        rest -= cnt;
+      }
+      const int a0 = 2 * k * h, b0 = a0 + h;
+      const int tm = rest % (h2 / 16), tn = rest / (h2 / 16);
+      const int i0 = 16 * tm, j0 = 8 * tn, kb = j0 & ~3;
       double c[4] = {0, 0, 0, 0};
-      int kbeg = (jb + 1) * SB, kcnt = (ib - jb) * SB;
-      mma_tile_smem(c, s + (ib * SB + 16 * tm) + kbeg * FLS, 1, FLS, s + kbeg + (j0 + 8 * tn) * FLS, 1, FLS, kcnt);
-      double* T = tmp + (ib - jb - 1) * SB * XLD;
-      int row = 16 * tm + g, col = 8 * tn + 2 * t4;
-      T[row + col * XLD] = c[0];
-      T[row + (col + 1) * XLD] = c[1];
-      T[(row + 8) + col * XLD] = c[2];
-      T[(row + 8) + (col + 1) * XLD] = c[3];
+      mma_tile_smem(c, s + (b0 + i0) + (a0 + kb) * FLS, 1, FLS, s + (a0 + kb) + (a0 + j0) * FLS, 1, FLS, h - kb);
+      double* T = tmp + k * h * TL;
+      const int row = i0 + g, col = j0 + 2 * t4;
+      T[row + col * TL] = c[0];
+      T[row + (col + 1) * TL] = c[1];
+      T[(row + 8) + col * TL] = c[2];
+      T[(row + 8) + (col + 1) * TL] = c[3];
     }
     __syncthreads();
-    const double* Xjj = xd + jb * SB * XLD;
-    for (int tile = warp; tile < nout * 8; tile += nw) {
-      int ib = jb + 1 + tile / 8, tm = (tile % 8) / 4, tn = tile % 4;
-      const double* T = tmp + (ib - jb - 1) * SB * XLD;
+    for (int tile = warp; tile < ntile; tile += nw) {
+      int rest = tile, k = 0, h2 = 0;
+      for (;; ++k) {
+        const int b = 2 * k * h + h;
+        h2 = min(h, npad - b);
+        const int cnt = (h2 / 16) * (h / 8);
+        if (rest < cnt) break;
+        rest -= cnt;
+      }
+      const int a0 = 2 * k * h, b0 = a0 + h;
+      const int tm = rest % (h2 / 16), tn = rest / (h2 / 16);
+      const int i0 = 16 * tm, j0 = 8 * tn;
+      const double* T = tmp + k * h * TL;
       double c[4] = {0, 0, 0, 0};
-      mma_tile_smem(c, T + 16 * tm, 1, XLD, Xjj + 8 * tn * XLD, 1, XLD, SB);
-      int row = ib * SB + 16 * tm + g, col = j0 + 8 * tn + 2 * t4;
+      mma_tile_smem(c, s + (b0 + i0) + b0 * FLS, 1, FLS, T + j0 * TL, 1, TL, i0 + 16);
+      const int row = b0 + i0 + g, col = a0 + j0 + 2 * t4;
       s[row + col * FLS] = -c[0];
       s[row + (col + 1) * FLS] = -c[1];
       s[(row + 8) + col * FLS] = -c[2];
       s[(row + 8) + (col + 1) * FLS] = -c[3];
-    }
-    for (int e = tid; e < SB * SB; e += nt) {
-      int rr = e % SB, cc = e / SB;
-      s[(j0 + rr) + (j0 + cc) * FLS] = (rr >= cc) ? Xjj[rr + cc * XLD] : 0.0;
     }
     __syncthreads();
   }
@@ -317,6 +284,6 @@ static __device__ int diag_block_factor_inv(double* A, long long lda, long long 
 }
 
 
-inline size_t diag_block_smem() { return (size_t)(NB_DIAG * FLS + 7 * SB * XLD) * sizeof(double); }
+inline size_t diag_block_smem() { return (size_t)(NB_DIAG * FLS + TMP_DOUBLES + NB_DIAG) * sizeof(double); }
 
 }  // namespace gprx
