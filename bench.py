@@ -9,20 +9,24 @@ in log space (100 perturbations, cycled).  All data are synthetic, from the
 restated SeededRng; no dataset is read.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
-                    [--workload all|exact|batched|serving|sgpr|hessian] [--impl ours|reference]
+                    [--workload all|exact|c1|batched|serving|sgpr|hessian] [--impl ours|reference]
 
 The default line's value is the mixed form (FP64 products emulated on the
 int8 tensor cores); the plain FP64 form is timed beside it ("fp64") with the
 largest error of the mixed results against it.  The other workloads ride in
-the same line: "batched" (4096 ragged exact fits), "serving" (a Poisson
-request stream, p50/p99), "sgpr" (VFE at n = 10⁶, m = 1024) and "hessian"
-(the NLML Hessian, gprx_exact_hessian, at the exact workload's θ in both
-forms); each is also available alone through --workload.
+the same line in brief: "c1" (exact RBF n = 512, d = 2: default L-BFGS fit
+and a 256-point predict), "batched" (4096 ragged exact fits), "serving" (a
+Poisson request stream, p50/p99), "sgpr" (VFE at n = 10⁶, m = 1024) and
+"hessian" (the NLML Hessian at the exact workload's θ in both forms); each is
+also available alone, in full, through --workload.  Floats in the default
+line carry 4 significant digits so that the line stays within a few KB.
 
 N > 1 runs N independent replicas (one exact problem does not shard; launched
 by torchrun, one rank per GPU); `value` is the aggregate evals/s over ranks,
 timed as the maximum over ranks.  `--impl reference` times the CPU
-restatement of the reference's algorithm (oracle/) on the host cores.
+restatement of the reference's algorithm (oracle/) on the host cores, one
+full n = 8192 evaluation per step; it draws its data from the Python
+SynthRng below and never loads the CUDA library.
 """
 
 import argparse
@@ -45,11 +49,63 @@ NOISE = 0.05 ** 2
 CONST = 2.0
 
 
+_M64 = (1 << 64) - 1
+
+
+class SynthRng:
+    """Xoshiro256++ seeded by SplitMix64 with the reference's unit and
+    Box–Muller normal draws (gprx src/rng.rs:10-87), in Python: the exact
+    workloads' data come from here in both arms of this benchmark, so the
+    reference arm never loads the CUDA library.  Scalar libm log/cos keep the
+    draws bit-identical to the library's gprx_rng_* (tests/test_bench_cpu.py)."""
+
+    def __init__(self, seed):
+        x = int(seed) & _M64
+        s = []
+        for _ in range(4):
+            x = (x + 0x9E3779B97F4A7C15) & _M64
+            z = x
+            z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+            z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+            s.append(z ^ (z >> 31))
+        self.s = s
+
+    def next_u64(self):
+        s = self.s
+        r = (s[0] + s[3]) & _M64
+        r = (((r << 23) | (r >> 41)) & _M64) + s[0] & _M64
+        t = (s[1] << 17) & _M64
+        s[2] ^= s[0]
+        s[3] ^= s[1]
+        s[1] ^= s[2]
+        s[0] ^= s[3]
+        s[2] ^= t
+        s[3] = ((s[3] << 45) | (s[3] >> 19)) & _M64
+        return r
+
+    def _unit1(self):
+        return (self.next_u64() >> 11) * (1.0 / 9007199254740992.0)
+
+    def _open_unit(self):
+        u = self._unit1()
+        eps = 1.0 / 9007199254740992.0
+        return eps if u <= eps else (1.0 - eps if u >= 1.0 - eps else u)
+
+    def _normal1(self):
+        u1 = max(self._open_unit(), 2.2250738585072014e-308)
+        u2 = self._open_unit()
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+    def unit(self, count):
+        return np.array([self._unit1() for _ in range(int(count))])
+
+    def normal(self, count):
+        return np.array([self._normal1() for _ in range(int(count))])
+
+
 def synth(n, d, seed=0):
     """x, y, true θ for the C2 workload (seeded Xoshiro256++)."""
-    import gprx_b200 as gx
-
-    rng = gx.SeededRng(seed)
+    rng = SynthRng(seed)
     x = rng.normal(n * d)                      # column-major n×d, N(0, 1)
     u = rng.unit(d)
     ls = np.exp(math.log(0.3) + u * (math.log(3.0) - math.log(0.3)))
@@ -65,9 +121,7 @@ def synth(n, d, seed=0):
 
 
 def perturbations(theta, count=100, seed=1):
-    import gprx_b200 as gx
-
-    rng = gx.SeededRng(seed)
+    rng = SynthRng(seed)
     return [theta + 0.1 * rng.normal(theta.size) for _ in range(count)]
 
 
@@ -222,35 +276,89 @@ def emu_kernel_roofline(n, peaks, traffic, int8_peak=None):
             "max_rel_err_vs_dmma": out[3]}
 
 
-def cpu_reference(n, d, x, y, thetas, steps, warmup, budget_s=6.0):
-    """Times the oracle (a CPU restatement of the reference's algorithm)."""
+def cpu_reference(n, d, x, y, thetas, steps, warmup):
+    """Times the oracle (a CPU restatement of the reference's algorithm) on
+    the full workload: each step is one NLML + gradient evaluation at n."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as O
 
     lib = O.lib()
     cores = int(lib.orc_num_threads())
     nodes = [[2, 2], [12, 0], [11, d]]
-    # a step is one full evaluation at n when it fits the budget, else one
-    # evaluation at n/2 scaled by 8 (the evaluation is O(n³)).
-    t0 = time.perf_counter()
-    O.exact_eval(nodes, thetas[0], x, n, d, y)
-    t_full = time.perf_counter() - t0
-    if t_full <= budget_s:
-        ns, scale, xs, ys = n, 1.0, x, y
-    else:
-        ns = n // 2
-        xs = x.reshape(d, n)[:, :ns].reshape(-1).copy()
-        ys = y[:ns].copy()
-        scale = (n / ns) ** 3
     for i in range(warmup):
-        O.exact_eval(nodes, thetas[i % len(thetas)], xs, ns, d, ys)
+        O.exact_eval(nodes, thetas[i % len(thetas)], x, n, d, y)
     t0 = time.perf_counter()
     for i in range(steps):
-        O.exact_eval(nodes, thetas[i % len(thetas)], xs, ns, d, ys)
-    dt = (time.perf_counter() - t0) / steps * scale
-    sample = ("one NLML+gradient evaluation per step at n=%d" % ns) + (
-        "" if scale == 1.0 else ", time scaled by (%d/%d)^3 to n=%d" % (n, ns, n))
+        O.exact_eval(nodes, thetas[i % len(thetas)], x, n, d, y)
+    dt = (time.perf_counter() - t0) / steps
+    sample = "%d NLML+gradient evaluation(s) at n=%d, the full workload" % (steps, n)
     return 1.0 / dt, dt, cores, sample
+
+
+# ---------------------------------------------------------------------------
+# C1: exact RBF, n = 512, d = 2, default L-BFGS fit, then predict 256 points
+# ---------------------------------------------------------------------------
+C1_N, C1_D, C1_Q = 512, 2, 256
+
+
+def c1_synth(seed=10):
+    """x ~ U[0,10]² (column-major), y = sin(x0) + 0.5 cos(x1) + N(0, 0.1²),
+    256 query points ~ U[0,10]²."""
+    rng = SynthRng(seed)
+    x = 10.0 * rng.unit(C1_N * C1_D)
+    y = np.sin(x[:C1_N]) + 0.5 * np.cos(x[C1_N:]) + 0.1 * rng.normal(C1_N)
+    xs = 10.0 * rng.unit(C1_Q * C1_D)
+    return x, y, xs
+
+
+def c1_measure(torch, local, steps=10, warm=3):
+    """Fit + predict through the public API with host buffers (a step = one
+    Gpr(RbfKernel(1.0), GaussianLikelihood(0.1)).fit by the default L-BFGS
+    and one predict of mean and variance at 256 points), and the oracle beside
+    it: its evaluation at n = 512 times the fit's evaluations, plus its
+    prediction."""
+    import gprx_b200 as gx
+
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+
+    x, y, xs = c1_synth()
+
+    def step():
+        m = gx.Gpr(gx.RbfKernel(1.0), gx.GaussianLikelihood(0.1), device=local).fit(x, C1_N, C1_D, y)
+        p = m.predict(xs, C1_Q, C1_D)
+        return m, p
+
+    for _ in range(warm):
+        step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        m, p = step()
+    dt = (time.perf_counter() - t0) / steps
+    theta = np.array(m.get_params())
+    evals = int(m.report.evaluations)
+    # the predict alone, on the fitted model
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        m.predict(xs, C1_Q, C1_D)
+    pred_ms = (time.perf_counter() - t0) / steps * 1e3
+    nodes = [[10, 0]]
+    t0 = time.perf_counter()
+    reps = 20
+    for _ in range(reps):
+        O.exact_eval(nodes, theta, x, C1_N, C1_D, y)
+    orc_eval = (time.perf_counter() - t0) / reps
+    t0 = time.perf_counter()
+    mo, vo = O.exact_predict(nodes, theta, x, C1_N, C1_D, y, xs, C1_Q, 1)
+    orc_pred = time.perf_counter() - t0
+    err = max(float(np.max(O.rel_err(p.mean, mo))), float(np.max(O.rel_err(p.variance, vo))))
+    return {"value": 1.0 / dt, "unit": "fits/s", "ms_per_fit_predict": dt * 1e3, "predict_ms": pred_ms,
+            "evaluations": evals, "iterations": int(m.report.iterations), "converged": bool(m.report.converged),
+            "nlml": m.neg_log_marginal_likelihood(), "predict_err_vs_oracle": err,
+            "cpu_baseline": {"value": 1.0 / (evals * orc_eval + orc_pred), "unit": "fits/s",
+                             "cores": int(O.lib().orc_num_threads()), "kind": "port",
+                             "sample": "oracle eval x the fit's evaluations + oracle predict"}}
 
 
 # ---------------------------------------------------------------------------
@@ -595,6 +703,23 @@ def hessian_measure(torch, dev, local, spec, x, y, theta, n, d, steps, warm, for
                     "one launch)"}
 
 
+def brief(d, keys):
+    """The listed keys of a result dict (the default line stays within the
+    few KB a log tail keeps)."""
+    return {k: d[k] for k in keys if k in d}
+
+
+def rounded(obj, digits=4):
+    """Floats to `digits` significant digits, recursively."""
+    if isinstance(obj, float):
+        return float("%.*g" % (digits, obj)) if math.isfinite(obj) else obj
+    if isinstance(obj, dict):
+        return {k: rounded(v, digits) for k, v in obj.items()}
+    if isinstance(obj, (list, tuple)):
+        return [rounded(v, digits) for v in obj]
+    return obj
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -607,7 +732,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-evals", type=int, default=0,
                     help="only factor once and run this many evaluations (for an ncu launch list), no JSON line")
-    ap.add_argument("--workload", default="all", choices=["all", "exact", "batched", "serving", "sgpr", "hessian"],
+    ap.add_argument("--workload", default="all", choices=["all", "exact", "c1", "batched", "serving", "sgpr", "hessian"],
                     help="all: the exact line with the batched measurement as its 'batched' key")
     ap.add_argument("--batch-problems", type=int, default=BATCH_P)
     ap.add_argument("--serve-rates", default="2,4,8", help="arrival rates (requests/s) of the serving sweep")
@@ -621,9 +746,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     workload = "exact_gpr_nlml_grad_n%d_d%d_const_rbfard" % (n, d)
-    config = {"workload": workload, "n": n, "d": d, "kernel": "ConstantKernel(2.0) * RbfArdKernel(d=8)",
-              "noise_variance": NOISE, "perturbations": "100 θ + N(0, 0.1²) in log space, cycled",
-              "l2": "inputs larger than L2 (two n×n FP64 buffers of %d MiB each)" % (n * n * 8 // 2 ** 20),
+    config = {"workload": workload, "n": n, "d": d,
+              "l2": "inputs > L2 (two n x n FP64 buffers of %d MiB)" % (n * n * 8 // 2 ** 20),
               "parallelism": "replicas" if args.gpus > 1 else "single"}
     metric = "NLML+grad evals/s n=%d (%s)" % (n, {"both": "mixed; FP64 beside", "mixed": "mixed",
                                                    "fp64": "FP64"}[args.precision])
@@ -670,6 +794,15 @@ def main():
         out = sgpr_measure(torch, dev, args.steps, warm, fp64_peak=fp64_peak_tflops(torch, dev))
         out.update({"n_gpus": 1, "warmup": warm, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                     "dtype": "f64", "data": "synthetic"})
+        print(json.dumps(out), flush=True)
+        return
+
+    if args.workload == "c1":
+        out = c1_measure(torch, local, steps=args.steps, warm=warm)
+        out.update({"metric": "exact RBF n=512 d=2: L-BFGS fit + predict 256 per second", "n_gpus": 1,
+                    "steps": args.steps, "warmup": warm, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                    "config": {"workload": "exact_gpr_fit_predict_n512_d2_rbf"}})
         print(json.dumps(out), flush=True)
         return
 
@@ -809,48 +942,64 @@ def main():
                               "n^3/3) over the factor + inverse stage time",
                       "stage_ms": {"fill": stage[0], "factor": stage[1], "inverse": stage[2], "gradient": stage[3],
                                    "total": stage[4]}}
-    roofline = dict(stage_roofline)
+    roofline = {k: stage_roofline[k] for k in ("bound", "achieved", "peak", "unit", "frac")}
+    roofline["kernel"] = "factor + inverse stages (n^3 flop)"
+    roofline["traffic"] = traffic.get("dgemm_bytes_per_eval") if traffic else None
     if mixed and rank == 0:
         k = emu_kernel_roofline(n, peaks, traffic, int8_peak_tops(torch, dev))
         if k is not None:
-            roofline = k
-            roofline["stage"] = stage_roofline
-    else:
-        roofline["traffic"] = traffic.get("dgemm_bytes_per_eval") if traffic else None
-    if mixed:
-        config["precision"] = ("mixed: factor and inverse by recursive halving, coupling products and K^-1 = X^T X "
-                               "as FP64 products emulated on int8 tensor cores (7 slices); FP64 fill, 4096-row "
-                               "leaves, log-det and gradient")
+            roofline = {"bound": "tensor", "kernel": "emu_gemm_kernel<7> at (n/2)^3", "achieved": k["achieved"],
+                        "peak": k["peak"], "unit": "TOP/s int8", "frac": k["frac"], "traffic": k["traffic"],
+                        "peak_src": "cuBLASLt int8 (of measured)" if "cuBLASLt" in k["peak_source"]
+                        else k["peak_source"][:40], "fp64_eq_tflops": k["fp64_equivalent_tflops"]}
+    roofline["stage_frac_of_dgemm"] = stage_roofline["frac"]
+    clk = head["clocks"]
     line = {"metric": metric, "value": head["value"], "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": warm, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if not mixed else "f64 (int8-emulated products)",
             "data": "synthetic", "config": config, "e2e": head["e2e"], "gpu_launches": head["launches"],
-            "roofline": roofline, "clocks": head["clocks"], "bf16_peak_reference": peaks.get("bf16_tflops")}
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
+            "roofline": roofline,
+            "stage_ms": {k: stage[i] for i, k in enumerate(("fill", "factor", "inverse", "gradient", "total"))}}
     if mixed and "fp64" in res:
         f, m = res["fp64"], res["mixed"]
         nl_err = max(abs(a[0] - b[0]) / max(abs(b[0]), 1.0) for a, b in zip(m["outs"], f["outs"]))
         g_err = max(float(np.max(np.abs(a[1] - b[1]) / np.maximum(np.abs(b[1]), 1.0)))
                     for a, b in zip(m["outs"], f["outs"]))
-        line["fp64"] = {"value": f["value"], "unit": "evals/s", "ms_per_step": f["ms_per_step"], "e2e": f["e2e"],
-                        "stage_ms": {"fill": f["stage"][0], "factor": f["stage"][1], "inverse": f["stage"][2],
-                                     "gradient": f["stage"][3], "total": f["stage"][4]},
-                        "roofline_frac": (n ** 3) / ((f["stage"][1] + f["stage"][2]) * 1e-3) / 1e12 / fp64_peak
+        line["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "e2e": f["e2e"]["value"],
+                        "frac_of_dgemm": (n ** 3) / ((f["stage"][1] + f["stage"][2]) * 1e-3) / 1e12 / fp64_peak
                         if fp64_peak else None}
         line["mixed_vs_fp64"] = m["value"] / f["value"]
-        line["mixed_error_vs_fp64"] = {"nlml_rel_max": nl_err, "grad_rel_max": g_err,
-                                       "measure": "max over the timed evaluations of |a − e| / max(|e|, 1)"}
+        line["mixed_error_vs_fp64"] = {"nlml": nl_err, "grad": g_err}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, dt, cores, sample = cpu_reference(n, d, x, y, thetas, steps=1, warmup=0, budget_s=30.0)
+        v, dt, cores, sample = cpu_reference(n, d, x, y, thetas, steps=1, warmup=0)
         line["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": cores, "kind": "port", "sample": sample}
     if args.workload == "all" and world == 1:
         torch.cuda.empty_cache()
-        line["batched"] = batched_measure(torch, dev, args.batch_problems, fp64_peak=fp64_peak)
+        c1 = c1_measure(torch, local)
+        line["c1"] = brief(c1, ("value", "unit", "ms_per_fit_predict", "predict_ms", "evaluations", "converged",
+                                "predict_err_vs_oracle"))
+        line["c1"]["cpu"] = c1["cpu_baseline"]["value"]
+        bt = batched_measure(torch, dev, args.batch_problems, fp64_peak=fp64_peak)
+        line["batched"] = brief(bt, ("value", "unit", "speedup_vs_one_model_per_launch", "status_ok", "converged"))
+        line["batched"].update({"e2e": bt["e2e"]["value"], "one_model_per_launch": bt["one_model_per_launch"]["value"],
+                                "round_ms": bt["roofline"]["round_ms"], "frac_of_dgemm": bt["roofline"]["frac"],
+                                "cpu": bt["cpu_baseline"]["value"]})
         datasets = serving_synth(torch, dev)
-        line["serving"] = [serving_measure(torch, dev, 4.0, 12.0, prec, datasets) for prec in ("fp64", "mixed")]
+        line["serving"] = [brief(r, ("precision", "arrival_rate_per_s", "requests", "requests_per_s", "p50_ms",
+                                     "p99_ms", "merged_predict_launches"))
+                           for r in (serving_measure(torch, dev, 4.0, 12.0, prec, datasets) for prec in ("fp64", "mixed"))]
         torch.cuda.empty_cache()
-        line["sgpr"] = sgpr_measure(torch, dev, 3, 2, fp64_peak=fp64_peak)
+        sg = sgpr_measure(torch, dev, 3, 2, fp64_peak=fp64_peak)
+        line["sgpr"] = brief(sg, ("value", "unit", "mixed_vs_fp64"))
+        line["sgpr"].update({"fp64": sg["fp64"]["value"], "err": [sg["mixed_error_vs_fp64"]["nlml_rel_max"],
+                                                                  sg["mixed_error_vs_fp64"]["grad_rel_max"]],
+                             "frac_of_dgemm": sg["roofline"]["frac"], "cpu": sg["cpu_baseline"]["value"]})
         torch.cuda.empty_cache()
-        line["hessian"] = hessian_measure(torch, dev, local, spec, x, y, theta, n, d, 3, 3)
+        hs = hessian_measure(torch, dev, local, spec, x, y, theta, n, d, 3, 3)
+        line["hessian"] = {"fp64_ms": hs["forms"]["fp64"]["ms_per_hessian"],
+                           "mixed_ms": hs["forms"]["mixed"]["ms_per_hessian"]}
+    line = rounded(line)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
