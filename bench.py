@@ -355,6 +355,7 @@ def c1_measure(torch, local, steps=10, warm=3):
     err = max(float(np.max(O.rel_err(p.mean, mo))), float(np.max(O.rel_err(p.variance, vo))))
     return {"value": 1.0 / dt, "unit": "fits/s", "ms_per_fit_predict": dt * 1e3, "predict_ms": pred_ms,
             "evaluations": evals, "iterations": int(m.report.iterations), "converged": bool(m.report.converged),
+            "grad_norm": float(m.report.grad_norm),
             "nlml": m.neg_log_marginal_likelihood(), "predict_err_vs_oracle": err,
             "cpu_baseline": {"value": 1.0 / (evals * orc_eval + orc_pred), "unit": "fits/s",
                              "cores": int(O.lib().orc_num_threads()), "kind": "port",
@@ -662,7 +663,8 @@ def serving_measure(torch, dev, rate, duration, precision, datasets, seed=5, wor
             "requests": len(res), "completed_ok": int(ok.sum()), "requests_per_s": float(ok.sum() / wall),
             "p50_ms": float(np.percentile(lat[ok], 50)) if ok.any() else None,
             "p99_ms": float(np.percentile(lat[ok], 99)) if ok.any() else None,
-            "per_kind": per, "merged_predict_launches": stats["merged_launches"], "workers": workers}
+            "per_kind": per, "merged_predict_launches": stats["merged_launches"],
+            "merged_fit_launches": stats["merged_fit_launches"], "workers": workers}
 
 
 def hessian_measure(torch, dev, local, spec, x, y, theta, n, d, steps, warm, forms=("fp64", "mixed")):
@@ -735,8 +737,8 @@ def main():
     ap.add_argument("--workload", default="all", choices=["all", "exact", "c1", "batched", "serving", "sgpr", "hessian"],
                     help="all: the exact line with the batched measurement as its 'batched' key")
     ap.add_argument("--batch-problems", type=int, default=BATCH_P)
-    ap.add_argument("--serve-rates", default="2,4,8", help="arrival rates (requests/s) of the serving sweep")
-    ap.add_argument("--serve-seconds", type=float, default=15.0)
+    ap.add_argument("--serve-rates", default="8,16,32,64", help="arrival rates (requests/s) of the serving sweep")
+    ap.add_argument("--serve-requests", type=int, default=300, help="requests per rate of the serving sweep")
     args = ap.parse_args()
     n, d = args.n, D
     warm = max(3, args.warmup)
@@ -811,7 +813,7 @@ def main():
         sweep = []
         for prec in ("fp64", "mixed"):
             for rate in [float(r) for r in args.serve_rates.split(",")]:
-                sweep.append(serving_measure(torch, dev, rate, args.serve_seconds, prec, datasets))
+                sweep.append(serving_measure(torch, dev, rate, args.serve_requests / rate, prec, datasets))
         head = max((r for r in sweep if r["precision"] == "mixed"), key=lambda r: r["requests_per_s"])
         out = {"metric": "serving p99 latency (ms) at the highest sustained rate", "value": head["p99_ms"],
                "unit": "ms", "higher_is_better": False, "n_gpus": 1, "steps": len(sweep), "warmup": 3,
@@ -978,7 +980,7 @@ def main():
         torch.cuda.empty_cache()
         c1 = c1_measure(torch, local)
         line["c1"] = brief(c1, ("value", "unit", "ms_per_fit_predict", "predict_ms", "evaluations", "converged",
-                                "predict_err_vs_oracle"))
+                                "grad_norm", "predict_err_vs_oracle"))
         line["c1"]["cpu"] = c1["cpu_baseline"]["value"]
         bt = batched_measure(torch, dev, args.batch_problems, fp64_peak=fp64_peak)
         line["batched"] = brief(bt, ("value", "unit", "speedup_vs_one_model_per_launch", "status_ok", "converged"))
@@ -986,9 +988,15 @@ def main():
                                 "round_ms": bt["roofline"]["round_ms"], "frac_of_dgemm": bt["roofline"]["frac"],
                                 "cpu": bt["cpu_baseline"]["value"]})
         datasets = serving_synth(torch, dev)
-        line["serving"] = [brief(r, ("precision", "arrival_rate_per_s", "requests", "requests_per_s", "p50_ms",
-                                     "p99_ms", "merged_predict_launches"))
-                           for r in (serving_measure(torch, dev, 4.0, 12.0, prec, datasets) for prec in ("fp64", "mixed"))]
+        # a sweep of Poisson arrival rates, 300 requests each (mixed; FP64 at
+        # two of the rates): precision, rate, requests, req/s, p50 / p99 ms,
+        # merged predict launches, merged fit launches
+        sweep = [("mixed", r) for r in (8.0, 16.0, 32.0, 64.0)] + [("fp64", r) for r in (16.0, 64.0)]
+        line["serving"] = []
+        for prec, rate in sweep:
+            r = serving_measure(torch, dev, rate, 300.0 / rate, prec, datasets)
+            line["serving"].append([prec, rate, r["requests"], r["requests_per_s"], r["p50_ms"], r["p99_ms"],
+                                    r["merged_predict_launches"], r["merged_fit_launches"]])
         torch.cuda.empty_cache()
         sg = sgpr_measure(torch, dev, 3, 2, fp64_peak=fp64_peak)
         line["sgpr"] = brief(sg, ("value", "unit", "mixed_vs_fp64"))

@@ -95,7 +95,7 @@ class RequestInfo(C.Structure):
 
 class ServerStats(C.Structure):
     _fields_ = [("completed", C.c_uint64), ("merged_launches", C.c_uint64), ("used_bytes", C.c_uint64),
-                ("resident_models", C.c_uint64)]
+                ("resident_models", C.c_uint64), ("merged_fit_launches", C.c_uint64)]
 
 
 class Rng(C.Structure):
@@ -127,6 +127,8 @@ _SIGS = {
     "gprx_exact_nlml": (C.c_int32, [C.c_void_p, D]),
     "gprx_exact_factor_jitter": (C.c_int32, [C.c_void_p, D]),
     "gprx_exact_predict": (C.c_int32, [C.c_void_p, D, C.c_uint64, C.c_int32, D, D]),
+    "gprx_exact_predict_group": (C.c_int32, [C.POINTER(C.c_void_p), C.c_uint64, C.POINTER(D), U64, C.c_int32,
+                                             C.POINTER(D), C.POINTER(D)]),
     "gprx_exact_alpha": (C.c_int32, [C.c_void_p, D, C.c_uint64]),
     "gprx_exact_fit": (C.c_int32, [C.c_void_p, C.POINTER(LbfgsOptions), C.POINTER(FitReport)]),
     "gprx_exact_fit_trust_region": (C.c_int32, [C.c_void_p, C.POINTER(TrustRegionOptions), C.POINTER(FitReport)]),

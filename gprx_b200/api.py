@@ -1354,6 +1354,31 @@ class GprBatch:
                         np.array([r.converged for r in reps], dtype=bool), st)
 
 
+def predict_group(models, xs_list, qs, kind=None):
+    """Mean and variance for several requests against several fitted exact
+    models in one launch (gprx_exact_predict_group): request i asks
+    models[i] at qs[i] points xs_list[i] (column-major qs[i] × d).  Returns a
+    list of Prediction.  Every model has at most 1024 points and 16
+    features, is not online, and all share d and the device."""
+    k = len(models)
+    if k == 0 or len(xs_list) != k or len(qs) != k:
+        raise ShapeMismatch("one query array and one size per model")
+    kind = VarianceKind.Observation if kind is None else kind
+    hs = (C.c_void_p * k)(*[m._h.value for m in models])
+    xs_a = [L.f64(x) for x in xs_list]
+    for m, x, q in zip(models, xs_a, qs):
+        if x.size != int(q) * m.d:
+            raise ShapeMismatch("xs has %d values, expected %d×%d" % (x.size, q, m.d))
+    means = [np.zeros(int(q)) for q in qs]
+    vars_ = [np.zeros(int(q)) for q in qs]
+    xp = (L.D * k)(*[L.ptr(x) for x in xs_a])
+    mp = (L.D * k)(*[L.ptr(v) for v in means])
+    vp = (L.D * k)(*[L.ptr(v) for v in vars_])
+    qa = np.ascontiguousarray(np.asarray(qs, dtype=np.uint64))
+    check(L.lib().gprx_exact_predict_group(hs, k, xp, qa.ctypes.data_as(L.U64), int(kind), mp, vp))
+    return [Prediction(mu, v, kind) for mu, v in zip(means, vars_)]
+
+
 def partition_by_cost(sizes, parts):
     """Splits problem indices 0..len(sizes)-1 into `parts` shards balanced by
     Σ n_i³ (an evaluation's work per problem is O(n_i³)): longest processing
@@ -1512,7 +1537,7 @@ class Server:
         s = L.ServerStats()
         check(L.lib().gprx_server_stats(self._h, C.byref(s)))
         return {"completed": s.completed, "merged_launches": s.merged_launches, "used_bytes": s.used_bytes,
-                "resident_models": s.resident_models}
+                "resident_models": s.resident_models, "merged_fit_launches": s.merged_fit_launches}
 
 
 # ---------------------------------------------------------------------------

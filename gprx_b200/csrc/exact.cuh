@@ -57,6 +57,8 @@ struct ExactState {
   HostPinned<double> res_h;
   HostPinned<DevStatus> status_h;
   DevBuf<double> qbuf, qx;  // predict scratch
+  DevBuf<unsigned char> group_dev;       // grouped-predict staging (this handle leads the group)
+  HostPinned<unsigned char> group_host;
   // mixed precision: the inverse's products emulated on the int8 tensor cores
   DevBuf<int8_t> emu_sa, emu_sb;
   DevBuf<int> emu_ea, emu_eb, emu_err;

@@ -6,11 +6,22 @@
 // free, its model is not busy and — for a fit — the model's device memory fits
 // in the HBM budget (idle models are evicted least-recently-used to make
 // room).  Every model owns a CUDA stream (its gprx_exact handle), so the work
-// of different models overlaps on the device.  Consecutive predict requests
-// queued for one model with the same variance kind are merged into one
-// predict launch (same-phase batching) and their outputs split back.
+// of different models overlaps on the device.  Same-phase work is batched:
+//  - fits of up to SERVE_BATCH_FIT_MAX_N points always run on the batched
+//    evaluator (gprx_batch_fit: one persistent launch per L-BFGS round, one
+//    CTA per problem); the fits waiting at the heads of different models'
+//    queues that share a kernel tree, d and optimizer settings are admitted
+//    together into one such launch, and a fit that arrives alone runs the
+//    same kernels as a batch of one;
+//  - small predicts (at most SERVE_GROUP_MAX_Q points against a fitted model
+//    of at most SERVE_GROUP_MAX_N points) always run as a grouped launch
+//    (gprx_exact_predict_group, one CTA per request tile): those waiting at
+//    the heads of several models' queues, and a model's consecutive ones,
+//    share one launch; larger consecutive predicts of one model with the
+//    same variance kind are merged into one predict launch and split back.
 // Requests on one model run in submission order; each model's results do
-// not depend on what else is running.
+// not depend on what else is running (a batched problem is evaluated by one
+// CTA in a fixed order whatever the batch holds).
 //
 // The per-request device work is the exact path of this library (the
 // reference's Gpr::fit / FittedGpr::predict_with / OnlineGpr insert and
@@ -75,6 +86,8 @@ struct Request {
 struct Model {
   gprx_exact* h = nullptr;
   uint64_t d = 0;
+  uint64_t n = 0;      // training points of the fitted model
+  uint64_t fit_req = 0;  // the fit request (its kernel tree)
   uint64_t bytes = 0;
   bool busy = false;
   bool ready = false;  // fitted and resident
@@ -83,6 +96,37 @@ struct Model {
   int64_t last_used = 0;
   std::deque<uint64_t> queue;  // request ids, submission order
 };
+
+// fits of at most this many points run on the batched evaluator (one CTA per
+// problem: beyond it the blocked factor on the whole GPU has lower latency)
+constexpr uint64_t SERVE_BATCH_FIT_MAX_N = 512;
+// problems per batched fit launch (one CTA each on the 148 SMs)
+constexpr size_t SERVE_BATCH_FIT_MAX = 148;
+
+bool batched_fit(const Request* r) { return r->kind == FIT && r->optimize && r->n <= SERVE_BATCH_FIT_MAX_N; }
+
+// Fits that may share one batched launch: the same tree, d, θ length,
+// jitter policy and optimizer settings (each problem keeps its own data and θ0).
+bool fit_compatible(const Request* a, const Request* b) {
+  if (a->d != b->d || a->nodes.size() != b->nodes.size() || a->theta.size() != b->theta.size()) return false;
+  for (size_t i = 0; i < a->nodes.size(); ++i)
+    if (a->nodes[i].kind != b->nodes[i].kind || a->nodes[i].arg != b->nodes[i].arg) return false;
+  const gprx_options &oa = a->opt, &ob = b->opt;
+  if (oa.jitter_kind != ob.jitter_kind || oa.jitter_initial != ob.jitter_initial ||
+      oa.jitter_multiplier != ob.jitter_multiplier || oa.jitter_max_retries != ob.jitter_max_retries ||
+      oa.jitter_max != ob.jitter_max)
+    return false;
+  return std::memcmp(&a->lopt, &b->lopt, sizeof(gprx_lbfgs_options)) == 0;
+}
+
+// predicts of at most this many points against a fitted (not online) model
+// of at most SERVE_GROUP_MAX_N points and SERVE_GROUP_MAX_D features run as
+// one grouped launch (gprx_exact_predict_group) with the other models' small
+// predicts waiting at the same time, alone or not
+constexpr uint64_t SERVE_GROUP_MAX_Q = 256;
+constexpr uint64_t SERVE_GROUP_MAX_N = 1024;
+constexpr uint64_t SERVE_GROUP_MAX_D = 16;
+constexpr size_t SERVE_GROUP_MAX = 64;
 
 uint64_t model_bytes(uint64_t n, uint64_t d) {
   const uint64_t ld = (n + 31) / 32 * 32, cap = std::max<uint64_t>(n, 1);
@@ -104,50 +148,84 @@ struct gprx_server {
   std::vector<std::thread> workers;
   // latency records of finished requests (ns): per kind
   std::vector<int64_t> lat[4];
-  uint64_t completed = 0, merged_launches = 0;
+  uint64_t completed = 0, merged_launches = 0, merged_fit_launches = 0;
 
   void run_worker();
   // picks a runnable request under the lock; returns its id (0: none)
   uint64_t pick(std::vector<uint64_t>& batch);
+  bool admit_fit(uint64_t model, Request* r);
+  bool small_predict(const Request* r);
+  bool same_tree(uint64_t a, uint64_t b);
+  void execute_predict_group(std::vector<uint64_t>& batch);
   void execute(std::vector<uint64_t>& batch);
+  void execute_fit_batch(std::vector<uint64_t>& batch);
   void finish(Request* r, gprx_status st, const char* why);
 };
 
+bool gprx_server::small_predict(const Request* r) {
+  if (r->kind != PREDICT) return false;
+  const Model& m = models[r->model];
+  return m.ready && !m.online && !m.failed && m.n <= SERVE_GROUP_MAX_N && m.d <= SERVE_GROUP_MAX_D &&
+         r->q <= SERVE_GROUP_MAX_Q;
+}
+
+// Models fitted with the same kernel tree (so one grouped launch serves both).
+bool gprx_server::same_tree(uint64_t a, uint64_t b) {
+  auto ra = reqs.find(models[a].fit_req), rb = reqs.find(models[b].fit_req);
+  if (ra == reqs.end() || rb == reqs.end()) return false;
+  const auto &na = ra->second->nodes, &nb = rb->second->nodes;
+  if (na.size() != nb.size() || models[a].d != models[b].d) return false;
+  for (size_t i = 0; i < na.size(); ++i)
+    if (na[i].kind != nb[i].kind || na[i].arg != nb[i].arg) return false;
+  return true;
+}
+
+// Makes room for a fit of r's size in the HBM budget (evicting idle resident
+// models, least recently used first) and accounts it; false if it does not fit.
+bool gprx_server::admit_fit(uint64_t model, Request* r) {
+  const uint64_t need = model_bytes(r->n, r->d);
+  if (used_bytes + need > opt.hbm_budget_bytes) {
+    std::vector<std::pair<int64_t, uint64_t>> idle;
+    for (auto& o : models)
+      if (o.first != model && o.second.ready && !o.second.busy && o.second.queue.empty())
+        idle.push_back({o.second.last_used, o.first});
+    std::sort(idle.begin(), idle.end());
+    uint64_t freeable = 0;
+    for (auto& e : idle) freeable += models[e.second].bytes;
+    if (used_bytes - std::min(used_bytes, freeable) + need > opt.hbm_budget_bytes) return false;
+    for (auto& e : idle) {
+      if (used_bytes + need <= opt.hbm_budget_bytes) break;
+      Model& o = models[e.second];
+      gprx_exact_destroy(o.h);
+      o.h = nullptr;
+      o.ready = false;
+      o.failed = true;  // later requests on an evicted model fail
+      used_bytes -= o.bytes;
+      o.bytes = 0;
+    }
+  }
+  Model& m = models[model];
+  m.bytes = need;
+  used_bytes += need;
+  return true;
+}
+
 uint64_t gprx_server::pick(std::vector<uint64_t>& batch) {
   batch.clear();
-  // oldest runnable head across models
+  // oldest runnable head across models (a fit must fit in the HBM budget,
+  // possibly after evicting idle models)
   uint64_t best = 0;
   int64_t best_t = INT64_MAX;
   for (auto& kv : models) {
     Model& m = kv.second;
     if (m.busy || m.queue.empty()) continue;
     Request* r = reqs[m.queue.front()].get();
-    if (r->kind == FIT) {
-      if (r->t_submit >= best_t) continue;
-      const uint64_t need = model_bytes(r->n, r->d);
-      if (used_bytes + need > opt.hbm_budget_bytes) {
-        // evict idle resident models, least recently used first
-        std::vector<std::pair<int64_t, uint64_t>> idle;
-        for (auto& o : models)
-          if (o.first != kv.first && o.second.ready && !o.second.busy && o.second.queue.empty())
-            idle.push_back({o.second.last_used, o.first});
-        std::sort(idle.begin(), idle.end());
-        uint64_t freeable = 0;
-        for (auto& e : idle) freeable += models[e.second].bytes;
-        if (used_bytes - std::min(used_bytes, freeable) + need > opt.hbm_budget_bytes) continue;
-        for (auto& e : idle) {
-          if (used_bytes + need <= opt.hbm_budget_bytes) break;
-          Model& o = models[e.second];
-          gprx_exact_destroy(o.h);
-          o.h = nullptr;
-          o.ready = false;
-          o.failed = true;  // later requests on an evicted model fail
-          used_bytes -= o.bytes;
-          o.bytes = 0;
-        }
-      }
-    } else if (r->t_submit >= best_t) {
-      continue;
+    if (r->t_submit >= best_t) continue;
+    if (r->kind == FIT && used_bytes + model_bytes(r->n, r->d) > opt.hbm_budget_bytes) {
+      uint64_t freeable = 0;
+      for (auto& o : models)
+        if (o.first != kv.first && o.second.ready && !o.second.busy && o.second.queue.empty()) freeable += o.second.bytes;
+      if (used_bytes - std::min(used_bytes, freeable) + model_bytes(r->n, r->d) > opt.hbm_budget_bytes) continue;
     }
     best_t = r->t_submit;
     best = kv.first;
@@ -155,22 +233,69 @@ uint64_t gprx_server::pick(std::vector<uint64_t>& batch) {
   if (!best) return 0;
   Model& m = models[best];
   Request* head = reqs[m.queue.front()].get();
+  if (head->kind == FIT && !admit_fit(best, head)) return 0;
   batch.push_back(head->id);
   m.queue.pop_front();
-  if (head->kind == PREDICT) {
-    // consecutive predicts of the same kind share one launch
-    while (!m.queue.empty()) {
+  m.busy = true;
+  if (head->kind == PREDICT && small_predict(head)) {
+    // small predicts: this model's consecutive ones, then the other models'
+    // waiting at the heads of their queues, share one grouped launch
+    while (!m.queue.empty() && batch.size() < SERVE_GROUP_MAX) {
       Request* nx = reqs[m.queue.front()].get();
-      if (nx->kind != PREDICT || nx->vkind != head->vkind) break;
+      if (!small_predict(nx) || nx->vkind != head->vkind) break;
       batch.push_back(nx->id);
       m.queue.pop_front();
     }
+    std::vector<std::pair<int64_t, uint64_t>> cand;
+    for (auto& kv : models) {
+      Model& o = kv.second;
+      if (kv.first == best || o.busy || o.queue.empty()) continue;
+      Request* r = reqs[o.queue.front()].get();
+      if (small_predict(r) && r->vkind == head->vkind && same_tree(best, kv.first))
+        cand.push_back({r->t_submit, kv.first});
+    }
+    std::sort(cand.begin(), cand.end());
+    for (auto& c : cand) {
+      Model& o = models[c.second];
+      bool took = false;
+      while (!o.queue.empty() && batch.size() < SERVE_GROUP_MAX) {
+        Request* r = reqs[o.queue.front()].get();
+        if (!small_predict(r) || r->vkind != head->vkind) break;
+        batch.push_back(r->id);
+        o.queue.pop_front();
+        took = true;
+      }
+      if (took) o.busy = true;
+      if (batch.size() >= SERVE_GROUP_MAX) break;
+    }
+  } else if (head->kind == PREDICT) {
+    // consecutive predicts of the same kind share one launch
+    while (!m.queue.empty()) {
+      Request* nx = reqs[m.queue.front()].get();
+      if (nx->kind != PREDICT || nx->vkind != head->vkind || small_predict(nx)) break;
+      batch.push_back(nx->id);
+      m.queue.pop_front();
+    }
+  } else if (batched_fit(head)) {
+    // other models' waiting small fits join the same batched launch, oldest first
+    std::vector<std::pair<int64_t, uint64_t>> cand;
+    for (auto& kv : models) {
+      Model& o = kv.second;
+      if (kv.first == best || o.busy || o.queue.empty()) continue;
+      Request* r = reqs[o.queue.front()].get();
+      if (batched_fit(r) && fit_compatible(head, r)) cand.push_back({r->t_submit, kv.first});
+    }
+    std::sort(cand.begin(), cand.end());
+    for (auto& c : cand) {
+      if (batch.size() >= SERVE_BATCH_FIT_MAX) break;
+      Model& o = models[c.second];
+      Request* r = reqs[o.queue.front()].get();
+      if (!admit_fit(c.second, r)) continue;
+      batch.push_back(r->id);
+      o.queue.pop_front();
+      o.busy = true;
+    }
   }
-  if (head->kind == FIT) {
-    m.bytes = model_bytes(head->n, head->d);
-    used_bytes += m.bytes;
-  }
-  m.busy = true;
   const int64_t t = now_ns();
   for (uint64_t id : batch) reqs[id]->t_start = t;
   return best;
@@ -185,7 +310,146 @@ void gprx_server::finish(Request* r, gprx_status st, const char* why) {
   }
 }
 
+// Small fits (one or several models): the batched evaluator fits every
+// problem (device L-BFGS, one CTA per problem), then each model is factored
+// at its fitted θ on its own handle for the requests that follow.
+void gprx_server::execute_fit_batch(std::vector<uint64_t>& batch) {
+  std::vector<Request*> rs;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    for (uint64_t id : batch) rs.push_back(reqs[id].get());
+  }
+  const Request* h0 = rs[0];
+  const size_t k = rs.size();
+  const uint64_t d = h0->d, p = h0->theta.size();
+  std::vector<uint64_t> ns(k);
+  std::vector<double> xall, yall, th0(k * p), thf(k * p);
+  for (size_t i = 0; i < k; ++i) {
+    ns[i] = rs[i]->n;
+    xall.insert(xall.end(), rs[i]->x.begin(), rs[i]->x.end());
+    yall.insert(yall.end(), rs[i]->y.begin(), rs[i]->y.end());
+    std::copy(rs[i]->theta.begin(), rs[i]->theta.end(), th0.begin() + i * p);
+  }
+  std::vector<gprx_fit_report> reps(k);
+  std::vector<int32_t> pst(k, GPRX_OK);
+  gprx_batch* b = nullptr;
+  gprx_options bo = h0->opt;
+  bo.device = opt.device;
+  gprx_status st = gprx_batch_create(xall.data(), yall.data(), ns.data(), k, d, h0->nodes.data(),
+                                     (int32_t)h0->nodes.size(), (int32_t)p, &bo, &b);
+  std::string why;
+  if (st == GPRX_OK) st = gprx_batch_fit(b, th0.data(), p, &h0->lopt, thf.data(), reps.data(), pst.data());
+  if (st != GPRX_OK) {
+    gprx_error_info info;
+    gprx_last_error(&info);
+    why = info.message;
+  }
+  if (b) gprx_batch_destroy(b);
+  std::vector<gprx_exact*> hs(k, nullptr);
+  std::vector<gprx_status> sts(k, st);
+  for (size_t i = 0; i < k; ++i) {
+    Request* r = rs[i];
+    if (st == GPRX_OK) {
+      sts[i] = (gprx_status)pst[i];
+      if (sts[i] == GPRX_OK)
+        sts[i] = gprx_exact_create(r->x.data(), r->n, r->d, r->y.data(), r->nodes.data(), (int32_t)r->nodes.size(),
+                                   thf.data() + i * p, (int32_t)p, &r->opt, &hs[i]);
+      if (sts[i] == GPRX_OK) sts[i] = gprx_exact_factor(hs[i]);
+      if (sts[i] != GPRX_OK && hs[i]) {
+        gprx_exact_destroy(hs[i]);
+        hs[i] = nullptr;
+      }
+      finish(r, sts[i], nullptr);
+    } else {
+      finish(r, st, why.c_str());
+    }
+    r->merged = (int)k;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  const int64_t t = now_ns();
+  if (k > 1) ++merged_fit_launches;
+  for (size_t i = 0; i < k; ++i) {
+    Request* r = rs[i];
+    Model& m = models[r->model];
+    m.h = hs[i];
+    m.d = r->d;
+    m.n = r->n;
+    m.fit_req = r->id;
+    m.ready = hs[i] != nullptr;
+    m.failed = hs[i] == nullptr;
+    if (m.failed && m.bytes) {
+      used_bytes -= m.bytes;
+      m.bytes = 0;
+    }
+    m.busy = false;
+    m.last_used = t;
+    r->t_end = t;
+    r->done = true;
+    lat[r->kind].push_back(r->t_end - r->t_submit);
+    ++completed;
+  }
+  cv_done.notify_all();
+  cv_work.notify_all();
+}
+
+// Small predicts of one or several models in one grouped launch.
+void gprx_server::execute_predict_group(std::vector<uint64_t>& batch) {
+  std::vector<Request*> rs;
+  std::vector<gprx_exact*> hs;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    for (uint64_t id : batch) {
+      rs.push_back(reqs[id].get());
+      hs.push_back(models[rs.back()->model].h);
+    }
+  }
+  const size_t k = rs.size();
+  std::vector<const double*> xs(k);
+  std::vector<uint64_t> qs(k);
+  std::vector<double*> means(k), vars(k);
+  for (size_t i = 0; i < k; ++i) {
+    xs[i] = rs[i]->xs.data();
+    qs[i] = rs[i]->q;
+    means[i] = rs[i]->mean_out;
+    vars[i] = rs[i]->var_out;
+  }
+  const gprx_status st =
+      gprx_exact_predict_group(hs.data(), k, xs.data(), qs.data(), rs[0]->vkind, means.data(), vars.data());
+  for (Request* r : rs) {
+    r->merged = (int)k;
+    finish(r, st, nullptr);
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  const int64_t t = now_ns();
+  if (k > 1) ++merged_launches;
+  for (Request* r : rs) {
+    Model& m = models[r->model];
+    m.busy = false;
+    m.last_used = t;
+    r->t_end = t;
+    r->done = true;
+    lat[r->kind].push_back(r->t_end - r->t_submit);
+    ++completed;
+  }
+  cv_done.notify_all();
+  cv_work.notify_all();
+}
+
 void gprx_server::execute(std::vector<uint64_t>& batch) {
+  bool small_fit, group;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    small_fit = batched_fit(reqs[batch[0]].get());
+    group = small_predict(reqs[batch[0]].get());
+  }
+  if (small_fit) {
+    execute_fit_batch(batch);
+    return;
+  }
+  if (group) {
+    execute_predict_group(batch);
+    return;
+  }
   std::vector<Request*> rs;
   Model* mp;
   gprx_exact* h;
@@ -271,8 +535,11 @@ void gprx_server::execute(std::vector<uint64_t>& batch) {
   if (head->kind == FIT) {
     m.h = ready ? h : nullptr;
     m.d = md;
+    m.n = head->n;
+    m.fit_req = head->id;
     m.ready = ready;
   }
+  if (online && n_now) m.n = n_now;
   m.failed = failed;
   m.online = online;
   const int64_t t = now_ns();
@@ -483,6 +750,7 @@ gprx_status gprx_server_stats(gprx_server* s, gprx_server_stats_t* out) {
   std::memset(out, 0, sizeof(*out));
   out->completed = s->completed;
   out->merged_launches = s->merged_launches;
+  out->merged_fit_launches = s->merged_fit_launches;
   out->used_bytes = s->used_bytes;
   uint64_t resident = 0;
   for (auto& kv : s->models)

@@ -222,6 +222,21 @@ gprx_status gprx_exact_factor_jitter(gprx_exact* h, double* jitter);
  * (GprCore::write_moments, src/gpr/shared.rs:754-820). */
 gprx_status gprx_exact_predict(gprx_exact* h, const double* xs, uint64_t q, int32_t variance_kind,
                                double* mean, double* var);
+/* Predictive mean and diagonal variance for k requests against k fitted
+ * exact models in one launch (no counterpart in the reference: each request
+ * is one GprCore::write_moments, src/gpr/shared.rs:754-820; the serving loop
+ * batches small predictions of different models with it).  Request i asks
+ * handles[i] at q[i] points xs[i] (column-major q[i]×d) and receives mean[i]
+ * and var[i] (q[i] values each); a handle may appear several times.  Every
+ * model has at most 1024 points and 16 features, is not online, and all share
+ * one device, d and the kernel's ARD width (else GPRX_CAPACITY /
+ * GPRX_INVALID_CONFIG).  One CTA computes each 16-query tile of a request in
+ * a fixed order, so a request's results do not depend on the others; they
+ * agree with gprx_exact_predict to rounding (a different summation order).
+ * The work runs on handles[0]'s stream; the call returns when it is done. */
+gprx_status gprx_exact_predict_group(gprx_exact* const* handles, uint64_t k, const double* const* xs,
+                                     const uint64_t* q, int32_t variance_kind, double* const* mean,
+                                     double* const* var);
 
 /* Saved models (gprx's format_version 1: <dir>/config.json and
  * <dir>/model.safetensors, docs/persist-format.md; src/persist/mod.rs).
@@ -357,7 +372,8 @@ gprx_status gprx_sgpr_insert(gprx_sgpr* h, const double* x_new, double y_new, ui
  * reassembly when the downdate fails or the pivot gate does not hold. */
 gprx_status gprx_sgpr_delete(gprx_sgpr* h, uint64_t id);
 uint64_t gprx_sgpr_n(const gprx_sgpr* h);
-/* 1 when the last insert/delete updated in place, 0 when it reassembled. */
+/* 1 when the last insert/delete (of a point or of an inducing point)
+ * updated in place, 0 when it reassembled. */
 int32_t gprx_sgpr_last_step_in_place(const gprx_sgpr* h);
 /* PointIds in registry order (src/points.rs:76). */
 gprx_status gprx_sgpr_point_ids(gprx_sgpr* h, uint64_t* out, uint64_t n);
@@ -368,10 +384,16 @@ gprx_status gprx_sgpr_set_inducing(gprx_sgpr* h, const double* z, uint64_t m);
 /* OnlineSgpr::insert_inducing / delete_inducing / inducing_ids
  * (src/sgpr/online/mod.rs:1943,1301,694): append one inducing point (its id
  * is returned; ids are never reused) or remove one by id (m ≤ 1 →
- * GPRX_INSUFFICIENT_DATA, unknown id → GPRX_INVALID_POINT_ID).  Each change
- * assembles the VFE system of the new set (O(n m²), the reference's own path
- * when its bordered update does not apply), so the model equals Sgpr::factor
- * at the same θ, X and Z; on an error the model keeps its inducing set. */
+ * GPRX_INSUFFICIENT_DATA, unknown id → GPRX_INVALID_POINT_ID).  An insert
+ * takes the bordered update of the factors and one new row of A (O(n m);
+ * inducing_append, src/sgpr/factor/updates.rs:296-390) when K_mm's factor
+ * took no jitter, its pivots hold (min L_ii² / K_ii > 1e-5) and both bordered
+ * pivots exceed 1e-5 of their diagonal, and room for the row exists;
+ * otherwise, and for a delete, the VFE system of the new set is assembled
+ * (O(n m²), the reference's own fallback), so the model equals Sgpr::factor
+ * at the same θ, X and Z (within 1e-10 after a bordered insert).
+ * gprx_sgpr_last_step_in_place tells which.  On an error the model keeps its
+ * inducing set. */
 gprx_status gprx_sgpr_insert_inducing(gprx_sgpr* h, const double* z_new, uint64_t* id);
 gprx_status gprx_sgpr_delete_inducing(gprx_sgpr* h, uint64_t id);
 uint64_t gprx_sgpr_m(const gprx_sgpr* h);
@@ -483,9 +505,10 @@ typedef struct {
 
 typedef struct {
   uint64_t completed;
-  uint64_t merged_launches;
+  uint64_t merged_launches;      /* predict launches that served several requests */
   uint64_t used_bytes;
   uint64_t resident_models;
+  uint64_t merged_fit_launches;  /* batched fit launches that served several models */
 } gprx_server_stats_t;
 
 void gprx_server_options_default(gprx_server_options* opt);

@@ -1,5 +1,7 @@
 """The serving loop (gprx_server_*): results are the same alone and in a mix,
-consecutive predicts share a launch, and the HBM budget evicts idle models.
+small fits of several models share a batched launch, small predicts of one
+or several models share a grouped launch, and the HBM budget evicts idle
+models.
 
 Each model's requests run in submission order on the model's own stream, so
 a model's fit, predictions and online steps must give the same values
@@ -14,6 +16,7 @@ import numpy as np
 import pytest
 
 import gprx_b200 as gx
+import oracle_lib as O
 
 pytestmark = pytest.mark.gpu
 
@@ -91,12 +94,13 @@ def test_results_same_alone_and_in_the_mix():
     assert len(alone) == len(mixed)
     for a, b in zip(alone, mixed):
         assert np.array_equal(a, b)
-    # and the same as the direct API
+    # and the direct API's fit (the server's small predicts run the grouped
+    # kernel, which sums in another order than gprx_exact_predict)
     f = gx.Gpr(spec(d), gx.GaussianLikelihood(0.05), optimizer=LB).fit(x, 600, d, y)
     rs = np.random.RandomState(7)
     xs = rs.standard_normal(40 * d)
     p = f.predict(xs, 40, d)
-    assert np.array_equal(p.mean, alone[0]) and np.array_equal(p.variance, alone[1])
+    assert np.all(O.rel_err(p.mean, alone[0]) <= 1e-10) and np.all(O.rel_err(p.variance, alone[1]) <= 1e-10)
 
 
 def test_consecutive_predicts_share_a_launch():
@@ -117,7 +121,7 @@ def test_consecutive_predicts_share_a_launch():
         r2, m2, v2 = srv.submit_predict(mid, xs, q)
         st, info = srv.wait(r2)
         assert st == 0 and info["merged"] == 1
-        assert np.allclose(mean, m2, rtol=1e-12, atol=1e-14) and np.allclose(var, v2, rtol=1e-12, atol=1e-14)
+        assert np.array_equal(mean, m2) and np.array_equal(var, v2)
     srv.close()
 
 
@@ -136,4 +140,80 @@ def test_hbm_budget_evicts_the_least_recently_used_model():
     assert srv.wait(rid)[0] == gx.api.L.INVALID_CONFIG  # evicted
     rid, _, _ = srv.submit_predict(ids[2], np.zeros(d), 1)
     assert srv.wait(rid)[0] == 0
+    srv.close()
+
+
+def test_small_fits_share_one_batched_launch_and_match_alone():
+    # fits of n ≤ 512 always run on the batched evaluator; fits waiting at the
+    # heads of several models' queues share one launch, and each model's
+    # results are bit for bit those of the same fit alone
+    d = 4
+    lb = gx.Lbfgs(max_iterations=25)
+    sizes = (120, 300, 64, 500)
+    sets = [data(n, d, 60 + k) for k, n in enumerate(sizes)]
+    xs = np.random.RandomState(9).standard_normal(30 * d)
+    alone = []
+    for (x, y), n in zip(sets, sizes):
+        srv = gx.Server(workers=2)
+        mid = srv.submit_fit(spec(d), gx.GaussianLikelihood(0.1), x, n, d, y, optimizer=lb)
+        st, info = srv.wait(mid)
+        assert st == 0 and info["merged"] == 1
+        rid, m, v = srv.submit_predict(mid, xs, 30)
+        assert srv.wait(rid)[0] == 0
+        alone.append((m.copy(), v.copy()))
+        assert srv.stats()["merged_fit_launches"] == 0
+        srv.close()
+    # together: one worker busy with a large fit while the small ones queue
+    srv = gx.Server(workers=1)
+    xb, yb = data(1500, d, 99)
+    big = srv.submit_fit(spec(d), gx.GaussianLikelihood(0.1), xb, 1500, d, yb, optimizer=lb)
+    mids = [srv.submit_fit(spec(d), gx.GaussianLikelihood(0.1), x, n, d, y, optimizer=lb)
+            for (x, y), n in zip(sets, sizes)]
+    assert srv.wait(big)[0] == 0
+    for k, mid in enumerate(mids):
+        st, info = srv.wait(mid)
+        assert st == 0 and info["merged"] == len(sizes)
+        rid, m, v = srv.submit_predict(mid, xs, 30)
+        assert srv.wait(rid)[0] == 0
+        assert np.array_equal(m, alone[k][0]) and np.array_equal(v, alone[k][1])
+    assert srv.stats()["merged_fit_launches"] == 1
+    srv.close()
+    # the plumbing: each model predicts from the batched fit's θ (the oracle's
+    # prediction at the θ GprBatch.fit reaches for the same problem)
+    for k, ((x, y), n) in enumerate(zip(sets, sizes)):
+        theta0 = np.array(spec(d).get_params() + [math.log(0.1)])
+        r = gx.GprBatch(spec(d), [x], [y], d).fit(theta0[None, :], lb)
+        mo, vo = O.exact_predict([[11, d]], r.params[0], x, n, d, y, xs, 30, 1)
+        assert np.all(O.rel_err(alone[k][0], mo) <= 1e-10) and np.all(O.rel_err(alone[k][1], vo) <= 1e-10)
+
+
+def test_small_predicts_of_several_models_share_a_launch():
+    d = 3
+    srv = gx.Server(workers=1)
+    mids = []
+    for k, n in enumerate((700, 300, 900)):
+        x, y = data(n, d, 70 + k)
+        mids.append(srv.submit_fit(spec(d), gx.GaussianLikelihood(0.1), x, n, d, y, optimizer=gx.Fixed()))
+    for mid in mids:
+        assert srv.wait(mid)[0] == 0
+    # a large fit keeps the one worker busy while predicts of the three models queue
+    xb, yb = data(1500, d, 99)
+    big = srv.submit_fit(spec(d), gx.GaussianLikelihood(0.1), xb, 1500, d, yb, optimizer=gx.Fixed())
+    rs = np.random.RandomState(2)
+    reqs = []
+    for mid in mids + mids:
+        q = int(rs.randint(1, 60))
+        xs = rs.standard_normal(q * d)
+        reqs.append((mid, srv.submit_predict(mid, xs, q), xs, q))
+    assert srv.wait(big)[0] == 0
+    for mid, (rid, mean, var), xs, q in reqs:
+        st, info = srv.wait(rid)
+        assert st == 0 and info["merged"] == len(reqs)
+    assert srv.stats()["merged_launches"] >= 1
+    # each equals the same request alone
+    for mid, (rid, mean, var), xs, q in reqs:
+        r2, m2, v2 = srv.submit_predict(mid, xs, q)
+        st, info = srv.wait(r2)
+        assert st == 0 and info["merged"] == 1
+        assert np.array_equal(mean, m2) and np.array_equal(var, v2)
     srv.close()
