@@ -300,8 +300,11 @@ gprx_status ExactState::online_delete(uint64_t id) {
   if ((st = read_status(&ds)) != GPRX_OK) return st;
   if (ds.code != GPRX_OK) return status_to_error(ds, 0.0, n, GPRX_STAGE_ONLINE_DELETE);
   std::swap(A.p, nA.p);
+  std::swap(A.n, nA.n);
   std::swap(x.p, nx.p);
+  std::swap(x.n, nx.n);
   std::swap(y.p, ny.p);
+  std::swap(y.n, ny.n);
   y_host.erase(y_host.begin() + idx);
   ids.erase(it);
   n -= 1;

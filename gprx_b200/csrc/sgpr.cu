@@ -261,6 +261,29 @@ __global__ void __launch_bounds__(R1C_THREADS) chol_rank1_kernel(double* L, long
   }
 }
 
+// Row m of a lower factor L (ld): L[m, 0..m-1] = v, L[m, m] = diag, and zeros
+// above the diagonal of column m.
+__global__ void border_row_kernel(double* L, long long ld, int m, const double* v, double diag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) {
+    L[m + (long long)i * ld] = v[i];
+    L[i + (long long)m * ld] = 0.0;
+  } else if (i == m) {
+    L[m + (long long)m * ld] = diag;
+  }
+}
+
+// The new row of A: a_c = (k(z, x_c) − (Aᵀ l)_c) / ℓ, into row m of A (ld)
+// and into a contiguous copy.
+__global__ void border_a_row_kernel(const double* krow, const double* atl, double inv_ell, double* A, long long ld,
+                                    int m, long long n, double* copy) {
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const double v = (krow[c] - atl[c]) * inv_ell;
+    A[m + c * ld] = v;
+    copy[c] = v;
+  }
+}
+
 __global__ void axpy_kernel(double* y, const double* x, double a, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] = fma(a, x[i], y[i]);
@@ -293,7 +316,7 @@ struct SgprState {
   int m = 0, d = 0;
   long long ldm = 0;
   DevBuf<double> x, y, z, Lmm, linv_mm, Amat, Bl, linv_B, w, ay, G, H, Wm, Xb, Xt, splitbuf, partials, res, vtmp,
-      qbuf, qbuf2, qx, Btrial, covbuf, covl, covlinv, zbuf;
+      qbuf, qbuf2, qx, Btrial, covbuf, covl, covlinv, zbuf, border;
   DevBuf<int> slot_param;
   DevBuf<DevStatus> status;
   // mixed precision: the two m×m Gram products over n (B = A Aᵀ and H = G Aᵀ)
@@ -375,6 +398,11 @@ struct SgprState {
   gprx_status insert_inducing(const double* znew, uint64_t* id);
   gprx_status delete_inducing(uint64_t id);
   gprx_status replace_inducing(const std::vector<double>& znew, int mm);
+  // the bordered insert of one inducing point; *applied = false when a gate
+  // sends the change to the assembly instead (nothing changed then)
+  gprx_status insert_inducing_bordered(const double* znew, bool* applied);
+  // out (m) = A v for a device vector v over the n points (split-K product)
+  gprx_status a_times(const double* v, double* out);
   // one shard of a VFE evaluation over n split across processes (the sums
   // over n travel in two exchange buffers that the caller sums over shards)
   gprx_status factor_kmm_and_a(EmuWork& ew, bool& emu);
@@ -447,8 +475,9 @@ gprx_status SgprState::create(const double* xh, uint64_t nn, uint64_t dd, const 
   GPRX_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   for (auto& e : ev) GPRX_CUDA_TRY(cudaEventCreate(&e));
   int nblk = ceil_div(m, NB);
-  if (z.alloc((size_t)m * d) || Lmm.alloc((size_t)ldm * m) || linv_mm.alloc((size_t)nblk * NB * NB) ||
-      Bl.alloc((size_t)ldm * m) || linv_B.alloc((size_t)nblk * NB * NB) || w.alloc(ldm) || ay.alloc(ldm) ||
+  // the m×m factors keep ld columns, the room a bordered inducing insert grows into
+  if (z.alloc((size_t)m * d) || Lmm.alloc((size_t)ldm * ldm) || linv_mm.alloc((size_t)nblk * NB * NB) ||
+      Bl.alloc((size_t)ldm * ldm) || linv_B.alloc((size_t)nblk * NB * NB) || w.alloc(ldm) || ay.alloc(ldm) ||
       vtmp.alloc(ldm) || partials.alloc((size_t)grad_max_blocks() * 2 * 64 + 4096) || res.alloc(128) ||
       slot_param.alloc(64) || status.alloc(1))
     return set_error(GPRX_OUT_OF_MEMORY, "device allocation failed");
@@ -972,7 +1001,8 @@ gprx_status SgprState::remove(uint64_t id) {
   bool ok = pivot_ratio > X_STEP_PIVOT_RTOL;
   if (ok) {
     // trial downdate of L_B with the point's column of A
-    if (Btrial.ensure((size_t)ldm * m) != cudaSuccess) return set_error(GPRX_OUT_OF_MEMORY, "trial factor");
+    // the trial factor becomes L_B on success: it keeps L_B's ld columns
+    if (Btrial.ensure((size_t)ldm * ldm) != cudaSuccess) return set_error(GPRX_OUT_OF_MEMORY, "trial factor");
     if ((st = reset_status()) != GPRX_OK) return st;
     const double* col = Amat.p + slot * ldm;
     GPRX_CUDA_TRY(cudaMemcpyAsync(Btrial.p, Bl.p, sizeof(double) * ldm * m, cudaMemcpyDeviceToDevice, stream));
@@ -990,6 +1020,7 @@ gprx_status SgprState::remove(uint64_t id) {
       axpy_kernel<<<ceil_div(m, 256), 256, 0, stream>>>(ay.p, col, -ydel, m);
       count_launch();
       std::swap(Bl.p, Btrial.p);
+      std::swap(Bl.n, Btrial.n);
       GPRX_CUDA_TRY(tri_inv_blocks(Bl.p, ldm, m, false, linv_B.p, status.p, stream));
     }
   }
@@ -1028,9 +1059,15 @@ static gprx_status download_z(SgprState& s, std::vector<double>& out) {
 }
 
 // Assembles the VFE system of a changed inducing set; on failure the model
-// goes back to the set it had (OnlineSgpr::atomically).  Every change is the
-// assembly of the new set (the reference's own fallback, O(n m²)), so its
-// results are those of Sgpr::factor at the same θ, X and Z.
+// goes back to the set it had (OnlineSgpr::atomically).  An insert takes the
+// bordered update below when its gates hold; a delete, and an insert whose
+// gates do not hold, assemble the new set (the reference's own fallback,
+// O(n m²)), so their results are those of Sgpr::factor at the same θ, X and
+// Z.  The reference's trailing delete (a rank-1 update of L_mm, then A solved
+// against it from K(Z, X) = L A and B formed again) keeps the assembly's
+// O(n m²) solve and Gram product and saves only the kernel evaluations of
+// K(Z, X), which on the GPU cost a small part of the assembly; the delete
+// takes the assembly.
 gprx_status SgprState::replace_inducing(const std::vector<double>& znew, int mm) {
   std::vector<double> old;
   gprx_status st = download_z(*this, old);
@@ -1045,11 +1082,123 @@ gprx_status SgprState::replace_inducing(const std::vector<double>& znew, int mm)
   return st;
 }
 
+gprx_status SgprState::a_times(const double* v, double* out) {
+  const int nn = (int)n;
+  const int S = (int)std::min<long long>(32, std::max<long long>(1, nn / 4096));
+  if (splitbuf.ensure((size_t)S * ldm) != cudaSuccess) return set_error(GPRX_OUT_OF_MEMORY, "split buffer");
+  GemmParams p = gemm_params(m, 1, nn, Amat.p, ldm, v, nn, splitbuf.p, ldm, 1.0, 0.0, status.p);
+  p.mode = GEMM_SPLIT_K;
+  p.splits = S;
+  p.split_stride = ldm;
+  GPRX_CUDA_TRY(dgemm(false, false, p, stream));
+  split_reduce_kernel<<<grid_for(m, 256), 256, 0, stream>>>(splitbuf.p, S, ldm, m, 0, 0.0, false, out, status.p);
+  count_launch();
+  return GPRX_OK;
+}
+
+// OnlineSgpr::insert_inducing by the bordered update (inducing_append,
+// src/sgpr/factor/updates.rs:296-390; ADR 0005): from a factor of K_mm without
+// jitter whose pivots hold (min L_ii² / K_ii > 1e-5), l = L⁻¹ k(Z, z),
+// ℓ² = k(z, z) − ‖l‖², the new row of A a = (k(z, X) − Aᵀ l) / ℓ (O(n m)),
+// b = L_B⁻¹ (A a), β² = σ² + ‖a‖² − ‖b‖²; both bordered pivots must exceed
+// 1e-5 of the diagonal they cancel from.  Needs room for row m in the
+// buffers (m + 1 ≤ ld and the same number of diagonal blocks); otherwise,
+// or when a gate does not hold, *applied is false and nothing changed.
+gprx_status SgprState::insert_inducing_bordered(const double* znew, bool* applied) {
+  *applied = false;
+  constexpr double TAU = 1e-5;
+  if (kmm_jitter > 0.0 || !(pivot_ratio > TAU)) return GPRX_OK;
+  if (m + 1 > ldm || ceil_div(m + 1, NB) != ceil_div(m, NB) || n > INT32_MAX) return GPRX_OK;
+  const size_t need = (size_t)ldm * (size_t)(m + 1);
+  if (Lmm.n < need || Bl.n < need || linv_mm.n < (size_t)ceil_div(m + 1, NB) * NB * NB ||
+      linv_B.n < (size_t)ceil_div(m + 1, NB) * NB * NB || Amat.n < (size_t)ldm * (size_t)std::max(cap, 1LL))
+    return GPRX_OK;
+  gprx_status st;
+  if (!assembled && (st = assemble()) != GPRX_OK) return st;
+  const int nn = (int)n;
+  if (border.ensure((size_t)3 * std::max(cap, 1LL) + 2 * ldm + d) != cudaSuccess)
+    return set_error(GPRX_OUT_OF_MEMORY, "border buffers");
+  double* krow = border.p;               // k(z, X) (n)
+  double* atl = krow + cap;              // Aᵀ l (n)
+  double* arow = atl + cap;              // the new row of A (n)
+  double* lvec = arow + cap;             // l (m)
+  double* bvec = lvec + ldm;             // b (m)
+  double* zdev = bvec + ldm;             // z (d)
+  if ((st = reset_status()) != GPRX_OK) return st;
+  GPRX_CUDA_TRY(cudaMemcpyAsync(zdev, znew, sizeof(double) * d, cudaMemcpyHostToDevice, stream));
+  GPRX_CUDA_TRY(fill_cross(kern, z.p, m, m, zdev, 1, 1, lvec, ldm, status.p, stream));
+  GPRX_CUDA_TRY(trsm_lower(Lmm.p, ldm, m, linv_mm.p, lvec, ldm, 1, status.p, stream));
+  GPRX_CUDA_TRY(dot_dev(lvec, lvec, m, res.p + 30, status.p, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p + 30, res.p + 30, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  if ((st = sync_check(GPRX_STAGE_ONLINE_INSERT)) != GPRX_OK) return st;
+  const double kdiag = kern.diag_value() + kmm_jitter;
+  const double ell2 = kdiag - res_h.p[30];
+  if (!(std::isfinite(ell2) && ell2 > TAU * kdiag)) return GPRX_OK;
+  const double ell = std::sqrt(ell2);
+  // a = (k(z, X) − Aᵀ l) / ℓ; ‖a‖², a·y; b = L_B⁻¹ (A a)
+  GPRX_CUDA_TRY(fill_cross(kern, zdev, 1, 1, x.p, cap, nn, krow, 1, status.p, stream));
+  GPRX_CUDA_TRY(gemv_t(Amat.p, ldm, m, nn, false, lvec, atl, status.p, stream));
+  border_a_row_kernel<<<grid_for(nn, 256), 256, 0, stream>>>(krow, atl, 1.0 / ell, Amat.p, ldm, m, nn, arow);
+  count_launch();
+  if ((st = a_times(arow, bvec)) != GPRX_OK) return st;
+  GPRX_CUDA_TRY(trsm_lower(Bl.p, ldm, m, linv_B.p, bvec, ldm, 1, status.p, stream));
+  GPRX_CUDA_TRY(dot_dev(arow, arow, nn, res.p + 31, status.p, stream));
+  GPRX_CUDA_TRY(dot_dev(bvec, bvec, m, res.p + 32, status.p, stream));
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p + 31, res.p + 31, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+  if ((st = sync_check(GPRX_STAGE_ONLINE_INSERT)) != GPRX_OK) return st;
+  const double an2 = res_h.p[31];
+  const double bdiag = noise() + an2;
+  const double beta2 = bdiag - res_h.p[32];
+  if (!(std::isfinite(beta2) && beta2 > TAU * bdiag)) return GPRX_OK;  // row m of A is scratch beyond m
+  // commit: Z, the bordered L and L_B and their diagonal-block inverses, A y, w
+  std::vector<double> zo, zn((size_t)(m + 1) * d);
+  if ((st = download_z(*this, zo)) != GPRX_OK) return st;
+  for (int f = 0; f < d; ++f) {
+    std::copy(zo.begin() + (size_t)f * m, zo.begin() + (size_t)(f + 1) * m, zn.begin() + (size_t)f * (m + 1));
+    zn[(size_t)f * (m + 1) + m] = znew[f];
+  }
+  if (z.alloc(zn.size()) != cudaSuccess) return set_error(GPRX_OUT_OF_MEMORY, "inducing points");
+  GPRX_CUDA_TRY(cudaMemcpyAsync(z.p, zn.data(), sizeof(double) * zn.size(), cudaMemcpyHostToDevice, stream));
+  border_row_kernel<<<ceil_div(m + 1, 256), 256, 0, stream>>>(Lmm.p, ldm, m, lvec, ell);
+  border_row_kernel<<<ceil_div(m + 1, 256), 256, 0, stream>>>(Bl.p, ldm, m, bvec, std::sqrt(beta2));
+  count_launch(2);
+  m += 1;
+  GPRX_CUDA_TRY(tri_inv_blocks(Lmm.p, ldm, m, false, linv_mm.p, status.p, stream));
+  GPRX_CUDA_TRY(tri_inv_blocks(Bl.p, ldm, m, false, linv_B.p, status.p, stream));
+  if ((st = a_times(y.p, ay.p)) != GPRX_OK) return st;
+  pivot_ratio_kernel<<<1, 1024, 0, stream>>>(Lmm.p, ldm, m, res.p + 10);
+  count_launch();
+  GPRX_CUDA_TRY(cudaMemcpyAsync(res_h.p + 10, res.p + 10, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  if ((st = sync_check(GPRX_STAGE_ONLINE_INSERT)) != GPRX_OK) return st;
+  pivot_ratio = res_h.p[10];
+  trace_sum -= an2;
+  *applied = true;
+  last_in_place = 1;
+  return solve_w();
+}
+
 gprx_status SgprState::insert_inducing(const double* znew, uint64_t* id) {
   if (!znew || !id) return set_error(GPRX_INVALID_ARGUMENT, "null pointer");
   if (!all_finite(znew, d)) return set_error(GPRX_NONFINITE_INPUT, "non-finite inducing point");
+  drop_shard_state();
+  bool applied = false;
+  gprx_status st = insert_inducing_bordered(znew, &applied);
+  if (st != GPRX_OK) {
+    // a device failure part way: go back to the current set by assembly
+    gprx_error_info saved = last_error();
+    std::vector<double> zo;
+    if (download_z(*this, zo) == GPRX_OK) set_inducing(zo.data(), (uint64_t)m);
+    last_error() = saved;
+    return st;
+  }
+  if (applied) {
+    *id = next_inducing_id++;
+    inducing_ids.push_back(*id);
+    return GPRX_OK;
+  }
+  last_in_place = 0;
   std::vector<double> zo, zn((size_t)(m + 1) * d);
-  gprx_status st = download_z(*this, zo);
+  st = download_z(*this, zo);
   if (st != GPRX_OK) return st;
   for (int f = 0; f < d; ++f) {  // append a row (column-major)
     std::copy(zo.begin() + (size_t)f * m, zo.begin() + (size_t)(f + 1) * m, zn.begin() + (size_t)f * (m + 1));
@@ -1073,6 +1222,8 @@ gprx_status SgprState::delete_inducing(uint64_t id) {
   for (int f = 0; f < d; ++f)
     for (int i = 0; i < m; ++i)
       if (i != idx) zn.push_back(zo[(size_t)f * m + i]);
+  drop_shard_state();
+  last_in_place = 0;
   if ((st = replace_inducing(zn, m - 1)) != GPRX_OK) return st;
   inducing_ids.erase(inducing_ids.begin() + idx);
   return GPRX_OK;
@@ -1087,8 +1238,8 @@ gprx_status SgprState::set_inducing(const double* zh, uint64_t mm) {
     int nblk = ceil_div((int)mm, NB);
     // A is re-laid out for the new m (its contents are recomputed below)
     DevBuf<double> nA;
-    if (z.alloc((size_t)mm * d) || Lmm.alloc((size_t)new_ldm * mm) || linv_mm.alloc((size_t)nblk * NB * NB) ||
-        Bl.alloc((size_t)new_ldm * mm) || linv_B.alloc((size_t)nblk * NB * NB) || w.alloc(new_ldm) ||
+    if (z.alloc((size_t)mm * d) || Lmm.alloc((size_t)new_ldm * new_ldm) || linv_mm.alloc((size_t)nblk * NB * NB) ||
+        Bl.alloc((size_t)new_ldm * new_ldm) || linv_B.alloc((size_t)nblk * NB * NB) || w.alloc(new_ldm) ||
         ay.alloc(new_ldm) || vtmp.alloc(new_ldm) || nA.alloc((size_t)new_ldm * std::max(cap, 1LL)))
       return set_error(GPRX_OUT_OF_MEMORY, "inducing buffers");
     std::swap(Amat.p, nA.p);

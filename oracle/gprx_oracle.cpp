@@ -1564,9 +1564,103 @@ int orc_sgpr_delete(void* p, uint64_t id) {
   return sgpr_assemble(h);
 }
 
+// OnlineSgpr::insert_inducing (src/sgpr/online/mod.rs:1943-1992,1154-1220;
+// inducing_append, src/sgpr/factor/updates.rs:296-390): from a factor of
+// K_mm without jitter whose pivots hold (min L_ii²/K_ii > 1e-5), the bordered
+// LLT of K_mm and B and the new row of A, a_new = (k(z, X) − lᵀA)/ℓ; when a
+// bordered pivot is at most 1e-5 of its diagonal, or the factor's gate does
+// not hold, the VFE system of the new set is assembled.  last_in_place
+// tells which.
+int orc_sgpr_insert_inducing(void* p, const double* znew) {
+  OrcSgpr* h = (OrcSgpr*)p;
+  const int64_t n = h->n, m = h->m;
+  const int d = h->d;
+  const double tau = 1e-5;
+  std::vector<double> nz((size_t)(m + 1) * d);
+  for (int f = 0; f < d; ++f) {
+    for (int64_t i = 0; i < m; ++i) nz[(size_t)f * (m + 1) + i] = h->z[(size_t)f * m + i];
+    nz[(size_t)f * (m + 1) + m] = znew[f];
+  }
+  bool ok = h->kmm_jitter <= 0.0 && h->pivot_ratio > tau;
+  std::vector<double> l(m), a_new(n), b(m);
+  double ell = 0.0, beta = 0.0;
+  long double an2 = 0.0L;
+  if (ok) {
+    for (int64_t i = 0; i < m; ++i) l[i] = kval(h->t, h->z.data() + i, m, znew, 1, d);
+    trsm_lower(h->lmm.data(), m, m, l.data(), 1, m);
+    const double kdiag = kval(h->t, znew, 1, znew, 1, d) + h->kmm_jitter;
+    double ell2 = kdiag - sumsq_ld(l.data(), m);
+    ok = std::isfinite(ell2) && ell2 > tau * kdiag;
+    if (ok) {
+      ell = std::sqrt(ell2);
+#pragma omp parallel for schedule(static)
+      for (int64_t c = 0; c < n; ++c)
+        a_new[c] = (kval(h->t, znew, 1, h->x.data() + c, n, d) - dot_ld(l.data(), &AT(h->a, m, 0, c), m)) / ell;
+      for (int64_t c = 0; c < n; ++c) an2 += (long double)a_new[c] * a_new[c];
+      std::vector<long double> v(m, 0.0L);
+#pragma omp parallel
+      {
+        std::vector<long double> vt(m, 0.0L);
+#pragma omp for schedule(static)
+        for (int64_t c = 0; c < n; ++c)
+          for (int64_t i = 0; i < m; ++i) vt[i] += (long double)AT(h->a, m, i, c) * a_new[c];
+#pragma omp critical
+        for (int64_t i = 0; i < m; ++i) v[i] += vt[i];
+      }
+      for (int64_t i = 0; i < m; ++i) b[i] = (double)v[i];
+      trsm_lower(h->bl.data(), m, m, b.data(), 1, m);
+      const double bdiag = h->noise + (double)an2;
+      const double beta2 = bdiag - sumsq_ld(b.data(), m);
+      ok = std::isfinite(beta2) && beta2 > tau * bdiag;
+      beta = ok ? std::sqrt(beta2) : 0.0;
+    }
+  }
+  if (!ok) {
+    h->z.swap(nz);
+    h->m = m + 1;
+    h->last_in_place = 0;
+    return sgpr_assemble(h);
+  }
+  const int64_t m1 = m + 1;
+  Mat nl((size_t)m1 * m1, 0.0), nb((size_t)m1 * m1, 0.0), na((size_t)m1 * n);
+  for (int64_t j = 0; j < m; ++j)
+    for (int64_t i = j; i < m; ++i) {
+      AT(nl, m1, i, j) = AT(h->lmm, m, i, j);
+      AT(nb, m1, i, j) = AT(h->bl, m, i, j);
+    }
+  for (int64_t j = 0; j < m; ++j) {
+    AT(nl, m1, m, j) = l[j];
+    AT(nb, m1, m, j) = b[j];
+  }
+  AT(nl, m1, m, m) = ell;
+  AT(nb, m1, m, m) = beta;
+  for (int64_t c = 0; c < n; ++c) {
+    for (int64_t i = 0; i < m; ++i) AT(na, m1, i, c) = AT(h->a, m, i, c);
+    AT(na, m1, m, c) = a_new[c];
+  }
+  h->lmm.swap(nl);
+  h->bl.swap(nb);
+  h->a.swap(na);
+  h->z.swap(nz);
+  h->m = m1;
+  h->trace_sum -= (double)an2;
+  // A y and w from the new A and L_B (refresh_w)
+  std::vector<long double> ay(m1, 0.0L);
+  for (int64_t c = 0; c < n; ++c)
+    for (int64_t i = 0; i < m1; ++i) ay[i] += (long double)AT(h->a, m1, i, c) * h->y[c];
+  h->ay.assign(m1, 0.0);
+  for (int64_t i = 0; i < m1; ++i) h->ay[i] = (double)ay[i];
+  h->w = h->ay;
+  llt_solve(h->bl.data(), m1, m1, h->w.data());
+  h->pivot_ratio = min_pivot_ratio(h->lmm, m1);
+  h->last_in_place = 1;
+  return 0;
+}
+
 // Replaces the inducing set (an inducing insert/delete taken by reassembly).
 int orc_sgpr_set_inducing(void* p, const double* z, int64_t m) {
   OrcSgpr* h = (OrcSgpr*)p;
+  h->last_in_place = 0;
   h->z.assign(z, z + m * h->d);
   h->m = m;
   return sgpr_assemble(h);

@@ -75,6 +75,7 @@ def lib():
     L.orc_sgpr_insert.argtypes = [C.c_void_p, D, C.c_double, U64]
     L.orc_sgpr_delete.argtypes = [C.c_void_p, C.c_uint64]
     L.orc_sgpr_set_inducing.argtypes = [C.c_void_p, D, C.c_int64]
+    L.orc_sgpr_insert_inducing.argtypes = [C.c_void_p, D]
     L.orc_sgpr_n.argtypes = [C.c_void_p]
     L.orc_sgpr_n.restype = C.c_int64
     L.orc_sgpr_kmm_jitter.argtypes = [C.c_void_p]
@@ -317,6 +318,13 @@ class Sgpr:
 
     def set_inducing(self, z, m):
         st = lib().orc_sgpr_set_inducing(self.h, _ptr(_f(z)), m)
+        if st != 0:
+            raise OracleError(st)
+
+    def insert_inducing(self, z_new):
+        """Bordered insert when the gates hold, else the assembly of the new
+        set; last_in_place tells which (inducing_append, updates.rs:296-390)."""
+        st = lib().orc_sgpr_insert_inducing(self.h, _ptr(_f(z_new)))
         if st != 0:
             raise OracleError(st)
 

@@ -264,3 +264,36 @@ def test_inducing_ids_changes_and_errors():
     one = model(nodes, theta, 0.05, x.T.reshape(-1), n, d, y, x[:1].T.reshape(-1), 1).into_online()
     with pytest.raises(gx.InsufficientData):
         one.delete_inducing(0)
+
+
+def test_inducing_insert_bordered_matches_oracle_and_gate():
+    # inducing inserts take the bordered update (O(n m)) when the factor and
+    # the bordered pivots hold, else the assembly: the decision is the
+    # oracle's bit for bit, and NLML, gradient and predictions agree at 1e-10
+    rs = np.random.RandomState(12)
+    d, n, m = 2, 500, 9
+    nodes, theta = [[11, 2]], [math.log(0.3), math.log(0.45)]
+    params = np.array(theta + [math.log(0.05)])
+    x = rs.uniform(0, 1, size=(n, d))
+    y = np.sin(4 * x.sum(1)) + 0.05 * rs.standard_normal(n)
+    z = [x[i] for i in range(m)]
+    zc = np.array(z).T.reshape(-1)
+    on = model(nodes, theta, 0.05, x.T.reshape(-1), n, d, y, zc, m).into_online()
+    orc = O.Sgpr(nodes, params, x.T.reshape(-1), n, d, y, zc, m)
+    xs = rs.uniform(0, 1, size=(11, d)).T.reshape(-1)
+    kinds = []
+    for k in range(8):
+        zn = rs.uniform(0, 1, size=d) if k != 5 else z[2] + 1e-9  # a near duplicate sends it to the assembly
+        on.insert_inducing(zn)
+        orc.insert_inducing(zn)
+        z.append(zn)
+        assert on.last_step_in_place() == bool(orc.last_in_place), k
+        kinds.append(bool(orc.last_in_place))
+        assert O.rel_err(on.neg_log_marginal_likelihood(), orc.nlml()) <= TOL, k
+        nl, g = on.value_and_gradient(params)
+        assert O.rel_err(nl, orc.nlml()) <= TOL and np.all(O.rel_err(g, orc.grad()) <= TOL), k
+        p = on.predict(xs, 11, d)
+        mo, vo = orc.predict(xs, 11, 1)
+        assert np.all(O.rel_err(p.mean, mo) <= TOL) and np.all(O.rel_err(p.variance, vo) <= TOL), k
+    assert kinds[0] and not kinds[5]
+    assert on.m() == m + 8 and list(on.inducing_ids()) == list(range(m + 8))
