@@ -55,23 +55,32 @@ static __device__ __noinline__ int leaf16_factor(double* s, int off, double* rin
   for (int c = 0; c < 16; ++c) d[c] = (c <= r) ? s[(off + r) + (off + c) * FLS] : 0.0;
   int bad = -1;
   double my_inv = 1.0;
+  // the next pivot is formed first, by its own row from its own entry, so
+  // that the chain from one pivot to the next is a shuffle, the reciprocal
+  // square root, a product and an FMA; the other updates of the step overlap
+  // it (the values are those of the plain order, bit for bit)
+  double piv = __shfl_sync(0xffffffffu, d[0], 0);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    double piv = __shfl_sync(0xffffffffu, d[j], j);
     if (!(piv > 0.0) && bad < 0) bad = j;
-    double rs = rsqrt(fmax(piv, 1e-300));
+    const double rs = rsqrt(fmax(piv, 1e-300));
     if (r == j) {
       d[j] = piv * rs;
       my_inv = rs;
     } else if (r > j) {
       d[j] = d[j] * rs;
     }
+    if (j + 1 < 16) {
+      const double cand = (r == j + 1) ? fma(-d[j], d[j], d[j + 1]) : 0.0;
+      const double nxt = __shfl_sync(0xffffffffu, cand, j + 1);
 #pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      if (c > j) {
-        double lcj = __shfl_sync(0xffffffffu, d[j], c);
-        if (r >= c) d[c] = fma(-d[j], lcj, d[c]);
+      for (int c = 0; c < 16; ++c) {
+        if (c > j) {
+          const double lcj = __shfl_sync(0xffffffffu, d[j], c);
+          if (r >= c) d[c] = fma(-d[j], lcj, d[c]);
+        }
       }
+      piv = nxt;
     }
   }
   if (bad >= 0) return bad;
@@ -192,9 +201,20 @@ static __device__ int diag_block_factor_inv(double* A, long long lda, long long 
     }
   }
   if (fail >= 0) return fail;
-  // L back to global
-  for (int j = warp; j < nb; j += nw)
-    for (int i = j + lane; i < nb; i += 32) A[(k0 + i) + (k0 + j) * lda] = s[i + j * FLS];
+  // L back to global (16-byte stores from the first even row below the diagonal)
+  for (int j = warp; j < nb; j += nw) {
+    double* col = A + k0 + (k0 + j) * lda;
+    const double* sc = s + j * FLS;
+    if (vec) {
+      const int i0 = (j + 1) & ~1;
+      if ((j & 1) && lane == 0) col[j] = sc[j];
+      for (int i = i0 + 2 * lane; i + 1 < nb; i += 64)
+        *reinterpret_cast<double2*>(col + i) = *reinterpret_cast<const double2*>(sc + i);
+      if (((nb - i0) & 1) && lane == 0) col[nb - 1] = sc[nb - 1];
+    } else {
+      for (int i = j + lane; i < nb; i += 32) col[i] = sc[i];
+    }
+  }
   __syncthreads();
   // leaf inverses: lane q computes column q of L_pp⁻¹ by column-oriented
   // substitution, written over L_pp (its off-diagonal blocks stay L)
