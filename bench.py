@@ -254,7 +254,7 @@ def emu_kernel_roofline(n, peaks, traffic, int8_peak=None):
     from gprx_b200 import _lib as L
 
     h = n // 2
-    out = np.zeros(4)
+    out = np.zeros(5)
     st = L.lib().gprx_probe_emu_gemm(h, h, h, 7, 10, L.ptr(out))
     if st != 0 or out[0] <= 0:
         return None

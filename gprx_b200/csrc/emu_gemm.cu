@@ -213,6 +213,7 @@ struct EmuGemmArgs {
   int* err;
   int kz;              // > 0: blockIdx.z takes K chunks [z·kz, (z+1)·kz) into C + z·zstride
   long long zstride;
+  int nsm;             // SMs of the device (one resident CTA each): the size of a wave
 };
 
 template <int S>
@@ -255,6 +256,10 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
     kc1 = min(nkc, kc0 + g.kz);
   }
   const int nch = kc0 < kc1 ? kc1 - kc0 : 0;
+  // odd waves of CTAs walk K backwards: a wave then starts on the chunks the
+  // wave before it read last, which are still in L2 (the int32 sums are
+  // exact, so the order of the chunks does not change the result)
+  const bool rev = g.nsm > 0 && ((lid / g.nsm) & 1);
   double* const Cz = g.C + (long long)blockIdx.z * g.zstride;
 
   if (warp == 0) {
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
       if (c >= STAGES && !emu_wait(&empty[st], (uint32_t)(((c / STAGES) - 1) & 1), g.err)) break;
       uint8_t* base = smem + st * STAGE;
       expect_tx(&full[st], (uint32_t)STAGE);
-      const size_t off = (size_t)(kc0 + c) * 8192;
+      const size_t off = (size_t)(rev ? kc1 - 1 - c : kc0 + c) * 8192;
 #pragma unroll
       for (int p = 0; p < S; ++p) bulk_load(base + p * A_SL, Ab + p * planeA + off, A_SL, &full[st]);
 #pragma unroll
@@ -325,12 +330,19 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
     // every MMA done before the epilogue reads TMEM
     if (nch > 0 && ok) emu_wait(&empty[(nch - 1) % STAGES], (uint32_t)(((nch - 1) / STAGES) & 1), g.err);
   }
+  // epilogue: thread = output row.  With beta ≠ 0 the C values of a 16-column
+  // group are read all at once, one group ahead (the first group before the
+  // MMAs are waited for), so the memory latency is not paid per element.
+  const long long i = i0 + warp * 32 + lane;
+  const bool has_beta = g.beta != 0.0;
+  auto live = [&](long long j) { return i < g.M && j < g.N && !(g.lower && i + g.row0 < j + g.col0); };
+  double cv[16];
+#pragma unroll
+  for (int u = 0; u < 16; ++u) cv[u] = (has_beta && live(j0 + u)) ? Cz[i + (j0 + u) * g.ldc] : 0.0;
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-  // epilogue: thread = output row
-  const long long i = i0 + warp * 32 + lane;
   const int ea = i < g.M ? g.expA[i] : 0;
   const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
@@ -339,18 +351,25 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
 #pragma unroll
     for (int t = 0; t < S; ++t) tmem_ld16(trow + t * EMU_N + cb, v[t]);
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    double nx[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const long long j = j0 + cb + 16 + u;
+      nx[u] = (has_beta && cb + 16 < EMU_N && live(j)) ? Cz[i + j * g.ldc] : 0.0;
+    }
 #pragma unroll
     for (int u = 0; u < 16; ++u) {
       const long long j = j0 + cb + u;
-      if (i >= g.M || j >= g.N || (g.lower && i + g.row0 < j + g.col0)) continue;
+      if (!live(j)) continue;
       double acc = (double)(int)v[S - 1][u];
 #pragma unroll
       for (int t = S - 2; t >= 0; --t) acc = fma(acc, 0.0078125, (double)(int)v[t][u]);
       if (nch == 0) acc = 0.0;
       const double val = ldexp(acc, -(ea + g.expB[j]));
-      double* cp = Cz + i + j * g.ldc;
-      *cp = g.beta != 0.0 ? fma(g.alpha, val, g.beta * *cp) : g.alpha * val;
+      Cz[i + j * g.ldc] = has_beta ? fma(g.alpha, val, g.beta * cv[u]) : g.alpha * val;
     }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) cv[u] = nx[u];
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -359,6 +378,19 @@ __global__ void __launch_bounds__(EMU_THREADS, 1) emu_gemm_kernel(EmuGemmArgs g)
 
 size_t emu_gemm_smem(int S) {
   return (size_t)(S <= 6 ? 3 : 2) * S * (EMU_M + EMU_N) * EMU_KC;
+}
+
+// SM count of the current device (cached per device)
+static int emu_sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+  if (cached[dev] == 0) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    cached[dev] = v;
+  }
+  return cached[dev];
 }
 
 template <int S>
@@ -403,6 +435,7 @@ static EmuGemmArgs emu_args(const EmuOperand& A, const EmuOperand& B, double* C,
   g.err = err;
   g.kz = 0;
   g.zstride = 0;
+  g.nsm = emu_sm_count();
   return g;
 }
 

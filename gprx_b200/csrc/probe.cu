@@ -143,7 +143,7 @@ gprx_status gprx_probe_potrf(int32_t n, int32_t reps, double* ms_per_factor) {
 // FP64 DMMA product: out[0] ms per emulated GEMM, out[1] ms to slice both
 // operands, out[2] ms per DMMA GEMM, out[3] max |C − C_ref| / (|A|·|B|ᵀ).
 gprx_status gprx_probe_emu_gemm(int32_t m, int32_t n, int32_t k, int32_t S, int32_t reps, double* out) {
-  if (m <= 0 || n <= 0 || k <= 0 || reps <= 0 || !out || S < 4 || S > 7)
+  if (m <= 0 || n <= 0 || k <= 0 || reps <= 0 || !out || S < 4 || S > EMU_MAX_S)
     return set_error(GPRX_INVALID_ARGUMENT, "sizes");
   DevBuf<double> A, B, Aa, Ba, C, R, Cabs;
   DevBuf<int8_t> sa, sb;
@@ -182,13 +182,19 @@ gprx_status gprx_probe_emu_gemm(int32_t m, int32_t n, int32_t k, int32_t S, int3
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  float t_emu = 0.f, t_slice = 0.f, t_d = 0.f;
+  float t_emu = 0.f, t_slice = 0.f, t_d = 0.f, t_beta = 0.f;
   if (e == cudaSuccess) {
     cudaEventRecord(e0, s);
     for (int r = 0; r < reps && e == cudaSuccess; ++r) e = emu_gemm(a, b, C.p, m, 1.0, 0.0, false, 0, 0, 0, err.p, s);
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
     cudaEventElapsedTime(&t_emu, e0, e1);
+    // the update form C = C − A·Bᵀ (every C value read and written)
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = emu_gemm(a, b, C.p, m, -1.0, 1.0, false, 0, 0, 0, err.p, s);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&t_beta, e0, e1);
     cudaEventRecord(e0, s);
     for (int r = 0; r < reps && e == cudaSuccess; ++r) {
       e = emu_slice(A.p, m, false, a, s);
@@ -220,6 +226,7 @@ gprx_status gprx_probe_emu_gemm(int32_t m, int32_t n, int32_t k, int32_t S, int3
   double hd;
   std::memcpy(&hd, &hm, sizeof(hd));
   out[3] = hd;
+  out[4] = t_beta / reps;
   return GPRX_OK;
 }
 

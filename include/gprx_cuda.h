@@ -582,9 +582,11 @@ gprx_status gprx_probe_dgemm(int32_t m, int32_t n, int32_t k, int32_t trans_a, i
                              double* ms_per_launch);
 /* ms per blocked Cholesky factor of an n×n SPD matrix. */
 gprx_status gprx_probe_potrf(int32_t n, int32_t reps, double* ms_per_factor);
-/* int8-sliced FP64 product A·Bᵀ (S slices) against the DMMA product on
+/* int8-sliced FP64 product A·Bᵀ (S slices, 4..8) against the DMMA product on
  * random operands: out[0] ms per emulated GEMM, out[1] ms slicing both
- * operands, out[2] ms per DMMA GEMM, out[3] max |C − C_ref| / (|A|·|B|ᵀ). */
+ * operands, out[2] ms per DMMA GEMM, out[3] max |C − C_ref| / (|A|·|B|ᵀ),
+ * out[4] ms per emulated update C −= A·Bᵀ (C read and written).  out holds
+ * 5 doubles. */
 gprx_status gprx_probe_emu_gemm(int32_t m, int32_t n, int32_t k, int32_t S, int32_t reps, double* out);
 
 /* ------------------------------------------------------------------ */
