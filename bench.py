@@ -465,6 +465,8 @@ def batched_measure(torch, dev, count=BATCH_P, single_sample=32, cpu_sample=48, 
                    "kernel": "RbfKernel(1.0) + PeriodicKernel(1.0, p), p ~ U[10, 20]", "noise_variance": 0.1,
                    "tolerance": 1e-6},
         "status_ok": int((res.status == 0).sum()), "converged": int(res.converged.sum()),
+        "converged_share": float(res.converged.mean()),
+        "grad_norm_median": float(np.median(res.grad_norm)),
         "evaluations_mean": evals_per_fit, "evaluations_max": int(res.evaluations.max()),
         "gpu_launches": launches,
         "e2e": {"value": count / e2e_s, "unit": "fits/s", "h2d_bytes_per_step": bytes_in,
@@ -983,7 +985,8 @@ def main():
                                 "grad_norm", "predict_err_vs_oracle"))
         line["c1"]["cpu"] = c1["cpu_baseline"]["value"]
         bt = batched_measure(torch, dev, args.batch_problems, fp64_peak=fp64_peak)
-        line["batched"] = brief(bt, ("value", "unit", "speedup_vs_one_model_per_launch", "status_ok", "converged"))
+        line["batched"] = brief(bt, ("value", "unit", "speedup_vs_one_model_per_launch", "status_ok", "converged",
+                                     "converged_share", "grad_norm_median"))
         line["batched"].update({"e2e": bt["e2e"]["value"], "one_model_per_launch": bt["one_model_per_launch"]["value"],
                                 "round_ms": bt["roofline"]["round_ms"], "frac_of_dgemm": bt["roofline"]["frac"],
                                 "cpu": bt["cpu_baseline"]["value"]})
