@@ -125,10 +125,11 @@ __device__ inline Work work_of(double* base, int nmax) {
 // fill and gradient over 64×64 lower tiles
 // ---------------------------------------------------------------------------
 constexpr int FT_B = 64;
-// pairs one thread evaluates together (ARD trees take fewer: registers)
-template <int ARD_D>
+// pairs one thread evaluates together: more independent FP64 chains where
+// the tree's leaves (NL at most) and ARD differences leave registers for them
+template <int ARD_D, int NL>
 constexpr int pairs_w() {
-  return ARD_D == 0 ? 4 : ARD_D <= 8 ? 2 : 1;
+  return ARD_D == 0 ? (NL <= 2 ? 8 : 4) : ARD_D <= 8 ? 2 : 1;
 }
 
 template <int ARD_D>
@@ -155,7 +156,8 @@ __device__ inline void stage_points(const double* x, int n, int d, int i0, int j
 }
 
 // lower K + diag_add I into A (ld); returns true when every value is finite
-template <int ARD_D>
+// (trees of at most NL leaves)
+template <int ARD_D, int NL>
 __device__ bool cta_fill_lower(const KTree& t, const double* x, int n, double* A, long long ld, double diag_add,
                                double* smem, int* flag_sh) {
   double* xi = smem;
@@ -172,7 +174,7 @@ __device__ bool cta_fill_lower(const KTree& t, const double* x, int n, double* A
       __syncthreads();
       const int r = tid % FT_B, i = i0 + r;
       constexpr int CS = BT / FT_B;  // column stride of one thread
-      constexpr int PW = pairs_w<ARD_D>();
+      constexpr int PW = pairs_w<ARD_D, NL>();
 #pragma unroll 1
       for (int k0 = 0; k0 < FT_B / CS; k0 += PW) {
         const int cb = tid / FT_B + k0 * CS;
@@ -180,7 +182,7 @@ __device__ bool cta_fill_lower(const KTree& t, const double* x, int n, double* A
         double dx[PW][ARD_D > 0 ? ARD_D : 1], r2[PW], kv[PW];
 #pragma unroll
         for (int w = 0; w < PW; ++w) r2[w] = pair_dx<ARD_D>(xi + r, xj + cb + w * CS, d, dx[w]);
-        kt_value_w<ARD_D, PW>(t, dx, r2, kv);
+        kt_value_w<ARD_D, PW, NL>(t, dx, r2, kv);
 #pragma unroll
         for (int w = 0; w < PW; ++w) {
           const int j = j0 + cb + w * CS;
@@ -200,8 +202,9 @@ __device__ bool cta_fill_lower(const KTree& t, const double* x, int n, double* A
 }
 
 // Slot sums of Σ_{i≥j} c_ij W_ij ∂K_ij/∂θ (c = 1 on the diagonal, 2 off it),
-// W = ααᵀ − K⁻¹ (K⁻¹ lower in kinv), and Σ W_ii in the last slot.
-template <int ARD_D>
+// W = ααᵀ − K⁻¹ (K⁻¹ lower in kinv), and Σ W_ii in the last slot (trees of
+// at most NL leaves; the slots of absent leaves are zero).
+template <int ARD_D, int NL>
 __device__ void cta_grad(const KTree& t, const double* x, int n, const double* kinv, long long ld,
                          const double* alpha, double* smem, double* slots) {
   constexpr int AD = ARD_D > 0 ? ARD_D : 1;
@@ -212,11 +215,11 @@ __device__ void cta_grad(const KTree& t, const double* x, int n, const double* k
   double* aj = ai + FT_B;
   double* red = aj + FT_B;  // (BT / 32) × NS
   const int d = t.d, tid = threadIdx.x;
-  double acc_leaf[KT_MAX_LEAVES][KT_ACC_PER_LEAF];
+  double acc_leaf[NL][KT_ACC_PER_LEAF];
   double acc_ard[AD];
   double acc_noise = 0.0;
 #pragma unroll
-  for (int l = 0; l < KT_MAX_LEAVES; ++l) acc_leaf[l][0] = acc_leaf[l][1] = 0.0;
+  for (int l = 0; l < NL; ++l) acc_leaf[l][0] = acc_leaf[l][1] = 0.0;
 #pragma unroll
   for (int f = 0; f < AD; ++f) acc_ard[f] = 0.0;
   const int nt = (n + FT_B - 1) / FT_B;
@@ -232,7 +235,7 @@ __device__ void cta_grad(const KTree& t, const double* x, int n, const double* k
       __syncthreads();
       const int r = tid % FT_B, i = i0 + r;
       constexpr int CS = BT / FT_B;
-      constexpr int PW = pairs_w<ARD_D>();
+      constexpr int PW = pairs_w<ARD_D, NL>();
 #pragma unroll 1
       for (int k0 = 0; k0 < FT_B / CS; k0 += PW) {
         const int cb = tid / FT_B + k0 * CS;
@@ -250,7 +253,7 @@ __device__ void cta_grad(const KTree& t, const double* x, int n, const double* k
           }
           wt[w] = wv;
         }
-        kt_accumulate_grad_w<ARD_D, PW>(t, dx, r2, wt, acc_leaf, acc_ard);
+        kt_accumulate_grad_w<ARD_D, PW, NL>(t, dx, r2, wt, acc_leaf, acc_ard);
       }
     }
   const int lane = tid & 31, warp = tid >> 5;
@@ -258,7 +261,7 @@ __device__ void cta_grad(const KTree& t, const double* x, int n, const double* k
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     double v;
-    if (s < GRAD_SLOTS_LEAF) v = acc_leaf[s / KT_ACC_PER_LEAF][s % KT_ACC_PER_LEAF];
+    if (s < GRAD_SLOTS_LEAF) v = (s / KT_ACC_PER_LEAF < NL) ? acc_leaf[s / KT_ACC_PER_LEAF][s % KT_ACC_PER_LEAF] : 0.0;
     else if (s < GRAD_SLOTS_LEAF + AD) v = acc_ard[s - GRAD_SLOTS_LEAF];
     else v = acc_noise;
     v = warp_sum(v);
@@ -271,6 +274,21 @@ __device__ void cta_grad(const KTree& t, const double* x, int n, const double* k
     slots[s] = v;
   }
   __syncthreads();
+}
+
+// the two passes with the leaf bound of the problem's tree (isotropic trees
+// of at most two leaves have their own, wider form)
+template <int ARD_D>
+__device__ bool cta_fill_any(const KTree& t, const double* x, int n, double* A, long long ld, double diag_add,
+                             double* smem, int* flag_sh) {
+  if (ARD_D == 0 && t.n_leaves <= 2) return cta_fill_lower<ARD_D, 2>(t, x, n, A, ld, diag_add, smem, flag_sh);
+  return cta_fill_lower<ARD_D, KT_MAX_LEAVES>(t, x, n, A, ld, diag_add, smem, flag_sh);
+}
+template <int ARD_D>
+__device__ void cta_grad_any(const KTree& t, const double* x, int n, const double* kinv, long long ld,
+                             const double* alpha, double* smem, double* slots) {
+  if (ARD_D == 0 && t.n_leaves <= 2) cta_grad<ARD_D, 2>(t, x, n, kinv, ld, alpha, smem, slots);
+  else cta_grad<ARD_D, KT_MAX_LEAVES>(t, x, n, kinv, ld, alpha, smem, slots);
 }
 
 // ---------------------------------------------------------------------------
@@ -353,7 +371,7 @@ __device__ void cta_eval(const BatchEvalArgs& a, int q, const Work& w, double* s
   int fail = 0;
   for (int attempt = 0; attempt <= a.jit.count; ++attempt) {
     const double j = attempt == 0 ? 0.0 : a.jit.j[attempt - 1];
-    if (!cta_fill_lower<ARD_D>(tree, P.x, n, w.A, ld, noise + j, smem, &flag_sh)) {
+    if (!cta_fill_any<ARD_D>(tree, P.x, n, w.A, ld, noise + j, smem, &flag_sh)) {
       if (tid == 0) a.status[q] = GPRX_NONFINITE_KERNEL;
       return;
     }
@@ -390,7 +408,7 @@ __device__ void cta_eval(const BatchEvalArgs& a, int q, const Work& w, double* s
   const double quad = block_sum(acc, red);
   // K⁻¹ = Xᵀ X (lower) over L in A
   cta_gemm<true, false>(cfg, n, n, n, w.X, ld, w.X, ld, w.A, ld, 1.0, 0.0, true, CG_FROM_ROW, smem);
-  cta_grad<ARD_D>(tree, P.x, n, w.A, ld, w.alpha, smem, slots);
+  cta_grad_any<ARD_D>(tree, P.x, n, w.A, ld, w.alpha, smem, slots);
   if (tid == 0) {
     constexpr int NS = GRAD_SLOTS_LEAF + (ARD_D > 0 ? ARD_D : 1) + 1;
     const double nl = 0.5 * (quad + logdet + (double)n * log(2.0 * M_PI));

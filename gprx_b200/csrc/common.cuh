@@ -137,9 +137,10 @@ GPRX_HD inline int kt_set_theta(KTree& t, const double* th) {
 // the batched path).  W = 1 is the single-pair form of the large kernels.
 
 // Leaf values at W pairs.  dx[w][f] = x1_f − x2_f of pair w, r2[w] = |dx|².
-template <int ARD_D, int W>
+// NL bounds the leaves a caller's trees have (registers scale with it).
+template <int ARD_D, int W, int NL = KT_MAX_LEAVES>
 __device__ __forceinline__ void kt_leaf_values_w(const KTree& t, const double (&dx)[W][ARD_D > 0 ? ARD_D : 1],
-                                                 const double (&r2)[W], double (&v)[KT_MAX_LEAVES][W]) {
+                                                 const double (&r2)[W], double (&v)[NL][W]) {
   double ard_q[W];
 #pragma unroll
   for (int w = 0; w < W; ++w) {
@@ -151,7 +152,7 @@ __device__ __forceinline__ void kt_leaf_values_w(const KTree& t, const double (&
     }
   }
 #pragma unroll
-  for (int l = 0; l < KT_MAX_LEAVES; ++l) {
+  for (int l = 0; l < NL; ++l) {
     if (l >= t.n_leaves) {
 #pragma unroll
       for (int w = 0; w < W; ++w) v[l][w] = 0.0;
@@ -186,8 +187,8 @@ __device__ __forceinline__ void kt_leaf_values_w(const KTree& t, const double (&
   }
 }
 
-template <int W>
-__device__ __forceinline__ void kt_combine_w(const KTree& t, const double (&v)[KT_MAX_LEAVES][W], double (&k)[W]) {
+template <int W, int NL = KT_MAX_LEAVES>
+__device__ __forceinline__ void kt_combine_w(const KTree& t, const double (&v)[NL][W], double (&k)[W]) {
 #pragma unroll
   for (int w = 0; w < W; ++w) k[w] = 0.0;
 #pragma unroll
@@ -198,7 +199,7 @@ __device__ __forceinline__ void kt_combine_w(const KTree& t, const double (&v)[K
 #pragma unroll
     for (int w = 0; w < W; ++w) p[w] = 1.0;
 #pragma unroll
-    for (int l = 0; l < KT_MAX_LEAVES; ++l)
+    for (int l = 0; l < NL; ++l)
       if ((mask >> l) & 1u) {
 #pragma unroll
         for (int w = 0; w < W; ++w) p[w] *= v[l][w];
@@ -209,12 +210,12 @@ __device__ __forceinline__ void kt_combine_w(const KTree& t, const double (&v)[K
 }
 
 // k(x1, x2) at W pairs.
-template <int ARD_D, int W>
+template <int ARD_D, int W, int NL = KT_MAX_LEAVES>
 __device__ __forceinline__ void kt_value_w(const KTree& t, const double (&dx)[W][ARD_D > 0 ? ARD_D : 1],
                                            const double (&r2)[W], double (&k)[W]) {
-  double v[KT_MAX_LEAVES][W];
-  kt_leaf_values_w<ARD_D, W>(t, dx, r2, v);
-  kt_combine_w<W>(t, v, k);
+  double v[NL][W];
+  kt_leaf_values_w<ARD_D, W, NL>(t, dx, r2, v);
+  kt_combine_w<W, NL>(t, v, k);
 }
 
 // k(x1, x2) at one pair.
@@ -234,16 +235,16 @@ __device__ __forceinline__ double kt_value(const KTree& t, const double* dx, dou
 // and per-dim ARD slots (acc_ard[f]); the host maps slots to θ indices.  A Sum
 // gives each term the same weight; a Product gives a factor the weight times
 // the other factors (src/kernel/compiled/weighted.rs:274-345).
-template <int ARD_D, int W>
+template <int ARD_D, int W, int NL = KT_MAX_LEAVES>
 __device__ __forceinline__ void kt_accumulate_grad_w(const KTree& t, const double (&dx)[W][ARD_D > 0 ? ARD_D : 1],
                                                      const double (&r2)[W], const double (&wt)[W],
-                                                     double (&acc_leaf)[KT_MAX_LEAVES][KT_ACC_PER_LEAF],
+                                                     double (&acc_leaf)[NL][KT_ACC_PER_LEAF],
                                                      double (&acc_ard)[ARD_D > 0 ? ARD_D : 1]) {
-  double v[KT_MAX_LEAVES][W];
-  kt_leaf_values_w<ARD_D, W>(t, dx, r2, v);
-  double adj[KT_MAX_LEAVES][W];
+  double v[NL][W];
+  kt_leaf_values_w<ARD_D, W, NL>(t, dx, r2, v);
+  double adj[NL][W];
 #pragma unroll
-  for (int l = 0; l < KT_MAX_LEAVES; ++l)
+  for (int l = 0; l < NL; ++l)
 #pragma unroll
     for (int w = 0; w < W; ++w) adj[l][w] = 0.0;
 #pragma unroll
@@ -251,13 +252,13 @@ __device__ __forceinline__ void kt_accumulate_grad_w(const KTree& t, const doubl
     if (tt >= t.n_terms) break;
     const unsigned mask = t.term_mask[tt];
 #pragma unroll
-    for (int l = 0; l < KT_MAX_LEAVES; ++l) {
+    for (int l = 0; l < NL; ++l) {
       if (!((mask >> l) & 1u)) continue;
       double others[W];
 #pragma unroll
       for (int w = 0; w < W; ++w) others[w] = 1.0;
 #pragma unroll
-      for (int o = 0; o < KT_MAX_LEAVES; ++o)
+      for (int o = 0; o < NL; ++o)
         if (o != l && ((mask >> o) & 1u)) {
 #pragma unroll
           for (int w = 0; w < W; ++w) others[w] *= v[o][w];
@@ -267,7 +268,7 @@ __device__ __forceinline__ void kt_accumulate_grad_w(const KTree& t, const doubl
     }
   }
 #pragma unroll
-  for (int l = 0; l < KT_MAX_LEAVES; ++l) {
+  for (int l = 0; l < NL; ++l) {
     if (l >= t.n_leaves) break;
     const KLeaf& lf = t.leaf[l];
     switch (lf.kind) {
