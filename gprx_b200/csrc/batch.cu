@@ -94,7 +94,7 @@ struct BatchEvalArgs {
   int slot_param[64];
 };
 
-constexpr int BT = FD_THREADS;  // 256 threads: 8 warps
+constexpr int BT = 512;  // 16 warps: one CTA per SM holds a problem, so the warps hide the FP64 latencies
 static_assert(BT == CG_THREADS, "the diagonal step and the CTA GEMM share the block");
 
 __host__ __device__ inline long long batch_ld(int n) { return ((long long)n + 7) / 8 * 8; }
@@ -129,7 +129,7 @@ constexpr int FT_B = 64;
 // the tree's leaves (NL at most) and ARD differences leave registers for them
 template <int ARD_D, int NL>
 constexpr int pairs_w() {
-  return ARD_D == 0 ? (NL <= 2 ? 8 : 4) : ARD_D <= 8 ? 2 : 1;
+  return ARD_D == 0 ? (NL <= 2 ? 4 : 2) : 1;
 }
 
 template <int ARD_D>

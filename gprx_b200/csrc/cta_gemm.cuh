@@ -1,4 +1,4 @@
-// cta_gemm.cuh — FP64 GEMM run by ONE CTA of 256 threads over all output
+// cta_gemm.cuh — FP64 GEMM run by ONE CTA of 512 threads over all output
 // tiles of a small matrix product: the building block of the batched
 // per-problem evaluation, where each CTA owns a whole problem.
 //
@@ -6,9 +6,10 @@
 //   opA(i,k) = TA ? A[k + i·lda] : A[i + k·lda]
 //   opB(k,j) = TB ? B[j + k·ldb] : B[k + j·ldb]
 //
-// Output tiles are TM×TN (8 warps in a 2×4 grid of (TM/2)×(TN/4) DMMA
-// m16n8k4 blocks); the shapes the autotuner picks from are listed in
-// CgTile below.  The k chunks (TK deep) of ALL tiles form one stream through
+// Output tiles are TM×TN, 16 warps in a WGM×WGN grid of (TM/WGM)×(TN/WGN)
+// DMMA m16n8k4 blocks (32×32 tiles keep eight warps busy and let the other
+// eight load); the shapes the autotuner picks from are listed in CgTile
+// below.  The k chunks (TK deep) of ALL tiles form one stream through
 // a 3-stage cp.async ring, so the next tile's first chunks load while the
 // current tile computes, and the C values a tile needs (beta ≠ 0) are fetched
 // into registers when the tile starts.  Shared-memory layouts follow each
@@ -31,18 +32,18 @@
 
 namespace gprx {
 
-constexpr int CG_THREADS = 256;
+constexpr int CG_THREADS = 512;
 constexpr int CG_STAGES = 3;
 constexpr int CG_FULL = 0, CG_FROM_ROW = 1, CG_FROM_COL = 2;
 
-// tile shapes (TM × TN, k chunk TK) by configuration index
+// tile shapes (TM × TN, k chunk TK, warp grid WGM × WGN) by configuration index
 constexpr int CG_CONFIGS = 4;
 template <int CFG>
 struct CgTile;
-template <> struct CgTile<0> { static constexpr int M = 64, N = 128, K = 32; };
-template <> struct CgTile<1> { static constexpr int M = 64, N = 64, K = 32; };
-template <> struct CgTile<2> { static constexpr int M = 32, N = 64, K = 32; };
-template <> struct CgTile<3> { static constexpr int M = 32, N = 32, K = 16; };
+template <> struct CgTile<0> { static constexpr int M = 64, N = 128, K = 32, WGM = 4, WGN = 4; };
+template <> struct CgTile<1> { static constexpr int M = 64, N = 64, K = 32, WGM = 4, WGN = 4; };
+template <> struct CgTile<2> { static constexpr int M = 32, N = 64, K = 32, WGM = 2, WGN = 8; };
+template <> struct CgTile<3> { static constexpr int M = 32, N = 32, K = 16, WGM = 2, WGN = 4; };
 __host__ __device__ constexpr int cg_tile_n(int cfg) { return cfg == 0 ? 128 : cfg == 3 ? 32 : 64; }
 __host__ __device__ constexpr int cg_tile_m(int cfg) { return cfg <= 1 ? 64 : 32; }
 
@@ -85,12 +86,15 @@ template <bool TA, bool TB, int CFG>
 __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
                          double* C, long long ldc, double alpha, double beta, bool lower, int kmode, double* smem) {
   constexpr int CG_M = CgTile<CFG>::M, CG_N = CgTile<CFG>::N, CG_K = CgTile<CFG>::K;
-  constexpr int WM = CG_M / 2, WN = CG_N / 4, MI = WM / 16, NJ = WN / 8;
+  constexpr int WGM = CgTile<CFG>::WGM, WGN = CgTile<CFG>::WGN;
+  constexpr int WM = CG_M / WGM, WN = CG_N / WGN, MI = WM / 16, NJ = WN / 8;
+  static_assert(WGM * WGN <= CG_THREADS / 32 && MI >= 1 && NJ >= 1, "warp grid");
   using SA = CgA<TA, CG_M, CG_K>;
   using SB = CgB<TB, CG_N, CG_K>;
   constexpr int STAGE = SA::ELEMS + SB::ELEMS;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
-  const int wm = warp & 1, wn = warp >> 1;
+  const int wm = warp % WGM, wn = warp / WGM;
+  const bool wact = warp < WGM * WGN;  // warps past the grid only load
   const int tm_n = (M + CG_M - 1) / CG_M, tn_n = (N + CG_N - 1) / CG_N;
   const int ntiles = tm_n * tn_n;
   // 16-byte copies need even leading dimensions and 16-byte aligned bases
@@ -125,9 +129,7 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
       double* sB = sA + SA::ELEMS;
       // A chunk
       if (a16) {
-#pragma unroll
-        for (int it = 0; it < CG_M * CG_K / 2 / CG_THREADS; ++it) {
-          const int e = tid + it * CG_THREADS;
+        for (int e = tid; e < CG_M * CG_K / 2; e += CG_THREADS) {
           int i, k, bytes;
           const double* src;
           if (TA) {  // pairs along k
@@ -146,9 +148,7 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
           cp_async16(sA + SA::at(i, k), src, bytes);
         }
       } else {
-#pragma unroll 4
-        for (int it = 0; it < CG_M * CG_K / CG_THREADS; ++it) {
-          const int e = tid + it * CG_THREADS;
+        for (int e = tid; e < CG_M * CG_K; e += CG_THREADS) {
           int i, k;
           if (TA) { k = e % CG_K; i = e / CG_K; } else { i = e % CG_M; k = e / CG_M; }
           const int gi = m0 + i, gk = k0 + k;
@@ -159,9 +159,7 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
       }
       // B chunk
       if (b16) {
-#pragma unroll
-        for (int it = 0; it < CG_K * CG_N / 2 / CG_THREADS; ++it) {
-          const int e = tid + it * CG_THREADS;
+        for (int e = tid; e < CG_K * CG_N / 2; e += CG_THREADS) {
           int j, k, bytes;
           const double* src;
           if (TB) {  // pairs along j
@@ -180,9 +178,7 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
           cp_async16(sB + SB::at(k, j), src, bytes);
         }
       } else {
-#pragma unroll 4
-        for (int it = 0; it < CG_K * CG_N / CG_THREADS; ++it) {
-          const int e = tid + it * CG_THREADS;
+        for (int e = tid; e < CG_K * CG_N; e += CG_THREADS) {
           int k, j;
           if (TB) { j = e % CG_N; k = e / CG_N; } else { k = e % CG_K; j = e / CG_K; }
           const int gj = n0 + j, gk = k0 + k;
@@ -206,7 +202,7 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
   for (int ct = next_used(0); ct < ntiles; ct = next_used(ct + 1)) {
     const int m0 = (ct % tm_n) * CG_M, n0 = (ct / tm_n) * CG_N;
     const int nch = tile_nch(ct);
-    const bool wskip = lower && (m0 + wm * WM + WM - 1 < n0 + wn * WN);
+    const bool wskip = !wact || (lower && (m0 + wm * WM + WM - 1 < n0 + wn * WN));
     // C of this tile into registers now; consumed after the k loop
     double cv[MI][NJ][4];
 #pragma unroll
@@ -217,7 +213,7 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
         for (int r = 0; r < 4; ++r) {
           const int row = m0 + wm * WM + mi * 16 + g + ((r & 2) ? 8 : 0);
           const int col = n0 + wn * WN + nj * 8 + 2 * t4 + (r & 1);
-          const bool ok = beta != 0.0 && row < M && col < N && !(lower && row < col);
+          const bool ok = wact && beta != 0.0 && row < M && col < N && !(lower && row < col);
           cv[mi][nj][r] = ok ? C[row + (long long)col * ldc] : 0.0;
         }
     double acc[MI][NJ][4];
@@ -259,7 +255,7 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
         for (int r = 0; r < 4; ++r) {
           const int row = m0 + wm * WM + mi * 16 + g + ((r & 2) ? 8 : 0);
           const int col = n0 + wn * WN + nj * 8 + 2 * t4 + (r & 1);
-          if (row < M && col < N && !(lower && row < col)) {
+          if (wact && row < M && col < N && !(lower && row < col)) {
             double v = alpha * acc[mi][nj][r];
             if (beta != 0.0) v = fma(beta, cv[mi][nj][r], v);
             C[row + (long long)col * ldc] = v;
