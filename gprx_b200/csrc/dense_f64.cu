@@ -204,10 +204,15 @@ static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double
   return cudaGetLastError();
 }
 
-// CTAs of the bulk trailing update in the look-ahead factor (of 148 SMs).
-// A split that gave the chain more SMs when the bulk update is small was
-// measured and was slower (mixed n = 8192: 16.5 against 15.9 ms).
+// CTAs of the bulk trailing update in the look-ahead factor (of 148 SMs)
+// once its trailing block has at most BULK_CAP_ROWS rows; a larger block is
+// the slower side of a step and takes every SM.  Measured (FP64 factor
+// probe): n = 4096 3.07 ms with the cap against 3.14 without; n = 8192
+// 12.95 with the cap at every step against 12.37 without.  A split that
+// gave the chain more SMs when the bulk update is small was slower too
+// (mixed n = 8192: 16.5 against 15.9 ms).
 constexpr int BULK_CTAS = 132;
+constexpr int BULK_CAP_ROWS = 4096;
 
 cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatus* st, cudaStream_t s,
                           FactorCtx* ctx) {
@@ -260,7 +265,7 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
       const double* Pk2 = A + c2 + (long long)k0 * ld;
       GemmParams ps = gemm_params(m, m, NB, Pk2, ld, Pk2, ld, A + c2 + (long long)c2 * ld, ld, -1.0, 1.0, st);
       ps.mode = GEMM_LOWER_TILES;
-      ps.max_ctas = BULK_CTAS;  // leave SMs free for the side stream's chain
+      ps.max_ctas = m <= BULK_CAP_ROWS ? BULK_CTAS : 0;  // leave SMs free for the side stream's chain
       CK(dgemm(false, true, ps, s));
     }
     CK(cudaEventRecord(Es[k], s));
