@@ -31,11 +31,6 @@ cudaError_t dgemm_nn_fill(const GemmParams& p, cudaStream_t s, int batch) {
   return launch_dgemm<64, 64, 16, 32, 16, 3, false, false>(p, batch, s);
 }
 
-cudaError_t dgemm_nt_small(const GemmParams& p, cudaStream_t s, int tile) {
-  if (tile == 1) return launch_dgemm<64, 128, 16, 32, 32, 3, false, true>(p, 1, s);
-  return launch_dgemm<64, 64, 16, 32, 16, 3, false, true>(p, 1, s);
-}
-
 GemmParams gemm_params(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
                        double* C, long long ldc, double alpha, double beta, const DevStatus* st) {
   GemmParams p{};
@@ -188,6 +183,136 @@ cudaError_t FactorCtx::ensure(int nblk) {
   return cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// the chain's panel products: K ≤ NB, N ≤ NB
+// ---------------------------------------------------------------------------
+// C(M×N) = alpha · A(M×K) · B(N×K)ᵀ + beta · C with A(i,k) = A[i + k·lda],
+// B(j,k) = B[j + k·ldb], C column-major; lower: only i ≥ j is written.  One
+// CTA of 256 threads per PG_TM-row strip stages the strip of A and all of B
+// in shared memory in one go (K is one panel: no k pipeline, one memory
+// latency instead of one per k chunk), prefetches its C values meanwhile,
+// then runs the DMMA k steps.  A strip is read whole before it is written,
+// so C may be A's rows when beta = 0 (the in-place panel solve).
+constexpr int PG_TM = 32;
+constexpr int PG_LDA = PG_TM + 4;  // ≡ 4 mod 16 doubles: conflict-free fragments
+constexpr int PG_LDB = NB + 4;
+inline size_t panel_gemm_smem() { return (size_t)(NB * PG_LDA + NB * PG_LDB) * sizeof(double); }
+
+struct PanelGemmArgs {
+  int M, N, K;
+  const double* A;
+  long long lda;
+  const double* B;
+  long long ldb;
+  double* C;
+  long long ldc;
+  double alpha, beta;
+  int lower;
+  const DevStatus* st;
+};
+
+__global__ void __launch_bounds__(256) panel_gemm_kernel(PanelGemmArgs g) {
+  extern __shared__ __align__(16) double smem[];
+  if (dev_failed(g.st)) return;
+  double* sA = smem;                 // [k][i], ld PG_LDA
+  double* sB = smem + NB * PG_LDA;   // [k][j], ld PG_LDB
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gq = lane >> 2, t4 = lane & 3;
+  const int m0 = blockIdx.x * PG_TM;
+  const int KP = (g.K + 3) & ~3;
+  const bool a16 = ((g.lda & 1) == 0) && ((reinterpret_cast<unsigned long long>(g.A) & 15) == 0);
+  const bool b16 = ((g.ldb & 1) == 0) && ((reinterpret_cast<unsigned long long>(g.B) & 15) == 0);
+  // A strip: PG_TM × KP (zero past M and K)
+  if (a16) {
+    for (int e = tid; e < (PG_TM / 2) * KP; e += 256) {
+      const int i = 2 * (e % (PG_TM / 2)), k = e / (PG_TM / 2), gi = m0 + i;
+      const int bytes = (gi < g.M && k < g.K) ? (gi + 1 < g.M ? 16 : 8) : 0;
+      const unsigned d = (unsigned)__cvta_generic_to_shared(sA + k * PG_LDA + i);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d),
+                   "l"(bytes ? g.A + gi + (long long)k * g.lda : g.A), "r"(bytes));
+    }
+  } else {
+    for (int e = tid; e < PG_TM * KP; e += 256) {
+      const int i = e % PG_TM, k = e / PG_TM, gi = m0 + i;
+      const bool ok = gi < g.M && k < g.K;
+      cp_async8(sA + k * PG_LDA + i, ok ? g.A + gi + (long long)k * g.lda : g.A, ok);
+    }
+  }
+  // B: NB × KP (zero past N and K)
+  if (b16) {
+    for (int e = tid; e < (NB / 2) * KP; e += 256) {
+      const int j = 2 * (e % (NB / 2)), k = e / (NB / 2);
+      const int bytes = (j < g.N && k < g.K) ? (j + 1 < g.N ? 16 : 8) : 0;
+      const unsigned d = (unsigned)__cvta_generic_to_shared(sB + k * PG_LDB + j);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d),
+                   "l"(bytes ? g.B + j + (long long)k * g.ldb : g.B), "r"(bytes));
+    }
+  } else {
+    for (int e = tid; e < NB * KP; e += 256) {
+      const int j = e % NB, k = e / NB;
+      const bool ok = j < g.N && k < g.K;
+      cp_async8(sB + k * PG_LDB + j, ok ? g.B + j + (long long)k * g.ldb : g.B, ok);
+    }
+  }
+  cp_async_commit();
+  // warps in a 2 × 4 grid of 16 × 32 blocks (MI = 1, NJ = 4)
+  const int wm = warp & 1, wn = warp >> 1;
+  const int rb = wm * 16, cb = wn * 32;
+  const bool wskip = (cb >= g.N) || (g.lower && m0 + rb + 15 < cb);
+  double cv[4][4];
+#pragma unroll
+  for (int nj = 0; nj < 4; ++nj)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int row = m0 + rb + gq + ((r & 2) ? 8 : 0), col = cb + nj * 8 + 2 * t4 + (r & 1);
+      const bool ok = !wskip && g.beta != 0.0 && row < g.M && col < g.N && !(g.lower && row < col);
+      cv[nj][r] = ok ? g.C[row + (long long)col * g.ldc] : 0.0;
+    }
+  cp_async_wait<0>();
+  __syncthreads();
+  if (wskip) return;
+  double acc[4][4];
+#pragma unroll
+  for (int nj = 0; nj < 4; ++nj)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) acc[nj][r] = 0.0;
+#pragma unroll 4
+  for (int kk = 0; kk < KP; kk += 4) {
+    const double a0 = sA[(kk + t4) * PG_LDA + rb + gq];
+    const double a1 = sA[(kk + t4) * PG_LDA + rb + gq + 8];
+    double b[4];
+#pragma unroll
+    for (int nj = 0; nj < 4; ++nj) b[nj] = sB[(kk + t4) * PG_LDB + cb + nj * 8 + gq];
+#pragma unroll
+    for (int nj = 0; nj < 4; ++nj) dmma_16x8x4(acc[nj], a0, a1, b[nj]);
+  }
+#pragma unroll
+  for (int nj = 0; nj < 4; ++nj)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int row = m0 + rb + gq + ((r & 2) ? 8 : 0), col = cb + nj * 8 + 2 * t4 + (r & 1);
+      if (row < g.M && col < g.N && !(g.lower && row < col)) {
+        double v = g.alpha * acc[nj][r];
+        if (g.beta != 0.0) v = fma(g.beta, cv[nj][r], v);
+        g.C[row + (long long)col * g.ldc] = v;
+      }
+    }
+}
+
+static cudaError_t panel_gemm(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
+                              double* C, long long ldc, double alpha, double beta, bool lower, const DevStatus* st,
+                              cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(panel_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_gemm_smem()));
+    attr = true;
+  }
+  if (M <= 0 || N <= 0) return cudaSuccess;
+  if (N > NB || K > NB || K < 0) return cudaErrorInvalidValue;
+  PanelGemmArgs g{M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, lower ? 1 : 0, st};
+  GPRX_LAUNCH(panel_gemm_kernel, ceil_div(M, PG_TM), 256, panel_gemm_smem(), s, g);
+  return cudaGetLastError();
+}
+
 static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double* linv, DevStatus* st,
                                   cudaStream_t s) {
   int nbk = min(NB, n - k0);
@@ -196,10 +321,9 @@ static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double
   int rest = n - k0 - nbk;
   if (rest > 0) {
     double* P = A + (k0 + nbk) + (long long)k0 * ld;
-    // panel: P := P · L_kk⁻ᵀ (in place; a 64×128 tile covers all nbk columns
-    // of its rows, and twice the CTAs of 128×128 tiles shorten the chain)
-    GemmParams pp = gemm_params(rest, nbk, nbk, P, ld, lk, NB, P, ld, 1.0, 0.0, st);
-    CK(dgemm_nt_small(pp, s, 1));
+    // panel: P := P · L_kk⁻ᵀ, i.e. P(i,j) = Σ_k P(i,k) L_kk⁻¹(j,k) (in place:
+    // a strip is staged whole before it is written)
+    CK(panel_gemm(rest, nbk, nbk, P, ld, lk, NB, P, ld, 1.0, 0.0, false, st, s));
   }
   return cudaGetLastError();
 }
@@ -249,10 +373,9 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
     // critical chain of block k+1 (side stream)
     if (k >= 1) CK(cudaStreamWaitEvent(X, Es[k - 1], 0));
     {
+      // column block k+1 −= panel k · (its top rows)ᵀ, lower part
       int m = n - c1, w = min(NB, n - c1);
-      GemmParams pc = gemm_params(m, w, NB, Pk, ld, Pk, ld, A + c1 + (long long)c1 * ld, ld, -1.0, 1.0, st);
-      pc.mode = GEMM_LOWER_TILES;
-      CK(dgemm_nt_small(pc, X, 2));  // 64×64 tiles: four times the CTAs on the chain
+      CK(panel_gemm(m, w, NB, Pk, ld, Pk, ld, A + c1 + (long long)c1 * ld, ld, -1.0, 1.0, true, st, X));
     }
     CK(diag_and_panel(A, ld, n, c1, linv, st, X));
     CK(cudaEventRecord(Ep[k + 1], X));

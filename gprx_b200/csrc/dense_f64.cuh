@@ -14,10 +14,6 @@ constexpr int NB = 128;
 
 // C = alpha·opA·opB + beta·C with the 128×128 DMMA tile (see gemm_f64.cuh).
 cudaError_t dgemm(bool ta, bool tb, const GemmParams& p, cudaStream_t s, int batch = 1);
-// A·Bᵀ with smaller output tiles, for the few-tile products on the factor's
-// critical chain: tile 1 = 64×128 (keeps a 128-wide N in one tile, so C may
-// alias A's rows), tile 2 = 64×64.
-cudaError_t dgemm_nt_small(const GemmParams& p, cudaStream_t s, int tile);
 // A·B (NN) with 64×64 tiles when 128×128 tiles would leave most SMs idle
 // (fewer than two waves); C must not alias A or B.
 cudaError_t dgemm_nn_fill(const GemmParams& p, cudaStream_t s, int batch);
