@@ -121,10 +121,21 @@ __device__ void blk_store_full(double* dst, int ldd, const double* s, int ls, in
   }
 }
 
+// Programmatic dependent launch on the factor's chain: a chain kernel first
+// waits for its predecessor in the stream to complete (its writes visible),
+// then lets its own dependent start launching, so the launch of the next
+// chain kernel overlaps this one instead of following its completion.  Both
+// instructions are no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void chain_dependency_wait_and_release() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __global__ void __launch_bounds__(FD_THREADS) potrf_diag_kernel(double* A, long long lda, long long k0, int nb,
                                                                  double* linv, DevStatus* st) {
   extern __shared__ __align__(16) double smem[];
   __shared__ int fail;
+  chain_dependency_wait_and_release();
   if (dev_failed(st)) return;
   int f = diag_block_factor_inv(A, lda, k0, nb, linv, smem, &fail);
   if (f >= 0 && threadIdx.x == 0) dev_fail(st, GPRX_CHOLESKY_FAILED, k0 + f);
@@ -213,6 +224,7 @@ struct PanelGemmArgs {
 
 __global__ void __launch_bounds__(256) panel_gemm_kernel(PanelGemmArgs g) {
   extern __shared__ __align__(16) double smem[];
+  chain_dependency_wait_and_release();
   if (dev_failed(g.st)) return;
   double* sA = smem;                 // [k][i], ld PG_LDA
   double* sB = smem + NB * PG_LDA;   // [k][j], ld PG_LDB
@@ -298,9 +310,28 @@ __global__ void __launch_bounds__(256) panel_gemm_kernel(PanelGemmArgs g) {
     }
 }
 
+// launch with programmatic stream serialization (the kernel waits for its
+// predecessor itself: chain_dependency_wait_and_release)
+template <typename... Params, typename... Args>
+static cudaError_t launch_chain(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  count_launch();
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 static cudaError_t panel_gemm(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
                               double* C, long long ldc, double alpha, double beta, bool lower, const DevStatus* st,
-                              cudaStream_t s) {
+                              cudaStream_t s, bool chained = false) {
   static bool attr = false;
   if (!attr) {
     CK(cudaFuncSetAttribute(panel_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)panel_gemm_smem()));
@@ -309,21 +340,34 @@ static cudaError_t panel_gemm(int M, int N, int K, const double* A, long long ld
   if (M <= 0 || N <= 0) return cudaSuccess;
   if (N > NB || K > NB || K < 0) return cudaErrorInvalidValue;
   PanelGemmArgs g{M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, lower ? 1 : 0, st};
+  if (chained) return launch_chain(panel_gemm_kernel, dim3(ceil_div(M, PG_TM)), dim3(256), panel_gemm_smem(), s, g);
   GPRX_LAUNCH(panel_gemm_kernel, ceil_div(M, PG_TM), 256, panel_gemm_smem(), s, g);
   return cudaGetLastError();
 }
+
+// rows below the diagonal block up to which the chain uses dependent launch
+// (the same bound as the bulk update's cap, BULK_CAP_ROWS)
+constexpr int CHAIN_PDL_ROWS = 4096;
 
 static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double* linv, DevStatus* st,
                                   cudaStream_t s) {
   int nbk = min(NB, n - k0);
   double* lk = linv + (long long)(k0 / NB) * NB * NB;
-  GPRX_LAUNCH(potrf_diag_kernel, 1, FD_THREADS, fast_diag_smem(nbk), s, A, ld, (long long)k0, nbk, lk, st);
   int rest = n - k0 - nbk;
+  // dependent launch only where the bulk update runs capped: uncapped, it
+  // needs every SM, and panel CTAs launched early would sit waiting on them
+  const bool chained = rest <= CHAIN_PDL_ROWS;
+  if (chained) {
+    CK(launch_chain(potrf_diag_kernel, dim3(1), dim3(FD_THREADS), fast_diag_smem(nbk), s, A, ld, (long long)k0, nbk,
+                    lk, st));
+  } else {
+    GPRX_LAUNCH(potrf_diag_kernel, 1, FD_THREADS, fast_diag_smem(nbk), s, A, ld, (long long)k0, nbk, lk, st);
+  }
   if (rest > 0) {
     double* P = A + (k0 + nbk) + (long long)k0 * ld;
     // panel: P := P · L_kk⁻ᵀ, i.e. P(i,j) = Σ_k P(i,k) L_kk⁻¹(j,k) (in place:
     // a strip is staged whole before it is written)
-    CK(panel_gemm(rest, nbk, nbk, P, ld, lk, NB, P, ld, 1.0, 0.0, false, st, s));
+    CK(panel_gemm(rest, nbk, nbk, P, ld, lk, NB, P, ld, 1.0, 0.0, false, st, s, chained));
   }
   return cudaGetLastError();
 }
