@@ -10,7 +10,7 @@
 // DMMA m16n8k4 blocks (32×32 tiles keep eight warps busy and let the other
 // eight load); the shapes the autotuner picks from are listed in CgTile
 // below.  The k chunks (TK deep) of ALL tiles form one stream through
-// a 3-stage cp.async ring, so the next tile's first chunks load while the
+// a 2- or 3-stage cp.async ring, so the next tile's first chunks load while the
 // current tile computes, and the C values a tile needs (beta ≠ 0) are fetched
 // into registers when the tile starts.  Shared-memory layouts follow each
 // operand's contiguous direction (16-byte copies) with leading dimensions
@@ -33,17 +33,19 @@
 namespace gprx {
 
 constexpr int CG_THREADS = 512;
-constexpr int CG_STAGES = 3;
 constexpr int CG_FULL = 0, CG_FROM_ROW = 1, CG_FROM_COL = 2;
 
-// tile shapes (TM × TN, k chunk TK, warp grid WGM × WGN) by configuration index
+// tile shapes (TM × TN, k chunk TK, warp grid WGM × WGN, copy-ring stages ST)
+// by configuration index; the 64×128 tile takes 64-deep chunks in two stages
+// (half the barriers of 32-deep chunks in three; a chunk's DMMA work covers
+// the next chunk's copy)
 constexpr int CG_CONFIGS = 4;
 template <int CFG>
 struct CgTile;
-template <> struct CgTile<0> { static constexpr int M = 64, N = 128, K = 32, WGM = 4, WGN = 4; };
-template <> struct CgTile<1> { static constexpr int M = 64, N = 64, K = 32, WGM = 4, WGN = 4; };
-template <> struct CgTile<2> { static constexpr int M = 32, N = 64, K = 32, WGM = 2, WGN = 8; };
-template <> struct CgTile<3> { static constexpr int M = 32, N = 32, K = 16, WGM = 2, WGN = 4; };
+template <> struct CgTile<0> { static constexpr int M = 64, N = 128, K = 64, WGM = 4, WGN = 4, ST = 2; };
+template <> struct CgTile<1> { static constexpr int M = 64, N = 64, K = 32, WGM = 4, WGN = 4, ST = 3; };
+template <> struct CgTile<2> { static constexpr int M = 32, N = 64, K = 32, WGM = 2, WGN = 8, ST = 3; };
+template <> struct CgTile<3> { static constexpr int M = 32, N = 32, K = 16, WGM = 2, WGN = 4, ST = 3; };
 __host__ __device__ constexpr int cg_tile_n(int cfg) { return cfg == 0 ? 128 : cfg == 3 ? 32 : 64; }
 __host__ __device__ constexpr int cg_tile_m(int cfg) { return cfg <= 1 ? 64 : 32; }
 
@@ -67,7 +69,7 @@ constexpr size_t cg_smem_bytes_cfg() {
                                                                                  : CgA<false, T::M, T::K>::ELEMS;
   constexpr int b = CgB<true, T::N, T::K>::ELEMS > CgB<false, T::N, T::K>::ELEMS ? CgB<true, T::N, T::K>::ELEMS
                                                                                  : CgB<false, T::N, T::K>::ELEMS;
-  return (size_t)CG_STAGES * (a + b) * sizeof(double);
+  return (size_t)T::ST * (a + b) * sizeof(double);
 }
 constexpr size_t cg_max2(size_t a, size_t b) { return a > b ? a : b; }
 // the largest stage ring over the shapes and the four orientations
@@ -86,7 +88,7 @@ template <bool TA, bool TB, int CFG>
 __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
                          double* C, long long ldc, double alpha, double beta, bool lower, int kmode, double* smem) {
   constexpr int CG_M = CgTile<CFG>::M, CG_N = CgTile<CFG>::N, CG_K = CgTile<CFG>::K;
-  constexpr int WGM = CgTile<CFG>::WGM, WGN = CgTile<CFG>::WGN;
+  constexpr int WGM = CgTile<CFG>::WGM, WGN = CgTile<CFG>::WGN, ST = CgTile<CFG>::ST;
   constexpr int WM = CG_M / WGM, WN = CG_N / WGN, MI = WM / 16, NJ = WN / 8;
   static_assert(WGM * WGN <= CG_THREADS / 32 && MI >= 1 && NJ >= 1, "warp grid");
   using SA = CgA<TA, CG_M, CG_K>;
@@ -197,7 +199,7 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
 
   __syncthreads();  // the previous user of the stages is done
 #pragma unroll
-  for (int s = 0; s < CG_STAGES - 1; ++s) load_next(s);
+  for (int s = 0; s < ST - 1; ++s) load_next(s);
   int gch = 0;  // chunks consumed so far
   for (int ct = next_used(0); ct < ntiles; ct = next_used(ct + 1)) {
     const int m0 = (ct % tm_n) * CG_M, n0 = (ct / tm_n) * CG_N;
@@ -224,11 +226,11 @@ __device__ void cta_gemm_tile(int M, int N, int K, const double* A, long long ld
 #pragma unroll
         for (int r = 0; r < 4; ++r) acc[mi][nj][r] = 0.0;
     for (int c = 0; c < nch; ++c, ++gch) {
-      cp_async_wait<CG_STAGES - 2>();
+      cp_async_wait<ST - 2>();
       __syncthreads();
-      load_next((gch + CG_STAGES - 1) % CG_STAGES);
+      load_next((gch + ST - 1) % ST);
       if (!wskip) {
-        const double* sA = smem + (gch % CG_STAGES) * STAGE;
+        const double* sA = smem + (gch % ST) * STAGE;
         const double* sB = sA + SA::ELEMS;
 #pragma unroll
         for (int kk = 0; kk < CG_K; kk += 4) {

@@ -466,7 +466,7 @@ gprx_status gprx_batch_stream(gprx_batch* h, void** stream);
 /* Schedule of the batched evaluation (no counterpart in the reference).
  * Problems fall into GPRX_BATCH_SIZE_CLASSES size classes (n ≤ 64, ≤ 128,
  * …, ≤ 4096, larger); each class runs its in-CTA FP64 GEMMs with one of
- * GPRX_BATCH_TILE_SHAPES tile shapes (0: 64×128×32, 1: 64×64×32,
+ * GPRX_BATCH_TILE_SHAPES tile shapes (0: 64×128×64, 1: 64×64×32,
  * 2: 32×64×32, 3: 32×32×16).  The first gprx_batch_eval / gprx_batch_fit
  * autotunes it: every class present is timed with every shape on a sample of
  * its problems and the fastest is kept (cached per device and kernel tree
