@@ -178,6 +178,7 @@ static cudaError_t diag_attrs() {
 FactorCtx::~FactorCtx() {
   for (auto e : ev) cudaEventDestroy(e);
   if (aux) cudaStreamDestroy(aux);
+  if (aux2) cudaStreamDestroy(aux2);
 }
 
 cudaError_t FactorCtx::ensure(int nblk) {
@@ -186,7 +187,12 @@ cudaError_t FactorCtx::ensure(int nblk) {
     CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     CK(cudaStreamCreateWithPriority(&aux, cudaStreamNonBlocking, hi));
   }
-  while ((int)ev.size() < 2 * nblk + 2) {
+  if (!aux2) {
+    int lo, hi;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&aux2, cudaStreamNonBlocking, hi));
+  }
+  while ((int)ev.size() < 3 * nblk + 2) {
     cudaEvent_t e;
     CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     ev.push_back(e);
@@ -349,8 +355,10 @@ static cudaError_t panel_gemm(int M, int N, int K, const double* A, long long ld
 // (the same bound as the bulk update's cap, BULK_CAP_ROWS)
 constexpr int CHAIN_PDL_ROWS = 4096;
 
+// The diagonal block at k0 and the panel below it.  before_panel: an event
+// the panel waits for (the rest of the column update on another stream).
 static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double* linv, DevStatus* st,
-                                  cudaStream_t s) {
+                                  cudaStream_t s, cudaEvent_t before_panel = nullptr) {
   int nbk = min(NB, n - k0);
   double* lk = linv + (long long)(k0 / NB) * NB * NB;
   int rest = n - k0 - nbk;
@@ -366,8 +374,10 @@ static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double
   if (rest > 0) {
     double* P = A + (k0 + nbk) + (long long)k0 * ld;
     // panel: P := P · L_kk⁻ᵀ, i.e. P(i,j) = Σ_k P(i,k) L_kk⁻¹(j,k) (in place:
-    // a strip is staged whole before it is written)
-    CK(panel_gemm(rest, nbk, nbk, P, ld, lk, NB, P, ld, 1.0, 0.0, false, st, s, chained));
+    // a strip is staged whole before it is written); after an event wait the
+    // launch is a plain one
+    if (before_panel) CK(cudaStreamWaitEvent(s, before_panel, 0));
+    CK(panel_gemm(rest, nbk, nbk, P, ld, lk, NB, P, ld, 1.0, 0.0, false, st, s, chained && !before_panel));
   }
   return cudaGetLastError();
 }
@@ -403,7 +413,9 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
   cudaStream_t X = ctx->aux;
   cudaEvent_t* Ep = ctx->ev.data();          // panel k done (on X)
   cudaEvent_t* Es = ctx->ev.data() + nblk;   // trailing update of step k done (on s)
+  cudaEvent_t* Ec = ctx->ev.data() + 2 * nblk + 2;  // column update's lower rows of step k done (on aux2)
   cudaEvent_t Ein = ctx->ev[2 * nblk];
+  cudaStream_t X2 = ctx->aux2;
   CK(cudaEventRecord(Ein, s));
   CK(cudaStreamWaitEvent(X, Ein, 0));
   CK(diag_and_panel(A, ld, n, 0, linv, st, X));
@@ -414,14 +426,23 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
     if (c1 >= n) break;
     const int k0 = k * NB;
     const double* Pk = A + c1 + (long long)k0 * ld;  // panel k, rows from c1
-    // critical chain of block k+1 (side stream)
+    // critical chain of block k+1 (side stream): column block k+1 −= panel
+    // k · (its top rows)ᵀ — the diagonal block's rows on the chain, the rows
+    // below on aux2 while the diagonal block is factored; the panel solve
+    // waits for both
     if (k >= 1) CK(cudaStreamWaitEvent(X, Es[k - 1], 0));
-    {
-      // column block k+1 −= panel k · (its top rows)ᵀ, lower part
-      int m = n - c1, w = min(NB, n - c1);
-      CK(panel_gemm(m, w, NB, Pk, ld, Pk, ld, A + c1 + (long long)c1 * ld, ld, -1.0, 1.0, true, st, X));
+    const int m = n - c1, w = min(NB, n - c1);
+    cudaEvent_t lower_done = nullptr;
+    if (m > NB) {
+      if (k >= 1) CK(cudaStreamWaitEvent(X2, Es[k - 1], 0));
+      CK(cudaStreamWaitEvent(X2, Ep[k], 0));
+      CK(panel_gemm(m - NB, w, NB, Pk + NB, ld, Pk, ld, A + (c1 + NB) + (long long)c1 * ld, ld, -1.0, 1.0, false, st,
+                    X2));
+      CK(cudaEventRecord(Ec[k], X2));
+      lower_done = Ec[k];
     }
-    CK(diag_and_panel(A, ld, n, c1, linv, st, X));
+    CK(panel_gemm(min(m, NB), w, NB, Pk, ld, Pk, ld, A + c1 + (long long)c1 * ld, ld, -1.0, 1.0, true, st, X));
+    CK(diag_and_panel(A, ld, n, c1, linv, st, X, lower_done));
     CK(cudaEventRecord(Ep[k + 1], X));
     last = k + 1;
     // bulk trailing update of step k (main stream): columns from c2

@@ -22,10 +22,13 @@ cudaError_t dgemm_nn_fill(const GemmParams& p, cudaStream_t s, int batch);
 GemmParams gemm_params(int M, int N, int K, const double* A, long long lda, const double* B, long long ldb,
                        double* C, long long ldc, double alpha, double beta, const DevStatus* st);
 
-// Side stream and events of the look-ahead factorization (one per handle).
+// Side streams and events of the look-ahead factorization (one per handle):
+// aux carries the chain, aux2 the column update's rows below the diagonal
+// block (concurrent with the diagonal block).
 struct FactorCtx {
   int device = -1;
   cudaStream_t aux = nullptr;
+  cudaStream_t aux2 = nullptr;
   std::vector<cudaEvent_t> ev;
   ~FactorCtx();
   cudaError_t ensure(int nblk);
