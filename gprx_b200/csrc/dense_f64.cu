@@ -352,7 +352,8 @@ static cudaError_t panel_gemm(int M, int N, int K, const double* A, long long ld
 }
 
 // rows below the diagonal block up to which the chain uses dependent launch
-// (the same bound as the bulk update's cap, BULK_CAP_ROWS)
+// (at larger trailing blocks the bulk update fills the GPU, and panel CTAs
+// launched early would sit waiting on SMs it could use)
 constexpr int CHAIN_PDL_ROWS = 4096;
 
 // The diagonal block at k0 and the panel below it.  before_panel: an event
@@ -362,8 +363,6 @@ static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double
   int nbk = min(NB, n - k0);
   double* lk = linv + (long long)(k0 / NB) * NB * NB;
   int rest = n - k0 - nbk;
-  // dependent launch only where the bulk update runs capped: uncapped, it
-  // needs every SM, and panel CTAs launched early would sit waiting on them
   const bool chained = rest <= CHAIN_PDL_ROWS;
   if (chained) {
     CK(launch_chain(potrf_diag_kernel, dim3(1), dim3(FD_THREADS), fast_diag_smem(nbk), s, A, ld, (long long)k0, nbk,
@@ -382,15 +381,14 @@ static cudaError_t diag_and_panel(double* A, long long ld, int n, int k0, double
   return cudaGetLastError();
 }
 
-// CTAs of the bulk trailing update in the look-ahead factor (of 148 SMs)
-// once its trailing block has at most BULK_CAP_ROWS rows; a larger block is
-// the slower side of a step and takes every SM.  Measured (FP64 factor
-// probe): n = 4096 3.07 ms with the cap against 3.14 without; n = 8192
-// 12.95 with the cap at every step against 12.37 without.  A split that
-// gave the chain more SMs when the bulk update is small was slower too
-// (mixed n = 8192: 16.5 against 15.9 ms).
-constexpr int BULK_CTAS = 132;
-constexpr int BULK_CAP_ROWS = 4096;
+// The bulk trailing update of the look-ahead factor (K = NB) runs on 64×128
+// tiles: half the registers of the 128×128 tile, so two CTAs share an SM and
+// one's copies and epilogue overlap the other's DMMA work, and CTAs short
+// enough that the chain's high-priority kernels get SMs as they retire (no
+// SM is held back).  Measured (FP64 factor probe, n = 4096 / 8192): 2.42 /
+// 10.35 ms, against 2.55 / 11.67 ms with 128×128 tiles capped at 132 CTAs
+// while the trailing block has at most 4096 rows, 3.14 / 11.34 ms with the
+// 64×128 tiles capped at 132 CTAs and 2.53 / 10.40 ms capped at 264.
 
 cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatus* st, cudaStream_t s,
                           FactorCtx* ctx) {
@@ -453,8 +451,7 @@ cudaError_t potrf_blocked(double* A, long long ld, int n, double* linv, DevStatu
       const double* Pk2 = A + c2 + (long long)k0 * ld;
       GemmParams ps = gemm_params(m, m, NB, Pk2, ld, Pk2, ld, A + c2 + (long long)c2 * ld, ld, -1.0, 1.0, st);
       ps.mode = GEMM_LOWER_TILES;
-      ps.max_ctas = m <= BULK_CAP_ROWS ? BULK_CTAS : 0;  // leave SMs free for the side stream's chain
-      CK(dgemm(false, true, ps, s));
+      CK((launch_dgemm<64, 128, 16, 32, 32, 3, false, true>(ps, 1, s)));
     }
     CK(cudaEventRecord(Es[k], s));
   }
