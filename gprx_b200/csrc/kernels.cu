@@ -406,6 +406,98 @@ __global__ void __launch_bounds__(GRAD_THREADS, ARD_D <= 8 ? 2 : 1) grad_contrac
   store_slots<NS>(vals, red, partials + (long long)blockIdx.x * NS);
 }
 
+// The same contraction for trees of at most NL leaves, PW pairs per thread
+// (independent FP64 chains the scheduler interleaves).  A thread takes the
+// same pairs in the same order as grad_contract_kernel and pairs outside the
+// lower triangle add exact zeros, so every accumulator receives the same
+// terms in the same order: the same bits (a tree has at most one ARD leaf,
+// so no two leaves share an accumulator).
+template <int ARD_D, int NL, int PW>
+__global__ void __launch_bounds__(GRAD_THREADS, 2) grad_contract_w_kernel(KTree t, const double* x, long long ldx,
+                                                                          int n, const double* kinv, long long ld,
+                                                                          const double* alpha, double* partials,
+                                                                          const DevStatus* st) {
+  constexpr int AD = ARD_D > 0 ? ARD_D : 1;
+  constexpr int NS = GRAD_SLOTS_LEAF + AD + 1;
+  constexpr int CS = GRAD_THREADS / FT;  // column stride of one thread
+  static_assert((FT / CS) % PW == 0, "pairs per thread");
+  __shared__ double xi[GPRX_MAX_DIM * FT];
+  __shared__ double xj[GPRX_MAX_DIM * FT];
+  __shared__ double ai[FT], aj[FT];
+  __shared__ double red[GRAD_THREADS / 32][NS];
+  if (dev_failed(st)) return;
+  const int d = t.d;
+  const bool amode = alpha != nullptr;
+  double acc_leaf[NL][KT_ACC_PER_LEAF];
+  double acc_ard[AD];
+  double acc_noise = 0.0;
+#pragma unroll
+  for (int l = 0; l < NL; ++l) acc_leaf[l][0] = acc_leaf[l][1] = 0.0;
+#pragma unroll
+  for (int f = 0; f < AD; ++f) acc_ard[f] = 0.0;
+
+  const int nt = (n + FT - 1) / FT;
+  const long long ntiles = (long long)nt * (nt + 1) / 2;
+  for (long long idx = blockIdx.x; idx < ntiles; idx += gridDim.x) {
+    int ti, tj;
+    lower_tile_of(idx, ti, tj);
+    const int i0 = ti * FT, j0 = tj * FT;
+    __syncthreads();
+    for (int e = threadIdx.x; e < d * FT; e += blockDim.x) {
+      int r = e % FT, f = e / FT;
+      xi[f * FT + r] = (i0 + r < n) ? x[(i0 + r) + (long long)f * ldx] : 0.0;
+      xj[f * FT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * ldx] : 0.0;
+    }
+    if (amode && threadIdx.x < FT) {
+      int r = threadIdx.x;
+      ai[r] = (i0 + r < n) ? alpha[i0 + r] : 0.0;
+      aj[r] = (j0 + r < n) ? alpha[j0 + r] : 0.0;
+    }
+    __syncthreads();
+    const int r = threadIdx.x % FT;
+    const int i = i0 + r;
+    if (i >= n) continue;
+#pragma unroll 1
+    for (int c0 = threadIdx.x / FT; c0 < FT; c0 += CS * PW) {
+      if (j0 + c0 > i) break;  // every later pair of this thread lies above the diagonal
+      double dx[PW][AD], r2[PW], wt[PW];
+#pragma unroll
+      for (int w = 0; w < PW; ++w) {
+        const int c = c0 + w * CS, j = j0 + c;
+        const bool in = j < n && i >= j;
+        double cw = 0.0;
+        if (in) {
+          const double m = kinv[i + (long long)j * ld];
+          const double wv = amode ? fma(ai[r], aj[c], -m) : m;
+          cw = (i == j) ? wv : 2.0 * wv;
+          if (i == j) acc_noise += wv;
+        }
+        wt[w] = cw;
+        double rr = 0.0;
+        for (int f = 0; f < d; ++f) {
+          const double v = xi[f * FT + r] - xj[f * FT + c];
+          rr = fma(v, v, rr);
+          if (ARD_D > 0) {
+#pragma unroll
+            for (int g = 0; g < AD; ++g)
+              if (g == f) dx[w][g] = v;
+          }
+        }
+        r2[w] = rr;
+      }
+      kt_accumulate_grad_w<ARD_D, PW, NL>(t, dx, r2, wt, acc_leaf, acc_ard);
+    }
+  }
+  double vals[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    if (s < GRAD_SLOTS_LEAF) vals[s] = (s / 2 < NL) ? acc_leaf[s / 2][s % 2] : 0.0;
+    else if (s < GRAD_SLOTS_LEAF + AD) vals[s] = acc_ard[s - GRAD_SLOTS_LEAF];
+    else vals[s] = acc_noise;
+  }
+  store_slots<NS>(vals, red, partials + (long long)blockIdx.x * NS);
+}
+
 // Rectangle contraction Σ_{i,c} W_ic ∂k(z_i, x_c)/∂θ (W is m×n, ldw).
 template <int ARD_D>
 __global__ void __launch_bounds__(GRAD_THREADS, ARD_D <= 8 ? 2 : 1) cross_contract_kernel(KTree t, const double* z, long long ldz, int m,
@@ -474,6 +566,19 @@ cudaError_t grad_contract(const HostKernel& k, const double* x, long long ldx, i
   *blocks_out = grid;
 #define GPRX_GRAD(D) \
   GPRX_LAUNCH(grad_contract_kernel<D>, grid, GRAD_THREADS, 0, s, k.tree, x, ldx, n, kinv, ld, alpha, partials, st)
+#define GPRX_GRAD_W(D)                                                                                         \
+  GPRX_LAUNCH((grad_contract_w_kernel<D, 2, 2>), grid, GRAD_THREADS, 0, s, k.tree, x, ldx, n, kinv, ld, alpha, \
+              partials, st)
+  // trees of at most two leaves: two pairs per thread
+  if (k.tree.n_leaves <= 2 && (k.ard_d == 0 || k.ard_d == 4 || k.ard_d == 8)) {
+    switch (k.ard_d) {
+      case 0: GPRX_GRAD_W(0); break;
+      case 4: GPRX_GRAD_W(4); break;
+      default: GPRX_GRAD_W(8); break;
+    }
+    return cudaGetLastError();
+  }
+#undef GPRX_GRAD_W
   switch (k.ard_d) {
     case 0: GPRX_GRAD(0); break;
     case 4: GPRX_GRAD(4); break;
