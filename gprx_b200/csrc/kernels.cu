@@ -234,6 +234,70 @@ __global__ void __launch_bounds__(FILL_THREADS) fill_lower_kernel(KTree t, const
   if (bad) dev_fail(st, GPRX_NONFINITE_KERNEL, 0);
 }
 
+// The lower fill for trees of at most NL leaves, PW pairs per thread
+// (independent FP64 chains); every value is computed as in fill_lower_kernel.
+template <int ARD_D, int NL, int PW>
+__global__ void __launch_bounds__(FILL_THREADS) fill_lower_w_kernel(KTree t, const double* x, long long ldx, int n,
+                                                                    double* K, long long ld, double diag_add,
+                                                                    DevStatus* st) {
+  constexpr int AD = ARD_D > 0 ? ARD_D : 1;
+  constexpr int CS = FILL_THREADS / FT;
+  static_assert((FT / CS) % PW == 0, "pairs per thread");
+  __shared__ double xi[GPRX_MAX_DIM * FT];
+  __shared__ double xj[GPRX_MAX_DIM * FT];
+  if (dev_failed(st)) return;
+  const int d = t.d;
+  const int nt = (n + FT - 1) / FT;
+  const long long ntiles = (long long)nt * (nt + 1) / 2;
+  bool bad = false;
+  for (long long idx = blockIdx.x; idx < ntiles; idx += gridDim.x) {
+    int ti, tj;
+    lower_tile_of(idx, ti, tj);
+    const int i0 = ti * FT, j0 = tj * FT;
+    __syncthreads();
+    for (int e = threadIdx.x; e < d * FT; e += blockDim.x) {
+      int r = e % FT, f = e / FT;
+      xi[f * FT + r] = (i0 + r < n) ? x[(i0 + r) + (long long)f * ldx] : 0.0;
+      xj[f * FT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * ldx] : 0.0;
+    }
+    __syncthreads();
+    const int r = threadIdx.x % FT;
+    const int i = i0 + r;
+    if (i >= n) continue;
+#pragma unroll 1
+    for (int c0 = threadIdx.x / FT; c0 < FT; c0 += CS * PW) {
+      if (j0 + c0 > i) break;  // every later pair of this thread lies above the diagonal
+      double dx[PW][AD], r2[PW], kv[PW];
+#pragma unroll
+      for (int w = 0; w < PW; ++w) {
+        const int c = c0 + w * CS;
+        double rr = 0.0;
+        for (int f = 0; f < d; ++f) {
+          const double v = xi[f * FT + r] - xj[f * FT + c];
+          rr = fma(v, v, rr);
+          if (ARD_D > 0) {
+#pragma unroll
+            for (int g = 0; g < AD; ++g)
+              if (g == f) dx[w][g] = v;
+          }
+        }
+        r2[w] = rr;
+      }
+      kt_value_w<ARD_D, PW, NL>(t, dx, r2, kv);
+#pragma unroll
+      for (int w = 0; w < PW; ++w) {
+        const int j = j0 + c0 + w * CS;
+        if (j >= n || i < j) continue;
+        double v = kv[w];
+        if (i == j) v += diag_add;
+        if (!isfinite(v)) bad = true;
+        K[i + (long long)j * ld] = v;
+      }
+    }
+  }
+  if (bad) dev_fail(st, GPRX_NONFINITE_KERNEL, 0);
+}
+
 template <int ARD_D>
 __global__ void __launch_bounds__(FILL_THREADS) fill_cross_kernel(KTree t, const double* x1, long long ldx1, int n1,
                                                                   const double* x2, long long ldx2, int n2,
@@ -276,6 +340,15 @@ cudaError_t fill_lower(const HostKernel& k, const double* x, long long ldx, int 
                        double diag_add, DevStatus* st, cudaStream_t s) {
   int nt = (n + FT - 1) / FT;
   int grid = fill_grid((long long)nt * (nt + 1) / 2);
+  // trees of at most two leaves: four pairs per thread
+  if (k.tree.n_leaves <= 2 && (k.ard_d == 0 || k.ard_d == 4 || k.ard_d == 8)) {
+    switch (k.ard_d) {
+      case 0: GPRX_LAUNCH((fill_lower_w_kernel<0, 2, 4>), grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
+      case 4: GPRX_LAUNCH((fill_lower_w_kernel<4, 2, 4>), grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
+      default: GPRX_LAUNCH((fill_lower_w_kernel<8, 2, 4>), grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
+    }
+    return cudaGetLastError();
+  }
   switch (k.ard_d) {
     case 0: GPRX_LAUNCH(fill_lower_kernel<0>, grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
     case 4: GPRX_LAUNCH(fill_lower_kernel<4>, grid, FILL_THREADS, 0, s, k.tree, x, ldx, n, K, ld, diag_add, st); break;
