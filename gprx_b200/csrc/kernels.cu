@@ -331,6 +331,66 @@ __global__ void __launch_bounds__(FILL_THREADS) fill_cross_kernel(KTree t, const
   if (bad) dev_fail(st, GPRX_NONFINITE_KERNEL, 0);
 }
 
+// The cross fill for trees of at most NL leaves, PW pairs per thread; every
+// value is computed as in fill_cross_kernel.
+template <int ARD_D, int NL, int PW>
+__global__ void __launch_bounds__(FILL_THREADS) fill_cross_w_kernel(KTree t, const double* x1, long long ldx1,
+                                                                    int n1, const double* x2, long long ldx2, int n2,
+                                                                    double* out, long long ld, DevStatus* st) {
+  constexpr int AD = ARD_D > 0 ? ARD_D : 1;
+  constexpr int CS = FILL_THREADS / FT;
+  static_assert((FT / CS) % PW == 0, "pairs per thread");
+  __shared__ double xi[GPRX_MAX_DIM * FT];
+  __shared__ double xj[GPRX_MAX_DIM * FT];
+  if (dev_failed(st)) return;
+  const int d = t.d;
+  const int tm = (n1 + FT - 1) / FT, tn = (n2 + FT - 1) / FT;
+  const long long ntiles = (long long)tm * tn;
+  bool bad = false;
+  for (long long idx = blockIdx.x; idx < ntiles; idx += gridDim.x) {
+    const int i0 = (int)(idx % tm) * FT, j0 = (int)(idx / tm) * FT;
+    __syncthreads();
+    for (int e = threadIdx.x; e < d * FT; e += blockDim.x) {
+      int r = e % FT, f = e / FT;
+      xi[f * FT + r] = (i0 + r < n1) ? x1[(i0 + r) + (long long)f * ldx1] : 0.0;
+      xj[f * FT + r] = (j0 + r < n2) ? x2[(j0 + r) + (long long)f * ldx2] : 0.0;
+    }
+    __syncthreads();
+    const int r = threadIdx.x % FT;
+    const int i = i0 + r;
+    if (i >= n1) continue;
+#pragma unroll 1
+    for (int c0 = threadIdx.x / FT; c0 < FT; c0 += CS * PW) {
+      if (j0 + c0 >= n2) break;
+      double dx[PW][AD], r2[PW], kv[PW];
+#pragma unroll
+      for (int w = 0; w < PW; ++w) {
+        const int c = c0 + w * CS;
+        double rr = 0.0;
+        for (int f = 0; f < d; ++f) {
+          const double v = xi[f * FT + r] - xj[f * FT + c];
+          rr = fma(v, v, rr);
+          if (ARD_D > 0) {
+#pragma unroll
+            for (int g = 0; g < AD; ++g)
+              if (g == f) dx[w][g] = v;
+          }
+        }
+        r2[w] = rr;
+      }
+      kt_value_w<ARD_D, PW, NL>(t, dx, r2, kv);
+#pragma unroll
+      for (int w = 0; w < PW; ++w) {
+        const int j = j0 + c0 + w * CS;
+        if (j >= n2) continue;
+        if (!isfinite(kv[w])) bad = true;
+        out[i + (long long)j * ld] = kv[w];
+      }
+    }
+  }
+  if (bad) dev_fail(st, GPRX_NONFINITE_KERNEL, 0);
+}
+
 static int fill_grid(long long ntiles) {
   long long cap = 148LL * 8;
   return (int)std::max<long long>(1, std::min(ntiles, cap));
@@ -366,6 +426,19 @@ cudaError_t fill_cross(const HostKernel& k, const double* x1, long long ldx1, in
   int grid = fill_grid(ntiles);
 #define GPRX_CROSS(D) \
   GPRX_LAUNCH(fill_cross_kernel<D>, grid, FILL_THREADS, 0, s, k.tree, x1, ldx1, n1, x2, ldx2, n2, out, ld, st)
+#define GPRX_CROSS_W(D)                                                                                         \
+  GPRX_LAUNCH((fill_cross_w_kernel<D, 2, 4>), grid, FILL_THREADS, 0, s, k.tree, x1, ldx1, n1, x2, ldx2, n2, out, \
+              ld, st)
+  // trees of at most two leaves: four pairs per thread
+  if (k.tree.n_leaves <= 2 && (k.ard_d == 0 || k.ard_d == 4 || k.ard_d == 8)) {
+    switch (k.ard_d) {
+      case 0: GPRX_CROSS_W(0); break;
+      case 4: GPRX_CROSS_W(4); break;
+      default: GPRX_CROSS_W(8); break;
+    }
+    return cudaGetLastError();
+  }
+#undef GPRX_CROSS_W
   switch (k.ard_d) {
     case 0: GPRX_CROSS(0); break;
     case 4: GPRX_CROSS(4); break;
@@ -631,6 +704,76 @@ __global__ void __launch_bounds__(GRAD_THREADS, ARD_D <= 8 ? 2 : 1) cross_contra
   store_slots<NS>(vals, red, partials + (long long)blockIdx.x * NS);
 }
 
+// The cross contraction for trees of at most NL leaves, PW pairs per thread;
+// every accumulator receives the terms of cross_contract_kernel in the same
+// order (pairs past the matrix add exact zeros): the same bits.
+template <int ARD_D, int NL, int PW>
+__global__ void __launch_bounds__(GRAD_THREADS, 2) cross_contract_w_kernel(KTree t, const double* z, long long ldz,
+                                                                           int m, const double* x, long long ldx,
+                                                                           int n, const double* W, long long ldw,
+                                                                           double* partials, const DevStatus* st) {
+  constexpr int AD = ARD_D > 0 ? ARD_D : 1;
+  constexpr int NS = GRAD_SLOTS_LEAF + AD + 1;
+  constexpr int CS = GRAD_THREADS / FT;
+  static_assert((FT / CS) % PW == 0, "pairs per thread");
+  __shared__ double xi[GPRX_MAX_DIM * FT];
+  __shared__ double xj[GPRX_MAX_DIM * FT];
+  __shared__ double red[GRAD_THREADS / 32][NS];
+  if (dev_failed(st)) return;
+  const int d = t.d;
+  double acc_leaf[NL][KT_ACC_PER_LEAF];
+  double acc_ard[AD];
+#pragma unroll
+  for (int l = 0; l < NL; ++l) acc_leaf[l][0] = acc_leaf[l][1] = 0.0;
+#pragma unroll
+  for (int f = 0; f < AD; ++f) acc_ard[f] = 0.0;
+  const int tm = (m + FT - 1) / FT, tn = (n + FT - 1) / FT;
+  const long long ntiles = (long long)tm * tn;
+  for (long long idx = blockIdx.x; idx < ntiles; idx += gridDim.x) {
+    const int i0 = (int)(idx % tm) * FT, j0 = (int)(idx / tm) * FT;
+    __syncthreads();
+    for (int e = threadIdx.x; e < d * FT; e += blockDim.x) {
+      int r = e % FT, f = e / FT;
+      xi[f * FT + r] = (i0 + r < m) ? z[(i0 + r) + (long long)f * ldz] : 0.0;
+      xj[f * FT + r] = (j0 + r < n) ? x[(j0 + r) + (long long)f * ldx] : 0.0;
+    }
+    __syncthreads();
+    const int r = threadIdx.x % FT;
+    const int i = i0 + r;
+    if (i >= m) continue;
+#pragma unroll 1
+    for (int c0 = threadIdx.x / FT; c0 < FT; c0 += CS * PW) {
+      if (j0 + c0 >= n) break;
+      double dx[PW][AD], r2[PW], wt[PW];
+#pragma unroll
+      for (int w = 0; w < PW; ++w) {
+        const int c = c0 + w * CS, j = j0 + c;
+        wt[w] = j < n ? W[i + (long long)j * ldw] : 0.0;
+        double rr = 0.0;
+        for (int f = 0; f < d; ++f) {
+          const double v = xi[f * FT + r] - xj[f * FT + c];
+          rr = fma(v, v, rr);
+          if (ARD_D > 0) {
+#pragma unroll
+            for (int g = 0; g < AD; ++g)
+              if (g == f) dx[w][g] = v;
+          }
+        }
+        r2[w] = rr;
+      }
+      kt_accumulate_grad_w<ARD_D, PW, NL>(t, dx, r2, wt, acc_leaf, acc_ard);
+    }
+  }
+  double vals[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    if (s < GRAD_SLOTS_LEAF) vals[s] = (s / 2 < NL) ? acc_leaf[s / 2][s % 2] : 0.0;
+    else if (s < GRAD_SLOTS_LEAF + AD) vals[s] = acc_ard[s - GRAD_SLOTS_LEAF];
+    else vals[s] = 0.0;
+  }
+  store_slots<NS>(vals, red, partials + (long long)blockIdx.x * NS);
+}
+
 cudaError_t grad_contract(const HostKernel& k, const double* x, long long ldx, int n, const double* kinv, long long ld,
                           const double* alpha, double* partials, int* blocks_out, DevStatus* st, cudaStream_t s) {
   int nt = (n + FT - 1) / FT;
@@ -672,6 +815,19 @@ cudaError_t cross_contract(const HostKernel& k, const double* z, long long ldz, 
 #define GPRX_CC(D)                                                                                                  \
   GPRX_LAUNCH(cross_contract_kernel<D>, grid, GRAD_THREADS, 0, s, k.tree, z, ldz, m, x, ldx, n, W, ldw, partials, \
               st)
+#define GPRX_CC_W(D)                                                                                             \
+  GPRX_LAUNCH((cross_contract_w_kernel<D, 2, 2>), grid, GRAD_THREADS, 0, s, k.tree, z, ldz, m, x, ldx, n, W, ldw, \
+              partials, st)
+  // trees of at most two leaves: two pairs per thread
+  if (k.tree.n_leaves <= 2 && (k.ard_d == 0 || k.ard_d == 4 || k.ard_d == 8)) {
+    switch (k.ard_d) {
+      case 0: GPRX_CC_W(0); break;
+      case 4: GPRX_CC_W(4); break;
+      default: GPRX_CC_W(8); break;
+    }
+    return cudaGetLastError();
+  }
+#undef GPRX_CC_W
   switch (k.ard_d) {
     case 0: GPRX_CC(0); break;
     case 4: GPRX_CC(4); break;
